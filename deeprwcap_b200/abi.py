@@ -1,0 +1,160 @@
+"""ctypes mirrors of the structs in ``include/drwc.h`` and the loader of the
+CUDA library ``deeprwcap_b200/libdrwc.so``.
+
+The library is the product: every compute entry point of this package goes
+through it. There is no CPU fallback — when the library or a CUDA device is
+missing the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+LIB_PATH = PKG / "libdrwc.so"
+
+MAX_NETS = 256
+MAX_LAYERS = 15
+MAX_CUBOIDS = 15
+LAYER_STRIDE = 2 * MAX_LAYERS
+CUBOID_STRIDE = 7 * MAX_CUBOIDS
+PADDING = -9999.0
+N_MIN, N_MAX = 4, 23
+
+GFT, WVTZ, WVTX, WVTY = 0, 1, 2, 3
+
+STATUS = {
+    0: "DRWC_OK", 1: "DRWC_ERR_INVALID", 2: "DRWC_ERR_CUDA", 3: "DRWC_ERR_NOMEM",
+    4: "DRWC_ERR_NOT_CONVERGED", 5: "DRWC_ERR_NO_DEVICE", 6: "DRWC_ERR_TIMEOUT",
+    7: "DRWC_ERR_SHUTDOWN", 8: "DRWC_ERR_GEOMETRY",
+}
+
+# Every symbol include/drwc.h declares (checked by the CPU tests).
+EXPORTS = [
+    "drwc_version", "drwc_status_string", "drwc_ctx_create", "drwc_ctx_destroy",
+    "drwc_ctx_stream", "drwc_ctx_synchronize", "drwc_ctx_launch_count",
+    "drwc_fdm_opts_default", "drwc_ggft_solve", "drwc_fdm_solve_batch_device",
+    "drwc_fdm_solve_batch", "drwc_structure_construction", "drwc_transition_batch",
+    "drwc_first_hop_batch", "drwc_job_params_default", "drwc_frw_run", "drwc_frw_walks",
+    "drwc_job_create", "drwc_job_destroy", "drwc_job_walks_device", "drwc_job_h2d_bytes",
+]
+
+
+class DrwcError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        super().__init__(f"{where}: {STATUS.get(status, status)}")
+        self.status = status
+
+
+class FdmOpts(C.Structure):
+    _fields_ = [("tol", C.c_double), ("inner_tol", C.c_double),
+                ("max_outer", C.c_int32), ("max_inner", C.c_int32)]
+
+
+class Box(C.Structure):
+    _fields_ = [("lo", C.c_double * 3), ("hi", C.c_double * 3), ("net", C.c_int32),
+                ("pad_", C.c_int32)]
+
+
+class DielBox(C.Structure):
+    _fields_ = [("lo", C.c_double * 3), ("hi", C.c_double * 3), ("eps", C.c_double)]
+
+
+class Structure(C.Structure):
+    _fields_ = [("n_boxes", C.c_int32), ("n_nets", C.c_int32), ("boxes", C.POINTER(Box)),
+                ("n_layers", C.c_int32), ("n_diel", C.c_int32),
+                ("layer_zlo", C.POINTER(C.c_double)), ("layer_eps", C.POINTER(C.c_double)),
+                ("diel", C.POINTER(DielBox)), ("encl_lo", C.c_double * 3),
+                ("encl_hi", C.c_double * 3)]
+
+
+class JobParams(C.Structure):
+    _fields_ = [("master", C.c_int32), ("N", C.c_int32), ("gauss_offset", C.c_double),
+                ("stop_dist", C.c_double), ("p_tol", C.c_double), ("c_tol", C.c_double),
+                ("c_ratio", C.c_double), ("min_walks", C.c_int64), ("max_walks", C.c_int64),
+                ("batch_walks", C.c_int64), ("max_hops", C.c_int32), ("pad_", C.c_int32),
+                ("seed", C.c_uint64), ("fdm", FdmOpts)]
+
+
+class JobResult(C.Structure):
+    _fields_ = [("n_entries", C.c_int32), ("converged", C.c_int32), ("walks", C.c_int64),
+                ("hops", C.c_int64), ("lost", C.c_int64), ("seconds", C.c_double),
+                ("cap", C.c_double * (MAX_NETS + 1)), ("stderr_", C.c_double * (MAX_NETS + 1))]
+
+
+_lib = None
+
+
+def load():
+    """Load libdrwc.so (built by ``deeprwcap_b200.build``). Raises when it is
+    missing: there is no fallback path."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise FileNotFoundError(
+            f"{LIB_PATH} is missing: build it with `python -m deeprwcap_b200.build` "
+            "(the FRW engine has no CPU fallback)")
+    L = C.CDLL(str(LIB_PATH))
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    L.drwc_version.restype = C.c_char_p
+    L.drwc_status_string.restype = C.c_char_p
+    L.drwc_status_string.argtypes = [C.c_int]
+    L.drwc_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
+    L.drwc_ctx_destroy.argtypes = [vp]
+    L.drwc_ctx_stream.argtypes = [vp, C.POINTER(vp)]
+    L.drwc_ctx_synchronize.argtypes = [vp]
+    L.drwc_ctx_launch_count.argtypes = [vp, C.POINTER(i64)]
+    L.drwc_fdm_opts_default.argtypes = [C.POINTER(FdmOpts)]
+    L.drwc_fdm_opts_default.restype = None
+    L.drwc_ggft_solve.argtypes = [vp, C.c_int, vp, C.c_int, dbl, vp, C.POINTER(i32)]
+    L.drwc_fdm_solve_batch_device.argtypes = [vp, C.c_int, vp, vp, vp, vp,
+                                              C.POINTER(FdmOpts), vp, vp, vp, vp, vp]
+    L.drwc_fdm_solve_batch.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.POINTER(FdmOpts), vp,
+                                       vp, vp, vp, vp]
+    L.drwc_structure_construction.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, vp, vp]
+    L.drwc_transition_batch.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_uint64, C.c_uint64,
+                                        vp]
+    L.drwc_first_hop_batch.argtypes = [vp, C.c_int, C.c_int, vp, vp, vp, C.c_uint64,
+                                       C.c_uint64, vp]
+    L.drwc_job_params_default.argtypes = [C.POINTER(JobParams)]
+    L.drwc_job_params_default.restype = None
+    L.drwc_frw_run.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams),
+                               C.POINTER(JobResult)]
+    L.drwc_frw_walks.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams), i64, i64, vp,
+                                 vp, vp, vp]
+    L.drwc_job_create.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams), C.POINTER(vp)]
+    L.drwc_job_destroy.argtypes = [vp]
+    L.drwc_job_walks_device.argtypes = [vp, i64, i64, vp, vp, vp, vp]
+    L.drwc_job_h2d_bytes.argtypes = [vp, C.POINTER(i64)]
+    _lib = L
+    return L
+
+
+def check(status: int, where: str) -> None:
+    if status != 0:
+        raise DrwcError(status, where)
+
+
+def ptr(a) -> int:
+    """Address of a numpy array or a torch tensor (host or device)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+def default_fdm_opts() -> FdmOpts:
+    o = FdmOpts()
+    load().drwc_fdm_opts_default(C.byref(o))
+    return o
+
+
+def default_job_params() -> JobParams:
+    p = JobParams()
+    load().drwc_job_params_default(C.byref(p))
+    return p

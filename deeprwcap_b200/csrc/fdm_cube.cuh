@@ -1,0 +1,417 @@
+// CTA-resident mixed-precision solve of one transition cube's FDM system.
+//
+// The reference's operator (ggft/src/ggft_solver.cpp:447-518 through
+// update_matrix :276-290) is A = K * diag(1/eps) with K symmetric positive
+// definite:  K_pq = -g_pq, g_pq = eps_p eps_q / (eps_p + eps_q) for face
+// neighbours, K_pp = sum_q g_pq + eps_p * (cube faces touched by p).
+// ggft's `inner` = eps .* y with K y = e, and gft = A13*inner (:594-596)
+// reads eps_c * y_c under each boundary panel. Right-hand sides e restate
+// update_ek (:137-274).
+//
+// One CTA owns one cube; the whole FP32 iteration state stays on chip:
+//   thread t < N^2 owns the z-column (i, j) = (t % N, t / N) and keeps its
+//   N cells of r, x and q = K~p in registers (fully unrolled over k);
+//   shared memory holds the search direction p and the three scaled link
+//   coefficients cx, cy, cz (cell -> +x/+y/+z neighbour), each padded with N
+//   zero guard cells on both ends so the 7-point stencil needs no branches:
+//   a link that leaves the cube has coefficient 0, and the neighbour read at
+//   c-1 / c-N / c+1 / c+N of a boundary cell lands on a guard or on a cell
+//   whose coefficient toward it is 0.
+// The inner solve is Jacobi-scaled CG on K~ = S K S (S = diag(K)^-1/2, so
+// K~_pp = 1) in FP32. Accuracy comes from FP64 iterative refinement: the
+// residual e - K y is evaluated in FP64 from the FP64 permittivity, the FP32
+// solve corrects y (kept in FP64 in global scratch), repeated until
+// ||e - K y|| <= tol ||e||.
+#pragma once
+
+#include "common.cuh"
+
+namespace drwc {
+
+struct FdmParams {
+    double tol;        // FP64 relative residual target
+    float inner_tol;   // relative residual reduction per FP32 sweep
+    int max_outer;     // FP64 refinement sweeps
+    int max_inner;     // FP32 CG iterations per sweep
+};
+
+// Per-cube solve outcome.
+struct FdmStats {
+    int iters;       // FP32 CG iterations (all sweeps)
+    int sweeps;      // FP64 residual evaluations (refinement sweeps + final check)
+    double relres;   // final ||e - K y|| / ||e||
+    int status;      // 0 converged, 1 not converged, 2 invalid permittivity
+};
+
+template <int N>
+struct Cube {
+    static constexpr int NN = N * N;
+    static constexpr int NNN = N * N * N;
+    static constexpr int NT = ((NN + 31) / 32) * 32;  // threads per CTA
+    static constexpr int NW = NT / 32;
+    static constexpr int PAD = N;                      // guard cells per side
+    static constexpr int LEN = NNN + 2 * PAD;
+    // dynamic shared memory: [red: 2*NW+8 doubles][rhs: 8 int + 8 double]
+    //                        [flags: 8 int][p | cx | cy | cz : LEN floats each]
+    static constexpr size_t kRedOff = 0;
+    static constexpr size_t kRhsIdxOff = kRedOff + sizeof(double) * (2 * NW + 8);
+    static constexpr size_t kRhsValOff = kRhsIdxOff + sizeof(int) * kMaxRhs;
+    static constexpr size_t kFlagOff = kRhsValOff + sizeof(double) * kMaxRhs;
+    static constexpr size_t kArrOff = ((kFlagOff + sizeof(int) * 8 + 127) / 128) * 128;
+    static constexpr size_t kArrBytes = ((sizeof(float) * LEN + 15) / 16) * 16;
+    static constexpr size_t kSmemBytes = kArrOff + 4 * kArrBytes;
+    static_assert(kSmemBytes <= 227 * 1024, "cube does not fit in shared memory");
+};
+
+template <int N>
+struct CubeSmem {
+    double* red;     // 2*NW+8 doubles: partial sums / sampling scratch
+    int* rhs_idx;
+    double* rhs_val;
+    int* flags;      // [0] rhs count, [1] invalid-eps flag
+    float* p;        // each points at cell 0 (PAD guard cells before it)
+    float* cx;
+    float* cy;
+    float* cz;
+    DRWC_DEV static CubeSmem carve(unsigned char* base) {
+        using D = Cube<N>;
+        CubeSmem s;
+        s.red = reinterpret_cast<double*>(base + D::kRedOff);
+        s.rhs_idx = reinterpret_cast<int*>(base + D::kRhsIdxOff);
+        s.rhs_val = reinterpret_cast<double*>(base + D::kRhsValOff);
+        s.flags = reinterpret_cast<int*>(base + D::kFlagOff);
+        float* a = reinterpret_cast<float*>(base + D::kArrOff);
+        const size_t stride = D::kArrBytes / sizeof(float);
+        s.p = a + D::PAD;
+        s.cx = a + stride + D::PAD;
+        s.cy = a + 2 * stride + D::PAD;
+        s.cz = a + 3 * stride + D::PAD;
+        return s;
+    }
+    // Raw start of the p|cz region (2 arrays) for staging FP64 input.
+    DRWC_DEV unsigned char* stage() const { return reinterpret_cast<unsigned char*>(p - Cube<N>::PAD); }
+};
+
+// ---------------------------------------------------------------- reductions
+// Block sum of a float (all threads receive the result). `slot` selects one of
+// two partial buffers so back-to-back reductions need only one barrier each.
+template <int NW>
+DRWC_DEV float block_sum_f(float v, double* red, int slot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[slot * NW + warp] = (double)v;
+    __syncthreads();
+    double s = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) s += red[slot * NW + w];
+    return (float)s;
+}
+
+template <int NW>
+DRWC_DEV double block_sum_d(double v, double* red, int slot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) red[slot * NW + warp] = v;
+    __syncthreads();
+    double s = 0;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) s += red[slot * NW + w];
+    return s;
+}
+
+// ------------------------------------------------------------ right-hand side
+// Centre sources of ggft_solver.cpp:137-274 (unit source / centre gradient,
+// h = 2/N). Written by thread 0 into smem as (cell, value) pairs.
+template <int N>
+DRWC_DEV void build_rhs(const double* __restrict__ eps, int code, const CubeSmem<N>& sm) {
+    if (threadIdx.x != 0) return;
+    const double h = 2.0 / N;
+    const int c = N / 2;
+    auto id = [](int i, int j, int k) { return i + j * N + k * N * N; };
+    int n = 0;
+    if (N % 2) {
+        const int zzz = id(c, c, c);
+        if (code == DRWC_GFT) {
+            sm.rhs_idx[0] = zzz; sm.rhs_val[0] = 1.0; n = 1;
+        } else {
+            const int stride = code == DRWC_WVTZ ? N * N : code == DRWC_WVTX ? 1 : N;
+            const int pp = zzz + stride, mm = zzz - stride;
+            const double d_plus = eps[pp] + eps[zzz];
+            const double d_minus = -(eps[zzz] + eps[mm]);
+            sm.rhs_idx[0] = pp;  sm.rhs_val[0] = eps[pp] / d_plus / h;
+            sm.rhs_idx[1] = zzz; sm.rhs_val[1] = eps[zzz] * (1. / d_plus + 1. / d_minus) / h;
+            sm.rhs_idx[2] = mm;  sm.rhs_val[2] = eps[mm] / d_minus / h;
+            n = 3;
+        }
+    } else {
+        const int zzz = id(c, c, c), zmz = id(c, c - 1, c), zzm = id(c, c, c - 1),
+                  zmm = id(c, c - 1, c - 1), mzz = id(c - 1, c, c), mmz = id(c - 1, c - 1, c),
+                  mzm = id(c - 1, c, c - 1), mmm = id(c - 1, c - 1, c - 1);
+        const double dsum = eps[zzz] + eps[zmz] + eps[zzm] + eps[zmm] + eps[mzz] + eps[mmz] +
+                            eps[mzm] + eps[mmm];
+        if (code == DRWC_GFT) {
+            const int cells[8] = {zzz, mzz, zmz, zzm, mmz, mzm, zmm, mmm};
+            for (int t = 0; t < 8; ++t) {
+                sm.rhs_idx[t] = cells[t];
+                sm.rhs_val[t] = eps[cells[t]] / dsum;
+            }
+        } else {
+            int plus[4], minus[4];
+            double d_minus;
+            if (code == DRWC_WVTZ) {
+                plus[0] = zzz; plus[1] = mzz; plus[2] = zmz; plus[3] = mmz;
+                minus[0] = zzm; minus[1] = mzm; minus[2] = zmm; minus[3] = mmm;
+                d_minus = -(eps[zzm] + eps[mzm] + eps[zmm] + eps[mmm]);
+            } else if (code == DRWC_WVTX) {
+                plus[0] = zzz; plus[1] = zmz; plus[2] = zzm; plus[3] = zmm;
+                minus[0] = mzz; minus[1] = mmz; minus[2] = mzm; minus[3] = mmm;
+                d_minus = -(eps[mzz] + eps[mmz] + eps[mzm] + eps[mmm]);
+            } else {
+                plus[0] = zzz; plus[1] = mzz; plus[2] = zzm; plus[3] = mzm;
+                minus[0] = zmz; minus[1] = mmz; minus[2] = zmm; minus[3] = mmm;
+                d_minus = -(eps[zmz] + eps[mmz] + eps[zmm] + eps[mmm]);
+            }
+            for (int t = 0; t < 4; ++t) {
+                sm.rhs_idx[t] = plus[t];
+                sm.rhs_val[t] = eps[plus[t]] / dsum / h * 2;
+                sm.rhs_idx[4 + t] = minus[t];
+                sm.rhs_val[4 + t] = eps[minus[t]] * (1. / dsum + 1. / d_minus) / h * 2;
+            }
+        }
+        n = 8;
+    }
+    sm.flags[0] = n;
+}
+
+template <int N>
+DRWC_DEV double rhs_at(const CubeSmem<N>& sm, int cell) {
+    double v = 0.0;
+    const int n = sm.flags[0];
+    for (int t = 0; t < n; ++t)
+        if (sm.rhs_idx[t] == cell) v = sm.rhs_val[t];
+    return v;
+}
+
+// Permittivity the first-hop weight is scaled by (ggft_solver.cpp:649-671):
+// odd N the centre cell, even N the mean of the four centre cells on the
+// minus side of the gradient axis.
+template <int N>
+DRWC_DEV double center_diel(const double* __restrict__ eps, int code) {
+    const int c = N / 2;
+    auto id = [](int i, int j, int k) { return i + j * N + k * N * N; };
+    if ((N % 2) || code == DRWC_GFT) return eps[id(c, c, c)];
+    if (code == DRWC_WVTZ)
+        return (eps[id(c, c, c - 1)] + eps[id(c - 1, c - 1, c - 1)] + eps[id(c, c - 1, c - 1)] +
+                eps[id(c - 1, c, c - 1)]) / 4;
+    if (code == DRWC_WVTX)
+        return (eps[id(c - 1, c, c)] + eps[id(c - 1, c - 1, c)] + eps[id(c - 1, c, c - 1)] +
+                eps[id(c - 1, c - 1, c - 1)]) / 4;
+    return (eps[id(c, c - 1, c)] + eps[id(c - 1, c - 1, c)] + eps[id(c, c - 1, c - 1)] +
+            eps[id(c - 1, c - 1, c - 1)]) / 4;
+}
+
+// --------------------------------------------------------------- the solver
+// eps:  N^3 FP64 permittivity in global memory (cell i + j*N + k*N*N).
+// ys:   N^3 doubles of global scratch (the FP64 solution y of K y = e).
+// ss:   N^3 floats of global scratch (the Jacobi scale S).
+// On return (all threads) ys holds y and the stats are filled; shared memory
+// p/cx/cy/cz are free for the caller.
+template <int N>
+__device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const double* __restrict__ eps,
+                                        double* __restrict__ ys, float* __restrict__ ss, int code,
+                                        const FdmParams& prm, FdmStats* st) {
+    using D = Cube<N>;
+    constexpr int NN = D::NN;
+    constexpr int NW = D::NW;
+    const int t = threadIdx.x;
+    const bool active = t < NN;
+    const int i = t % N, j = t / N;
+    const int base = active ? t : 0;
+
+    // ---- setup 1: validity, Jacobi scale S = diag(K)^-1/2 (FP32), y = 0,
+    //      guards zeroed, right-hand side.
+    if (t == 0) sm.flags[1] = 0;
+    for (int g = t; g < D::PAD; g += D::NT) {
+        sm.p[-D::PAD + g] = 0.f; sm.p[D::NNN + g] = 0.f;
+        sm.cx[-D::PAD + g] = 0.f; sm.cx[D::NNN + g] = 0.f;
+        sm.cy[-D::PAD + g] = 0.f; sm.cy[D::NNN + g] = 0.f;
+        sm.cz[-D::PAD + g] = 0.f; sm.cz[D::NNN + g] = 0.f;
+    }
+    build_rhs<N>(eps, code, sm);
+    __syncthreads();
+    if (active) {
+        bool bad = false;
+#pragma unroll 1
+        for (int k = 0; k < N; ++k) {
+            const int c = base + k * NN;
+            const double e64 = eps[c];
+            bad |= !(e64 > 0.0) || !isfinite(e64);
+            const float ec = (float)e64;
+            float d = 0.f;
+            d += (i + 1 < N) ? ec * (float)eps[c + 1] / (ec + (float)eps[c + 1]) : ec;
+            d += (i > 0) ? ec * (float)eps[c - 1] / (ec + (float)eps[c - 1]) : ec;
+            d += (j + 1 < N) ? ec * (float)eps[c + N] / (ec + (float)eps[c + N]) : ec;
+            d += (j > 0) ? ec * (float)eps[c - N] / (ec + (float)eps[c - N]) : ec;
+            d += (k + 1 < N) ? ec * (float)eps[c + NN] / (ec + (float)eps[c + NN]) : ec;
+            d += (k > 0) ? ec * (float)eps[c - NN] / (ec + (float)eps[c - NN]) : ec;
+            ss[c] = rsqrtf(d);
+            ys[c] = 0.0;
+        }
+        if (bad) atomicOr(&sm.flags[1], 1);
+    }
+    __syncthreads();
+    if (sm.flags[1]) {
+        st->status = 2; st->iters = 0; st->sweeps = 0; st->relres = CUDART_NAN;
+        return;
+    }
+    // ---- setup 2: scaled link coefficients cx/cy/cz = g * S_p * S_q.
+    if (active) {
+#pragma unroll 1
+        for (int k = 0; k < N; ++k) {
+            const int c = base + k * NN;
+            const float ec = (float)eps[c];
+            const float sc = ss[c];
+            float vx = 0.f, vy = 0.f, vz = 0.f;
+            if (i + 1 < N) { const float eq = (float)eps[c + 1]; vx = ec * eq / (ec + eq) * sc * ss[c + 1]; }
+            if (j + 1 < N) { const float eq = (float)eps[c + N]; vy = ec * eq / (ec + eq) * sc * ss[c + N]; }
+            if (k + 1 < N) { const float eq = (float)eps[c + NN]; vz = ec * eq / (ec + eq) * sc * ss[c + NN]; }
+            sm.cx[c] = vx; sm.cy[c] = vy; sm.cz[c] = vz;
+        }
+    }
+    // ||e|| (FP64) from the rhs table
+    double enorm2 = 0.0;
+    for (int q = 0; q < sm.flags[0]; ++q) enorm2 += sm.rhs_val[q] * sm.rhs_val[q];
+    const double enorm = sqrt(enorm2);
+
+    float r[N], x[N], q[N];
+    int total_inner = 0, outer = 0;
+    double relres = 1.0;
+    int status = 1;
+#pragma unroll 1
+    for (outer = 0; outer <= prm.max_outer; ++outer) {
+        // ---- FP64 residual r64 = e - K y, inner rhs b = S r64 (FP32 regs)
+        __syncthreads();  // ys writes of the previous sweep visible
+        double rn2 = 0.0;
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const int c = base + k * NN;
+                const double ec = eps[c];
+                const double yc = ys[c];
+                double diag = 0.0, off = 0.0;
+                if (i + 1 < N) { const double eq = eps[c + 1]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c + 1]; } else diag += ec;
+                if (i > 0) { const double eq = eps[c - 1]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c - 1]; } else diag += ec;
+                if (j + 1 < N) { const double eq = eps[c + N]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c + N]; } else diag += ec;
+                if (j > 0) { const double eq = eps[c - N]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c - N]; } else diag += ec;
+                if (k + 1 < N) { const double eq = eps[c + NN]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c + NN]; } else diag += ec;
+                if (k > 0) { const double eq = eps[c - NN]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c - NN]; } else diag += ec;
+                const double r64 = rhs_at<N>(sm, c) - (diag * yc - off);
+                rn2 += r64 * r64;
+                r[k] = (float)((double)ss[c] * r64);
+            }
+        }
+        rn2 = block_sum_d<NW>(rn2, sm.red, 0);
+        relres = sqrt(rn2) / enorm;
+        if (relres <= prm.tol) { status = 0; break; }
+        if (outer == prm.max_outer) break;
+
+        // ---- FP32 CG on K~ d = b, d in x[], starting from 0
+        float rr = 0.f;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            x[k] = 0.f;
+            if (active) {
+                sm.p[base + k * NN] = r[k];
+                rr += r[k] * r[k];
+            } else {
+                r[k] = 0.f;
+            }
+        }
+        rr = block_sum_f<NW>(rr, sm.red, 1);  // barrier also publishes p
+        const float stop2 = rr * prm.inner_tol * prm.inner_tol;
+        int it = 0;
+#pragma unroll 1
+        for (it = 0; it < prm.max_inner && rr > stop2; ++it) {
+            // q = K~ p  (K~_pp = 1)
+            float pq = 0.f;
+            if (active) {
+                float pm = 0.f, czm = 0.f;
+                float pc = sm.p[base];
+#pragma unroll
+                for (int k = 0; k < N; ++k) {
+                    const int c = base + k * NN;
+                    const float pn = (k + 1 < N) ? sm.p[c + NN] : 0.f;
+                    const float czc = sm.cz[c];
+                    const float nb = sm.cx[c - 1] * sm.p[c - 1] + sm.cx[c] * sm.p[c + 1] +
+                                     sm.cy[c - N] * sm.p[c - N] + sm.cy[c] * sm.p[c + N] +
+                                     czm * pm + czc * pn;
+                    q[k] = pc - nb;
+                    pq += pc * q[k];
+                    pm = pc; pc = pn; czm = czc;
+                }
+            }
+            pq = block_sum_f<NW>(pq, sm.red, 0);
+            const float alpha = rr / pq;
+            float rr2 = 0.f;
+            if (active) {
+#pragma unroll
+                for (int k = 0; k < N; ++k) {
+                    const int c = base + k * NN;
+                    x[k] += alpha * sm.p[c];
+                    r[k] -= alpha * q[k];
+                    rr2 += r[k] * r[k];
+                }
+            }
+            rr2 = block_sum_f<NW>(rr2, sm.red, 1);
+            const float beta = rr2 / rr;
+            rr = rr2;
+            if (active) {
+#pragma unroll
+                for (int k = 0; k < N; ++k) {
+                    const int c = base + k * NN;
+                    sm.p[c] = r[k] + beta * sm.p[c];
+                }
+            }
+            __syncthreads();
+        }
+        total_inner += it;
+        // ---- y += S d
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const int c = base + k * NN;
+                ys[c] += (double)ss[c] * (double)x[k];
+            }
+        }
+    }
+    st->status = status;
+    st->iters = total_inner;
+    st->sweeps = outer + 1;
+    st->relres = relres;
+    __syncthreads();
+}
+
+// Surface values gft[b] = eps_c * y_c under panel b (ggft panel order,
+// ggft_solver.h:65-77). Cooperative over the CTA; writes through `put(b, v)`.
+template <int N, class Put>
+DRWC_DEV void for_each_panel(const double* __restrict__ eps, const double* __restrict__ ys, Put put) {
+    constexpr int NN = N * N;
+    for (int b = threadIdx.x; b < 6 * NN; b += blockDim.x) {
+        const int f = b / NN, tt = b % NN;
+        const int a = tt % N, bb = tt / N;
+        int c;
+        switch (f) {
+            case 0: c = a + bb * N; break;                        // z-: (i,j,0)
+            case 1: c = a + bb * N + (N - 1) * NN; break;         // z+
+            case 2: c = a + bb * NN; break;                       // y-: (i,0,k)
+            case 3: c = a + (N - 1) * N + bb * NN; break;         // y+
+            case 4: c = a * N + bb * NN; break;                   // x-: (0,j,k)
+            default: c = (N - 1) + a * N + bb * NN; break;        // x+
+        }
+        put(b, eps[c] * ys[c]);
+    }
+}
+
+}  // namespace drwc

@@ -1,0 +1,874 @@
+// Device-resident floating-random-walk capacitance extraction (the role of
+// the reference's closed walker, executable/librwcapall.so) with every hop's
+// transition kernel from the on-chip FDM solve.
+//
+// Walk w (job seed s): Philox4x32-10 key s, counter (w, hop, draw, 0).
+//   hop 0: a point on the Gaussian surface (the master's bounding box grown
+//          by gauss_offset) chosen by area, the largest conductor-free cube
+//          around it, the centre-gradient surface values along the face
+//          normal (WVTX/Y/Z), a panel drawn with probability |g_b| / sum|g|
+//          and the walk weight
+//             w = -s_out * A_gauss * eps_w * sum|g| * sign(g_b) / a0 * eps0
+//          (dnn_solver_gradient.cpp:143-162 gives sum|g| * sign and the
+//          centre permittivity; the area, the half-width a0 and the outward
+//          sign s_out turn the normalised gradient into charge);
+//   hop h: the largest conductor-free cube around the walker, its surface
+//          Green's function (GFT), a panel drawn with probability G_b;
+//   end:   when the L-infinity distance to the nearest conductor or
+//          enclosure wall is below stop_dist; the walk adds w to the entry
+//          of the net it ends on.
+// One CTA carries one walk at a time from start to end (persistent grid,
+// walks claimed with an atomic counter) and writes its record; capacitance
+// sums are reduced afterwards in a fixed order, so results do not depend on
+// scheduling. Geometry uses explicitly rounded FP64 operations so the walk
+// visits exactly the points a non-contracted CPU evaluation visits.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
+#include "fdm_cube.cuh"
+#include "host.cuh"
+#include "sample.cuh"
+
+namespace drwc {
+
+FdmParams make_params(const drwc_fdm_opts* o, int N);
+
+constexpr double kEps0FfPerUm = 8.8541878128e-3;  // vacuum permittivity, fF/um
+constexpr int kBruteBoxes = 16;                  // <= this many boxes: scan all
+
+struct DevGeom {
+    int n_boxes, n_nets, n_layers, n_diel;
+    const double* box;      // n_boxes x 6 (lo xyz, hi xyz)
+    const int* net;         // n_boxes
+    const double* zlo;      // n_layers
+    const double* leps;     // n_layers
+    const double* diel;     // n_diel x 7
+    double encl_lo[3], encl_hi[3];
+    // uniform grid over the enclosure (CSR cell -> boxes)
+    int gdim[3];
+    double gcell[3];
+    double gmin_cell;
+    const int* gstart;      // ncells + 1
+    const int* gitems;
+};
+
+struct Gauss {
+    double lo[3], hi[3], area[6], total;
+};
+
+struct WalkParams {
+    int N, max_hops, master;
+    double stop;
+    uint64_t seed;
+    FdmParams prm;
+};
+
+// ------------------------------------------------------------------ geometry
+DRWC_DEV double box_dist(const double* b, const double r[3]) {
+    double d = 0.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double lo = dsub(b[a], r[a]);
+        const double hi = dsub(r[a], b[3 + a]);
+        const double m = lo > hi ? lo : hi;
+        if (m > d) d = m;
+    }
+    return d;
+}
+
+DRWC_DEV double encl_dist(const DevGeom& g, const double r[3]) {
+    double best = CUDART_INF;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double d1 = dsub(r[a], g.encl_lo[a]);
+        const double d2 = dsub(g.encl_hi[a], r[a]);
+        if (d1 < best) best = d1;
+        if (d2 < best) best = d2;
+    }
+    return best;
+}
+
+// Nearest conductor (L-infinity) for warp 0: the enclosure wins ties, then
+// the lowest box index. Result in lane 0 (and broadcast to the warp).
+DRWC_DEV void nearest(const DevGeom& g, const double r[3], double* d_out, int* net_out) {
+    const int lane = threadIdx.x & 31;
+    double best = CUDART_INF;
+    int bidx = 0x7fffffff;
+    if (g.n_boxes <= kBruteBoxes || g.gstart == nullptr) {
+        for (int b = lane; b < g.n_boxes; b += 32) {
+            const double d = box_dist(g.box + 6 * b, r);
+            if (d < best || (d == best && b < bidx)) { best = d; bidx = b; }
+        }
+    } else if (lane == 0) {
+        int ci[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            int v = (int)floor((r[a] - g.encl_lo[a]) / g.gcell[a]);
+            ci[a] = v < 0 ? 0 : (v >= g.gdim[a] ? g.gdim[a] - 1 : v);
+        }
+        const double dwall = encl_dist(g, r);
+        const int rmax = max(g.gdim[0], max(g.gdim[1], g.gdim[2]));
+        for (int ring = 0; ring <= rmax; ++ring) {
+            // boxes not met in rings < ring lie at least (ring-1) cells away
+            const double reach = (double)(ring - 1) * g.gmin_cell * (1.0 - 1e-12);
+            if (ring > 1 && (best < reach || dwall < reach)) break;
+            for (int z = ci[2] - ring; z <= ci[2] + ring; ++z) {
+                if (z < 0 || z >= g.gdim[2]) continue;
+                for (int y = ci[1] - ring; y <= ci[1] + ring; ++y) {
+                    if (y < 0 || y >= g.gdim[1]) continue;
+                    for (int x = ci[0] - ring; x <= ci[0] + ring; ++x) {
+                        if (x < 0 || x >= g.gdim[0]) continue;
+                        const int cheb = max(abs(x - ci[0]), max(abs(y - ci[1]), abs(z - ci[2])));
+                        if (cheb != ring) continue;
+                        const int cell = x + g.gdim[0] * (y + g.gdim[1] * z);
+                        for (int it = g.gstart[cell]; it < g.gstart[cell + 1]; ++it) {
+                            const int b = g.gitems[it];
+                            const double d = box_dist(g.box + 6 * b, r);
+                            if (d < best || (d == best && b < bidx)) { best = d; bidx = b; }
+                        }
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+        if (ob < best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
+    }
+    const double dw = encl_dist(g, r);
+    if (dw <= best) {
+        *d_out = dw;
+        *net_out = g.n_nets;
+    } else {
+        *d_out = best;
+        *net_out = g.net[bidx];
+    }
+}
+
+DRWC_DEV double eps_at(const DevGeom& g, const double p[3]) {
+    for (int b = 0; b < g.n_diel; ++b) {
+        const double* D = g.diel + 7 * b;
+        if (p[0] >= D[0] && p[0] <= D[3] && p[1] >= D[1] && p[1] <= D[4] && p[2] >= D[2] &&
+            p[2] <= D[5])
+            return D[6];
+    }
+    if (g.n_layers <= 0) return 1.0;
+    int li = 0;
+    for (int l = 0; l < g.n_layers; ++l) {
+        if (p[2] >= g.zlo[l]) li = l;
+        else break;
+    }
+    return g.leps[li];
+}
+
+template <int N>
+DRWC_DEV void voxelise(const DevGeom& g, const double c[3], double a, double* es) {
+    for (int v = threadIdx.x; v < N * N * N; v += blockDim.x) {
+        const int i = v % N, j = (v / N) % N, k = v / (N * N);
+        double p[3];
+        p[0] = dadd(c[0], dmul(a, dsub(ddiv(dadd(dmul(2.0, (double)i), 1.0), (double)N), 1.0)));
+        p[1] = dadd(c[1], dmul(a, dsub(ddiv(dadd(dmul(2.0, (double)j), 1.0), (double)N), 1.0)));
+        p[2] = dadd(c[2], dmul(a, dsub(ddiv(dadd(dmul(2.0, (double)k), 1.0), (double)N), 1.0)));
+        es[v] = eps_at(g, p);
+    }
+}
+
+struct WalkState {
+    double r[3];
+    double a;
+    double omega;
+    int net;
+    int hops;
+    int code;
+    int done;
+    long long walk;
+    double sgn_out;
+};
+
+template <int N>
+__global__ void __launch_bounds__(Cube<N>::NT)
+walk_kernel(DevGeom g, Gauss G, WalkParams P, long long walk0, long long nwalks,
+            unsigned long long* __restrict__ next, unsigned long long* __restrict__ stats,
+            int32_t* __restrict__ end_out,
+            int32_t* __restrict__ hops_out, double* __restrict__ w_out,
+            double* __restrict__ scratch_e, double* __restrict__ scratch_y,
+            float* __restrict__ scratch_s) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ WalkState S;
+    using D = Cube<N>;
+    constexpr int M = 6 * D::NN;
+    const CubeSmem<N> sm = CubeSmem<N>::carve(smem);
+    double* es = scratch_e + (size_t)blockIdx.x * D::NNN;
+    double* ys = scratch_y + (size_t)blockIdx.x * D::NNN;
+    float* ss = scratch_s + (size_t)blockIdx.x * D::NNN;
+    const int t = threadIdx.x;
+    unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0;
+    for (;;) {
+        if (t == 0) S.walk = (long long)atomicAdd(next, 1ull);
+        __syncthreads();
+        const long long idx = S.walk;
+        if (idx >= nwalks) break;
+        const uint64_t w = (uint64_t)(walk0 + idx);
+        // ---- start point on the Gaussian surface
+        if (t == 0) {
+            const double2 u = philox_uniform2(P.seed, w, 0, 0);
+            const double2 v = philox_uniform2(P.seed, w, 0, 1);
+            const double target = dmul(u.x, G.total);
+            double run = 0.0;
+            int f = 5;
+            for (int q = 0; q < 6; ++q) {
+                run = dadd(run, G.area[q]);
+                if (run > target) { f = q; break; }
+            }
+            const int axis = f < 2 ? 2 : f < 4 ? 1 : 0;
+            const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
+            S.r[t0] = dadd(G.lo[t0], dmul(u.y, dsub(G.hi[t0], G.lo[t0])));
+            S.r[t1] = dadd(G.lo[t1], dmul(v.x, dsub(G.hi[t1], G.lo[t1])));
+            S.r[axis] = (f & 1) ? G.hi[axis] : G.lo[axis];
+            S.sgn_out = (f & 1) ? 1.0 : -1.0;
+            S.code = axis == 0 ? DRWC_WVTX : axis == 1 ? DRWC_WVTY : DRWC_WVTZ;
+            S.hops = 0;
+            S.done = 0;
+            S.omega = 0.0;
+        }
+        __syncthreads();
+        for (;;) {
+            // ---- distance to the nearest conductor: cube size / absorption
+            if (t < 32) {
+                double d;
+                int net;
+                double r[3] = {S.r[0], S.r[1], S.r[2]};
+                nearest(g, r, &d, &net);
+                if (t == 0) {
+                    S.a = d;
+                    S.net = net;
+                    if (d < P.stop) S.done = 1;
+                    else if (S.hops >= P.max_hops) { S.done = 1; S.net = -1; }
+                }
+            }
+            __syncthreads();
+            if (S.done) break;
+            const double c[3] = {S.r[0], S.r[1], S.r[2]};
+            const double a = S.a;
+            const bool first = S.hops == 0;
+            const int code = first ? S.code : DRWC_GFT;
+            voxelise<N>(g, c, a, es);
+            __syncthreads();
+            FdmStats st;
+            cube_solve<N>(sm, es, ys, ss, code, P.prm, &st);
+            double* wv = reinterpret_cast<double*>(sm.stage());
+            for_each_panel<N>(es, ys, [&](int b, double v) { wv[b] = v; });
+            __syncthreads();
+            const double2 u = first ? philox_uniform2(P.seed, w, 0, 1)
+                                    : philox_uniform2(P.seed, w, (uint32_t)S.hops, 0);
+            const double ud = first ? u.y : u.x;
+            double tot = 0.0;
+            const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
+            if (t == 0) {
+                my_hops += 1;
+                my_iters += (unsigned long long)st.iters;
+                my_sweeps += (unsigned long long)st.sweeps;
+                if (b < 0 || st.status == 2) {
+                    S.net = -1;  // no transition possible: count as lost
+                    S.done = 2;
+                } else {
+                    if (first) {
+                        const double sg = wv[b] < 0.0 ? -1.0 : 1.0;
+                        const double eps_w = center_diel<N>(es, code);
+                        double om = dmul(-S.sgn_out, G.total);
+                        om = dmul(om, eps_w);
+                        om = dmul(om, tot);
+                        om = dmul(om, sg);
+                        om = ddiv(om, a);
+                        S.omega = dmul(om, kEps0FfPerUm);
+                    }
+                    double loc[3];
+                    locate_f64(N, b, loc);
+                    for (int d = 0; d < 3; ++d) S.r[d] = dadd(S.r[d], dmul(a, loc[d]));
+                    S.hops += 1;
+                }
+            }
+            __syncthreads();
+            if (S.done) break;
+        }
+        if (t == 0) {
+            end_out[idx] = S.net;
+            hops_out[idx] = S.hops;
+            w_out[idx] = S.omega;
+        }
+        __syncthreads();
+    }
+    if (t == 0 && stats) {
+        atomicAdd(stats + 0, my_hops);
+        atomicAdd(stats + 1, my_iters);
+        atomicAdd(stats + 2, my_sweeps);
+    }
+}
+
+// Per-entry sums of one batch of walk records, fixed order: block e sums
+// entry e (0..n_nets = ground) over all walks; lost walks (net -1) go to the
+// last slot. out[e] = {sum w, sum w^2, count}.
+__global__ void reduce_kernel(int n_entries, long long nw, const int32_t* __restrict__ end,
+                              const double* __restrict__ w,
+                              double* __restrict__ out) {
+    const int e = blockIdx.x;  // 0..n_entries (n_entries = lost + hops slot)
+    double s = 0, s2 = 0, cnt = 0;
+    for (long long i = threadIdx.x; i < nw; i += blockDim.x) {
+        const int ne = end[i] < 0 ? n_entries : end[i];
+        if (ne == e) {
+            const double v = w[i];
+            s += v; s2 += v * v; cnt += 1.0;
+        }
+    }
+    __shared__ double r0[256], r1[256], r2[256];
+    r0[threadIdx.x] = s; r1[threadIdx.x] = s2; r2[threadIdx.x] = cnt;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) {
+            r0[threadIdx.x] += r0[threadIdx.x + o];
+            r1[threadIdx.x] += r1[threadIdx.x + o];
+            r2[threadIdx.x] += r2[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        out[3 * e + 0] = r0[0];
+        out[3 * e + 1] = r1[0];
+        out[3 * e + 2] = r2[0];
+    }
+}
+
+__global__ void hop_sum_kernel(long long nw, const int32_t* __restrict__ hops,
+                               unsigned long long* __restrict__ out) {
+    unsigned long long s = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nw;
+         i += (long long)gridDim.x * blockDim.x)
+        s += (unsigned long long)hops[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+// ------------------------------------------------------------------ host side
+struct HostGeom {
+    std::vector<double> box, zlo, leps, diel;
+    std::vector<int> net, gstart, gitems;
+    DevGeom dev{};
+    void* dbuf = nullptr;
+};
+
+static int validate(const drwc_structure* s) {
+    if (!s || s->n_boxes < 1 || s->n_nets < 1 || s->n_nets > DRWC_MAX_NETS || !s->boxes)
+        return DRWC_ERR_INVALID;
+    if (s->n_layers < 0 || s->n_diel < 0) return DRWC_ERR_INVALID;
+    if (s->n_layers > 0 && (!s->layer_zlo || !s->layer_eps)) return DRWC_ERR_INVALID;
+    if (s->n_diel > 0 && !s->diel) return DRWC_ERR_INVALID;
+    for (int a = 0; a < 3; ++a)
+        if (!(s->encl_hi[a] > s->encl_lo[a])) return DRWC_ERR_GEOMETRY;
+    for (int b = 0; b < s->n_boxes; ++b) {
+        const drwc_box& B = s->boxes[b];
+        if (B.net < 0 || B.net >= s->n_nets) return DRWC_ERR_INVALID;
+        for (int a = 0; a < 3; ++a)
+            if (!(B.hi[a] > B.lo[a]) || B.lo[a] < s->encl_lo[a] || B.hi[a] > s->encl_hi[a])
+                return DRWC_ERR_GEOMETRY;
+    }
+    for (int l = 0; l < s->n_layers; ++l) {
+        if (!(s->layer_eps[l] > 0)) return DRWC_ERR_INVALID;
+        if (l > 0 && !(s->layer_zlo[l] >= s->layer_zlo[l - 1])) return DRWC_ERR_INVALID;
+    }
+    for (int d = 0; d < s->n_diel; ++d)
+        if (!(s->diel[d].eps > 0)) return DRWC_ERR_INVALID;
+    return DRWC_OK;
+}
+
+static int upload_geom(drwc_ctx* ctx, const drwc_structure* s, HostGeom* h) {
+    const int nb = s->n_boxes;
+    h->box.resize(6 * nb);
+    h->net.resize(nb);
+    for (int b = 0; b < nb; ++b) {
+        for (int a = 0; a < 3; ++a) {
+            h->box[6 * b + a] = s->boxes[b].lo[a];
+            h->box[6 * b + 3 + a] = s->boxes[b].hi[a];
+        }
+        h->net[b] = s->boxes[b].net;
+    }
+    h->zlo.assign(s->layer_zlo, s->layer_zlo + s->n_layers);
+    h->leps.assign(s->layer_eps, s->layer_eps + s->n_layers);
+    h->diel.resize(7 * s->n_diel);
+    for (int d = 0; d < s->n_diel; ++d) {
+        for (int a = 0; a < 3; ++a) {
+            h->diel[7 * d + a] = s->diel[d].lo[a];
+            h->diel[7 * d + 3 + a] = s->diel[d].hi[a];
+        }
+        h->diel[7 * d + 6] = s->diel[d].eps;
+    }
+    // uniform grid: about 4 cells per box, at most 128 per axis
+    double ext[3], vol = 1.0;
+    for (int a = 0; a < 3; ++a) {
+        ext[a] = s->encl_hi[a] - s->encl_lo[a];
+        vol *= ext[a];
+    }
+    const double hcell = std::cbrt(vol / (4.0 * nb));
+    int dim[3];
+    double cell[3], minc = 1e300;
+    for (int a = 0; a < 3; ++a) {
+        dim[a] = (int)std::min(128.0, std::max(1.0, std::ceil(ext[a] / hcell)));
+        cell[a] = ext[a] / dim[a];
+        minc = std::min(minc, cell[a]);
+    }
+    const int ncell = dim[0] * dim[1] * dim[2];
+    std::vector<std::vector<int>> lists(ncell);
+    for (int b = 0; b < nb; ++b) {
+        int lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = (int)std::floor((s->boxes[b].lo[a] - s->encl_lo[a]) / cell[a]) - 1;
+            hi[a] = (int)std::floor((s->boxes[b].hi[a] - s->encl_lo[a]) / cell[a]) + 1;
+            lo[a] = std::max(0, lo[a]);
+            hi[a] = std::min(dim[a] - 1, hi[a]);
+        }
+        for (int z = lo[2]; z <= hi[2]; ++z)
+            for (int y = lo[1]; y <= hi[1]; ++y)
+                for (int x = lo[0]; x <= hi[0]; ++x) {
+                    // keep the box in every cell its (slightly grown) extent touches
+                    const double cx0 = s->encl_lo[0] + x * cell[0], cx1 = cx0 + cell[0];
+                    const double cy0 = s->encl_lo[1] + y * cell[1], cy1 = cy0 + cell[1];
+                    const double cz0 = s->encl_lo[2] + z * cell[2], cz1 = cz0 + cell[2];
+                    const double tol = 1e-9 * minc;
+                    if (s->boxes[b].lo[0] <= cx1 + tol && s->boxes[b].hi[0] >= cx0 - tol &&
+                        s->boxes[b].lo[1] <= cy1 + tol && s->boxes[b].hi[1] >= cy0 - tol &&
+                        s->boxes[b].lo[2] <= cz1 + tol && s->boxes[b].hi[2] >= cz0 - tol)
+                        lists[x + dim[0] * (y + dim[1] * z)].push_back(b);
+                }
+    }
+    h->gstart.assign(ncell + 1, 0);
+    for (int c = 0; c < ncell; ++c) h->gstart[c + 1] = h->gstart[c] + (int)lists[c].size();
+    h->gitems.clear();
+    for (int c = 0; c < ncell; ++c) h->gitems.insert(h->gitems.end(), lists[c].begin(), lists[c].end());
+    if (h->gitems.empty()) h->gitems.push_back(0);
+
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    const size_t o_box = take(h->box.size() * 8), o_net = take(h->net.size() * 4),
+                 o_zlo = take(std::max<size_t>(1, h->zlo.size()) * 8),
+                 o_leps = take(std::max<size_t>(1, h->leps.size()) * 8),
+                 o_diel = take(std::max<size_t>(1, h->diel.size()) * 8),
+                 o_gs = take(h->gstart.size() * 4), o_gi = take(h->gitems.size() * 4);
+    void* d = nullptr;
+    int rc = ws_get(ctx, WS_AUX2, off, &d);
+    if (rc) return rc;
+    std::vector<unsigned char> hb(off, 0);
+    std::memcpy(hb.data() + o_box, h->box.data(), h->box.size() * 8);
+    std::memcpy(hb.data() + o_net, h->net.data(), h->net.size() * 4);
+    if (!h->zlo.empty()) std::memcpy(hb.data() + o_zlo, h->zlo.data(), h->zlo.size() * 8);
+    if (!h->leps.empty()) std::memcpy(hb.data() + o_leps, h->leps.data(), h->leps.size() * 8);
+    if (!h->diel.empty()) std::memcpy(hb.data() + o_diel, h->diel.data(), h->diel.size() * 8);
+    std::memcpy(hb.data() + o_gs, h->gstart.data(), h->gstart.size() * 4);
+    std::memcpy(hb.data() + o_gi, h->gitems.data(), h->gitems.size() * 4);
+    DRWC_CUDA_TRY(cudaMemcpyAsync(d, hb.data(), off, cudaMemcpyHostToDevice, ctx->stream));
+    unsigned char* base = (unsigned char*)d;
+    DevGeom& g = h->dev;
+    g.n_boxes = nb;
+    g.n_nets = s->n_nets;
+    g.n_layers = s->n_layers;
+    g.n_diel = s->n_diel;
+    g.box = (const double*)(base + o_box);
+    g.net = (const int*)(base + o_net);
+    g.zlo = (const double*)(base + o_zlo);
+    g.leps = (const double*)(base + o_leps);
+    g.diel = (const double*)(base + o_diel);
+    for (int a = 0; a < 3; ++a) {
+        g.encl_lo[a] = s->encl_lo[a];
+        g.encl_hi[a] = s->encl_hi[a];
+        g.gdim[a] = dim[a];
+        g.gcell[a] = cell[a];
+    }
+    g.gmin_cell = minc;
+    g.gstart = (const int*)(base + o_gs);
+    g.gitems = (const int*)(base + o_gi);
+    h->dbuf = d;
+    return DRWC_OK;
+}
+
+// Same arithmetic (order, no contraction) as the CPU restatement.
+static int gauss_build(const drwc_structure* s, const drwc_job_params* p, Gauss* G) {
+    for (int a = 0; a < 3; ++a) {
+        G->lo[a] = INFINITY;
+        G->hi[a] = -INFINITY;
+    }
+    bool any = false;
+    for (int b = 0; b < s->n_boxes; ++b) {
+        if (s->boxes[b].net != p->master) continue;
+        any = true;
+        for (int a = 0; a < 3; ++a) {
+            if (s->boxes[b].lo[a] < G->lo[a]) G->lo[a] = s->boxes[b].lo[a];
+            if (s->boxes[b].hi[a] > G->hi[a]) G->hi[a] = s->boxes[b].hi[a];
+        }
+    }
+    if (!any) return DRWC_ERR_INVALID;
+    for (int a = 0; a < 3; ++a) {
+        volatile double lo = G->lo[a] - p->gauss_offset;
+        volatile double hi = G->hi[a] + p->gauss_offset;
+        G->lo[a] = lo;
+        G->hi[a] = hi;
+        if (lo < s->encl_lo[a] || hi > s->encl_hi[a]) return DRWC_ERR_GEOMETRY;
+    }
+    // the Gaussian surface must not cut another net's box
+    for (int b = 0; b < s->n_boxes; ++b) {
+        if (s->boxes[b].net == p->master) continue;
+        bool overlap = true;
+        for (int a = 0; a < 3; ++a)
+            overlap &= s->boxes[b].lo[a] < G->hi[a] && s->boxes[b].hi[a] > G->lo[a];
+        if (overlap) return DRWC_ERR_GEOMETRY;
+    }
+    volatile double dx = G->hi[0] - G->lo[0], dy = G->hi[1] - G->lo[1], dz = G->hi[2] - G->lo[2];
+    volatile double az = dx * dy, ay = dx * dz, ax = dy * dz;
+    G->area[0] = az; G->area[1] = az;
+    G->area[2] = ay; G->area[3] = ay;
+    G->area[4] = ax; G->area[5] = ax;
+    volatile double tot = 0;
+    for (int f = 0; f < 6; ++f) tot = tot + G->area[f];
+    G->total = tot;
+    return DRWC_OK;
+}
+
+struct WalkShape { int per_sm = 0; };
+
+template <int N>
+static int walk_shape(WalkShape* s) {
+    static WalkShape cached;
+    if (!cached.per_sm) {
+        using D = Cube<N>;
+        DRWC_CUDA_TRY(cudaFuncSetAttribute(walk_kernel<N>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)D::kSmemBytes));
+        int nb = 0;
+        DRWC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<N>, D::NT,
+                                                                    D::kSmemBytes));
+        cached.per_sm = nb < 1 ? 1 : nb;
+    }
+    *s = cached;
+    return DRWC_OK;
+}
+
+// Device buffers for one batch of walk records.
+struct WalkBuffers {
+    int32_t* end;
+    int32_t* hops;
+    double* w;
+    unsigned long long* counter;  // [0] claim counter, [1] hop sum, [2..4] solver stats
+    double* sums;                 // 3 * (n_entries + 1)
+};
+
+static int launch_walks(drwc_ctx* ctx, const HostGeom& hg, const Gauss& G, const WalkParams& P,
+                        long long walk0, long long nw, WalkBuffers& wb) {
+    return dispatch_N(P.N, [&](auto nc) -> int {
+        constexpr int NC = decltype(nc)::value;
+        using D = Cube<NC>;
+        WalkShape sh;
+        int rc = walk_shape<NC>(&sh);
+        if (rc) return rc;
+        const int grid = (int)std::min<long long>(nw, (long long)sh.per_sm * ctx->sm_count);
+        void* scratch = nullptr;
+        rc = ws_get(ctx, WS_SCRATCH, (size_t)grid * D::NNN * 20, &scratch);
+        if (rc) return rc;
+        double* se = (double*)scratch;
+        double* sy = se + (size_t)grid * D::NNN;
+        float* sf = (float*)(sy + (size_t)grid * D::NNN);
+        DRWC_CUDA_TRY(cudaMemsetAsync(wb.counter, 0, 8 * sizeof(unsigned long long), ctx->stream));
+        walk_kernel<NC><<<grid, D::NT, D::kSmemBytes, ctx->stream>>>(
+            hg.dev, G, P, walk0, nw, wb.counter, wb.counter + 2, wb.end, wb.hops, wb.w, se, sy, sf);
+        return launch_check(ctx);
+    });
+}
+
+static int prepare(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
+                   HostGeom* hg, Gauss* G, WalkParams* P) {
+    int rc = validate(s);
+    if (rc) return rc;
+    if (!p || !n_supported(p->N) || p->master < 0 || p->master >= s->n_nets ||
+        !(p->gauss_offset > 0) || !(p->stop_dist > 0) || p->max_hops < 1)
+        return DRWC_ERR_INVALID;
+    rc = gauss_build(s, p, G);
+    if (rc) return rc;
+    rc = upload_geom(ctx, s, hg);
+    if (rc) return rc;
+    P->N = p->N;
+    P->max_hops = p->max_hops;
+    P->master = p->master;
+    P->stop = p->stop_dist;
+    P->seed = p->seed;
+    P->prm = make_params(&p->fdm, p->N);
+    return DRWC_OK;
+}
+
+static int walk_buffers(drwc_ctx* ctx, long long nw, int n_entries, WalkBuffers* wb) {
+    const size_t bytes = nw * (4 + 4 + 8) + 64 + 8 * 3 * (n_entries + 2) + 1024;
+    void* d = nullptr;
+    int rc = ws_get(ctx, WS_RES, bytes, &d);
+    if (rc) return rc;
+    unsigned char* b = (unsigned char*)d;
+    wb->w = (double*)b;
+    wb->sums = (double*)(b + nw * 8);
+    wb->counter = (unsigned long long*)(wb->sums + 3 * (n_entries + 2));
+    wb->end = (int32_t*)(wb->counter + 8);
+    wb->hops = wb->end + nw;
+    return DRWC_OK;
+}
+
+}  // namespace drwc
+
+using namespace drwc;
+
+extern "C" {
+
+DRWC_API void drwc_job_params_default(drwc_job_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->master = 0;
+    p->N = 16;
+    p->gauss_offset = 0.05;
+    p->stop_dist = 1e-5;
+    p->p_tol = 0.01;
+    p->c_tol = 0.01;
+    p->c_ratio = 0.95;
+    p->min_walks = 4096;
+    p->max_walks = 1LL << 26;
+    p->batch_walks = 1LL << 16;
+    p->max_hops = 10000;
+    p->seed = 1;
+    drwc_fdm_opts_default(&p->fdm);
+}
+
+}  // extern "C"
+
+// A prepared job: validated structure uploaded once, walk buffers reusable.
+struct drwc_job {
+    drwc_ctx* ctx;
+    HostGeom hg;
+    Gauss G;
+    WalkParams P;
+    int n_entries;
+    int64_t h2d_bytes;
+};
+
+extern "C" {
+
+DRWC_API int drwc_job_create(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
+                             drwc_job** out) {
+    if (!ctx || !out) return DRWC_ERR_INVALID;
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DRWC_CUDA_TRY(cudaSetDevice(ctx->device));
+    drwc_job* j = new drwc_job();
+    j->ctx = ctx;
+    int rc = prepare(ctx, s, p, &j->hg, &j->G, &j->P);
+    if (rc) { delete j; return rc; }
+    // the job owns its geometry copy (the context workspace is shared)
+    const size_t bytes = ctx->ws_bytes[WS_AUX2];
+    void* own = nullptr;
+    if (cudaMalloc(&own, bytes) != cudaSuccess) { cudaGetLastError(); delete j; return DRWC_ERR_NOMEM; }
+    DRWC_CUDA_TRY(cudaMemcpyAsync(own, j->hg.dbuf, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    const ptrdiff_t shift = (unsigned char*)own - (unsigned char*)j->hg.dbuf;
+    DevGeom& g = j->hg.dev;
+    auto mv = [&](auto*& ptr) { ptr = (std::remove_reference_t<decltype(ptr)>)((const unsigned char*)ptr + shift); };
+    mv(g.box); mv(g.net); mv(g.zlo); mv(g.leps); mv(g.diel); mv(g.gstart); mv(g.gitems);
+    j->hg.dbuf = own;
+    j->n_entries = s->n_nets + 1;
+    j->h2d_bytes = (int64_t)(j->hg.box.size() * 8 + j->hg.net.size() * 4 + j->hg.zlo.size() * 8 +
+                             j->hg.leps.size() * 8 + j->hg.diel.size() * 8 +
+                             j->hg.gstart.size() * 4 + j->hg.gitems.size() * 4);
+    DRWC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    *out = j;
+    return DRWC_OK;
+}
+
+DRWC_API int drwc_job_destroy(drwc_job* j) {
+    if (!j) return DRWC_ERR_INVALID;
+    std::lock_guard<std::mutex> lock(j->ctx->mu);
+    cudaSetDevice(j->ctx->device);
+    cudaStreamSynchronize(j->ctx->stream);
+    if (j->hg.dbuf) cudaFree(j->hg.dbuf);
+    delete j;
+    return DRWC_OK;
+}
+
+DRWC_API int drwc_job_walks_device(drwc_job* j, int64_t walk0, int64_t nwalks, int32_t* end_net,
+                                   int32_t* hops, double* weight, int64_t* solver_stats) {
+    if (!j || walk0 < 0 || nwalks < 0) return DRWC_ERR_INVALID;
+    if (nwalks == 0) return DRWC_OK;
+    if (!end_net || !hops || !weight) return DRWC_ERR_INVALID;
+    drwc_ctx* ctx = j->ctx;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DRWC_CUDA_TRY(cudaSetDevice(ctx->device));
+    WalkBuffers wb;
+    void* d = nullptr;
+    int rc = ws_get(ctx, WS_AUX, 64 * sizeof(unsigned long long), &d);
+    if (rc) return rc;
+    wb.counter = (unsigned long long*)d;
+    wb.end = end_net;
+    wb.hops = hops;
+    wb.w = weight;
+    wb.sums = nullptr;
+    rc = launch_walks(ctx, j->hg, j->G, j->P, walk0, nwalks, wb);
+    if (rc) return rc;
+    if (solver_stats) {
+        // stats are (hops, FP32 iterations, FP64 sweeps) as unsigned 64-bit
+        DRWC_CUDA_TRY(cudaMemcpyAsync(solver_stats, wb.counter + 2, 3 * sizeof(int64_t),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return DRWC_OK;
+}
+
+DRWC_API int drwc_job_h2d_bytes(drwc_job* j, int64_t* bytes) {
+    if (!j || !bytes) return DRWC_ERR_INVALID;
+    *bytes = j->h2d_bytes;
+    return DRWC_OK;
+}
+
+DRWC_API int drwc_frw_walks(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
+                            int64_t walk0, int64_t nwalks, int32_t* end_net, int32_t* hops,
+                            double* weight, int64_t* solver_stats) {
+    if (!ctx || walk0 < 0 || nwalks < 0) return DRWC_ERR_INVALID;
+    if (nwalks == 0) return DRWC_OK;
+    if (!end_net || !hops || !weight) return DRWC_ERR_INVALID;
+    drwc_job* j = nullptr;
+    int rc = drwc_job_create(ctx, s, p, &j);
+    if (rc) return rc;
+    void* d = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        rc = ws_get(ctx, WS_RES, (size_t)nwalks * 16 + 64, &d);
+    }
+    if (rc) { drwc_job_destroy(j); return rc; }
+    double* d_w = (double*)d;
+    int32_t* d_end = (int32_t*)(d_w + nwalks);
+    int32_t* d_hops = d_end + nwalks;
+    int64_t* d_st = (int64_t*)(((uintptr_t)(d_hops + nwalks) + 7) & ~(uintptr_t)7);
+    rc = drwc_job_walks_device(j, walk0, nwalks, d_end, d_hops, d_w, d_st);
+    if (rc) { drwc_job_destroy(j); return rc; }
+    int64_t st[3] = {0, 0, 0};
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        DRWC_CUDA_TRY(cudaMemcpyAsync(end_net, d_end, nwalks * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        DRWC_CUDA_TRY(cudaMemcpyAsync(hops, d_hops, nwalks * 4, cudaMemcpyDeviceToHost, ctx->stream));
+        DRWC_CUDA_TRY(cudaMemcpyAsync(weight, d_w, nwalks * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        DRWC_CUDA_TRY(cudaMemcpyAsync(st, d_st, sizeof st, cudaMemcpyDeviceToHost, ctx->stream));
+        DRWC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    }
+    if (solver_stats) {
+        solver_stats[0] = st[0];
+        solver_stats[1] = st[1];
+        solver_stats[2] = st[2];
+        solver_stats[3] = st[0] * p->N * p->N * p->N;
+    }
+    return drwc_job_destroy(j);
+}
+
+DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
+                          drwc_job_result* out) {
+    if (!ctx || !out) return DRWC_ERR_INVALID;
+    const auto t0 = std::chrono::steady_clock::now();
+    drwc_job* job = nullptr;
+    int rc = drwc_job_create(ctx, s, p, &job);
+    if (rc) return rc;
+    struct JobGuard { drwc_job* j; ~JobGuard() { drwc_job_destroy(j); } } guard{job};
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    DRWC_CUDA_TRY(cudaSetDevice(ctx->device));
+    const HostGeom& hg = job->hg;
+    const Gauss& G = job->G;
+    const WalkParams& P = job->P;
+    const int ne = s->n_nets + 1;  // nets + ground
+    const long long batch = std::max<long long>(1, p->batch_walks);
+    WalkBuffers wb;
+    rc = walk_buffers(ctx, batch, ne, &wb);
+    if (rc) return rc;
+    // Neumaier-compensated FP64 accumulators per entry
+    std::vector<double> S(ne + 1, 0.0), Sc(ne + 1, 0.0), S2(ne + 1, 0.0), S2c(ne + 1, 0.0);
+    auto kadd = [](double& s, double& c, double v) {
+        const double t = s + v;
+        if (std::fabs(s) >= std::fabs(v)) c += (s - t) + v;
+        else c += (v - t) + s;
+        s = t;
+    };
+    long long walks = 0, lost = 0;
+    unsigned long long hops_total = 0;
+    std::vector<double> sums(3 * (ne + 1));
+    int converged = 0;
+    std::memset(out, 0, sizeof(*out));
+    while (walks < p->max_walks) {
+        const long long nw = std::min<long long>(batch, p->max_walks - walks);
+        rc = launch_walks(ctx, hg, G, P, walks, nw, wb);
+        if (rc) return rc;
+        reduce_kernel<<<ne + 1, 256, 0, ctx->stream>>>(ne, nw, wb.end, wb.w, wb.sums);
+        rc = launch_check(ctx);
+        if (rc) return rc;
+        hop_sum_kernel<<<std::max(1, std::min<int>((int)((nw + 255) / 256), 1024)), 256, 0,
+                         ctx->stream>>>(nw, wb.hops, wb.counter + 1);
+        rc = launch_check(ctx);
+        if (rc) return rc;
+        unsigned long long hsum = 0;
+        DRWC_CUDA_TRY(cudaMemcpyAsync(sums.data(), wb.sums, sums.size() * 8,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+        DRWC_CUDA_TRY(cudaMemcpyAsync(&hsum, wb.counter + 1, 8, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+        DRWC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+        for (int e = 0; e <= ne; ++e) {
+            kadd(S[e], Sc[e], sums[3 * e]);
+            kadd(S2[e], S2c[e], sums[3 * e + 1]);
+        }
+        lost += (long long)sums[3 * ne + 2];
+        hops_total += hsum;
+        walks += nw;
+        if (walks < p->min_walks) continue;
+        // convergence: relative 1-sigma of the self term <= p_tol, and of every
+        // significant coupling (ground included) <= c_tol, where the
+        // significant couplings are the largest ones that together make up
+        // c_ratio of the summed coupling magnitude.
+        const double n = (double)walks;
+        auto mean = [&](int e) { return (S[e] + Sc[e]) / n; };
+        auto sem = [&](int e) {
+            const double m = mean(e);
+            const double var = std::max(0.0, (S2[e] + S2c[e]) / n - m * m);
+            return std::sqrt(var / n);
+        };
+        const double cs = mean(p->master);
+        bool ok = cs != 0.0 && sem(p->master) <= p->p_tol * std::fabs(cs);
+        std::vector<std::pair<double, int>> cpl;
+        double ctot = 0.0;
+        for (int e = 0; e < ne; ++e) {
+            if (e == p->master) continue;
+            cpl.push_back({std::fabs(mean(e)), e});
+            ctot += std::fabs(mean(e));
+        }
+        std::sort(cpl.begin(), cpl.end(), [](auto& a, auto& b) { return a.first > b.first; });
+        double acc = 0.0;
+        for (auto& ce : cpl) {
+            if (acc >= p->c_ratio * ctot) break;
+            acc += ce.first;
+            if (!(ce.first > 0.0) || sem(ce.second) > p->c_tol * ce.first) { ok = false; break; }
+        }
+        if (ok) { converged = 1; break; }
+    }
+    const double n = (double)std::max(1LL, walks);
+    out->n_entries = ne;
+    out->converged = converged;
+    out->walks = walks;
+    out->hops = (int64_t)hops_total;
+    out->lost = lost;
+    for (int e = 0; e < ne; ++e) {
+        const double m = (S[e] + Sc[e]) / n;
+        out->cap[e] = m;
+        const double var = std::max(0.0, (S2[e] + S2c[e]) / n - m * m);
+        out->stderr_[e] = std::sqrt(var / n);
+    }
+    out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return DRWC_OK;
+}
+
+}  // extern "C"

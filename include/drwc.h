@@ -1,0 +1,253 @@
+/*
+ * drwc.h — C ABI of the B200 floating-random-walk (FRW) transition engine.
+ *
+ * Plain C: pointers, sizes and status codes; no C++ or torch types cross the
+ * boundary and no exception leaves the library. Every entry point returns a
+ * drwc_status (0 = success). Entry points taking HOST buffers are synchronous;
+ * the *_device variants take device pointers and run asynchronously on the
+ * context's stream.
+ *
+ * The entry points replace two plug points of the reference (DeepRWCap):
+ *   - ggft's FDM Green's-function generator
+ *     (ggft/src/ggft_solver.h:112-198: DIEL, solve(solver_code), gft,
+ *     set_tolerance), and
+ *   - the walker's calls into the dnnsolver library
+ *     (inference_cpp/src/dnn_solver.h:43-201: DNNSolverPoisson::sample,
+ *     DNNSolverGrad::sample, DNNSolver::structureConstruction,
+ *     ParallelSampler::submit),
+ * plus the walker itself (the reference ships it closed, executable/), as a
+ * device-resident job API.
+ *
+ * Conventions shared by every entry point:
+ *   - Cube permittivity is N^3 values, cell (i,j,k) at i + j*N + k*N*N
+ *     (x fastest), the order of ggft_solver.h:48 and of the dnnsolver's
+ *     [z][y][x] tensors (cuda_kernels.cu:36-39, 82).
+ *   - Surface values are 6*N*N panels in ggft order (ggft_solver.h:65-77):
+ *     face 0 z- (i + j*N), 1 z+, 2 y- (i + k*N), 3 y+, 4 x- (j + k*N), 5 x+.
+ *   - Solver codes follow ggft_solver::solver_code (ggft_solver.h:119).
+ */
+#ifndef DRWC_H
+#define DRWC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define DRWC_API __declspec(dllexport)
+#else
+#define DRWC_API __attribute__((visibility("default")))
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+typedef enum drwc_status {
+    DRWC_OK = 0,
+    DRWC_ERR_INVALID = 1,       /* bad argument (null pointer, size, N, code) */
+    DRWC_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+    DRWC_ERR_NOMEM = 3,         /* device or host allocation failed */
+    DRWC_ERR_NOT_CONVERGED = 4, /* at least one cube missed its tolerance */
+    DRWC_ERR_NO_DEVICE = 5,     /* no CUDA device / wrong architecture */
+    DRWC_ERR_TIMEOUT = 6,       /* a bounded wait ran out */
+    DRWC_ERR_SHUTDOWN = 7,      /* object is shutting down */
+    DRWC_ERR_GEOMETRY = 8       /* structure rejected (overlaps, empty, ...) */
+} drwc_status;
+
+/* ---- solver codes (ggft_solver.h:119) -------------------------------------- */
+enum { DRWC_GFT = 0, DRWC_WVTZ = 1, DRWC_WVTX = 2, DRWC_WVTY = 3 };
+
+/* ---- limits ----------------------------------------------------------------- */
+#define DRWC_N_MIN 4             /* smallest cube resolution */
+#define DRWC_N_MAX 23            /* largest cube resolution (the CTA-resident solve holds 18 B per cell on chip) */
+#define DRWC_MAX_LAYERS 15       /* dnn_solver.h:29 */
+#define DRWC_MAX_CUBOIDS 15      /* dnn_solver.h:28 */
+#define DRWC_LAYER_STRIDE (2 * DRWC_MAX_LAYERS)    /* floats per query (30) */
+#define DRWC_CUBOID_STRIDE (7 * DRWC_MAX_CUBOIDS)  /* floats per query (105) */
+#define DRWC_PADDING (-9999.0f)  /* dnn_solver.h:30 */
+#define DRWC_MAX_NETS 256        /* conductor nets per structure (+1 ground) */
+
+/* ---- library / context ------------------------------------------------------ */
+typedef struct drwc_ctx drwc_ctx;
+
+DRWC_API const char* drwc_version(void);
+DRWC_API const char* drwc_status_string(int status);
+/* Create a context on `device`: a non-blocking stream and lazily grown device
+ * workspaces, as DNNSolver's constructor (dnn_solver.cpp:13-38). Fails with
+ * DRWC_ERR_NO_DEVICE when the device is not sm_100. */
+DRWC_API int drwc_ctx_create(int device, drwc_ctx** out);
+DRWC_API int drwc_ctx_destroy(drwc_ctx* ctx);
+/* The context's stream (a cudaStream_t) for callers that enqueue around it. */
+DRWC_API int drwc_ctx_stream(drwc_ctx* ctx, void** stream_out);
+DRWC_API int drwc_ctx_synchronize(drwc_ctx* ctx);
+/* Number of kernels this context has launched so far. */
+DRWC_API int drwc_ctx_launch_count(drwc_ctx* ctx, int64_t* count_out);
+
+/* ---- FDM surface Green's function (ggft replacement) ------------------------ */
+/* Solver knobs. tol is the FP64 relative residual ||e - K y|| / ||e|| the
+ * refinement loop stops at; inner_tol is the relative reduction each FP32 PCG
+ * sweep aims for. */
+typedef struct drwc_fdm_opts {
+    double tol;        /* default 1e-10 */
+    double inner_tol;  /* default 1e-5 */
+    int32_t max_outer; /* FP64 refinement sweeps, default 8 */
+    int32_t max_inner; /* FP32 PCG iterations per sweep, default 4 * N * N */
+} drwc_fdm_opts;
+DRWC_API void drwc_fdm_opts_default(drwc_fdm_opts* opts);
+
+/* Drop-in for ggft_solver::solve(code) followed by reading ggft_solver::gft
+ * (ggft/src/ggft_solver.cpp:521-636): one cube, host buffers.
+ * eps: N^3 doubles (ggft's DIEL), gft_out: 6*N^2 doubles. tol has the meaning
+ * of ggft_solver::set_tolerance (ggft_solver.h:193-198) applied to the
+ * relative residual. iters_out (nullable) receives the FP32 CG iterations
+ * of all refinement sweeps. Returns DRWC_ERR_NOT_CONVERGED where ggft's solve() would
+ * return false. */
+DRWC_API int drwc_ggft_solve(drwc_ctx* ctx, int N, const double* eps, int code,
+                             double tol, double* gft_out, int32_t* iters_out);
+
+/* Batched solve of ncubes cubes of mixed resolution, device buffers, async on
+ * the context stream. Cube c has resolution N[c], permittivity at
+ * eps + eps_off[c] (N^3 doubles), solver code code[c] (NULL: all GFT), and
+ * writes 6*N^2 doubles at out + out_off[c]. N, eps_off, code and out_off are
+ * HOST arrays (the library groups cubes by N). iters / relres / status are
+ * per-cube DEVICE outputs (nullable): status 0 = converged, 1 = not
+ * converged, 2 = invalid permittivity (non-positive or non-finite). */
+DRWC_API int drwc_fdm_solve_batch_device(drwc_ctx* ctx, int ncubes, const int32_t* N,
+                                         const int64_t* eps_off, const double* eps,
+                                         const int32_t* code, const drwc_fdm_opts* opts,
+                                         const int64_t* out_off, double* out,
+                                         int32_t* iters, double* relres, int32_t* status);
+
+/* Same, host buffers (eps/out/iters/relres/status on the host); synchronous. */
+DRWC_API int drwc_fdm_solve_batch(drwc_ctx* ctx, int ncubes, const int32_t* N,
+                                  const int64_t* eps_off, const double* eps,
+                                  const int32_t* code, const drwc_fdm_opts* opts,
+                                  const int64_t* out_off, double* out,
+                                  int32_t* iters, double* relres, int32_t* status);
+
+/* ---- dnnsolver replacements ------------------------------------------------- */
+/* Drop-in for DNNSolver::structureConstruction (dnn_solver.cpp:252-300) with
+ * fill_structure_kernel (cuda_kernels.cu:21-84): n queries of 30 layer floats
+ * (15 x (min_z, eps)) and 105 cuboid floats (15 x (x0,y0,z0,x1,y1,z1,eps)),
+ * cube-normalised [-1,1] coordinates, padding -9999. Writes n x N^3 floats
+ * (eps / max eps per query when normalise != 0) and n max values. Host
+ * buffers. */
+DRWC_API int drwc_structure_construction(drwc_ctx* ctx, int n, int N, const float* layers,
+                                         const float* cuboids, int normalise,
+                                         float* eps_out, float* max_out);
+
+/* Drop-in for DNNSolverPoisson::sample (dnn_solver_poisson.cpp:35-63): for
+ * each of n queries voxelise the cube, solve its surface Green's function
+ * (FDM, GFT), sample one panel with probability G[b] and write the panel
+ * centre on the surface of [-1,1]^3 (3 floats, locate_index_simple_kernel,
+ * cuda_kernels.cu:219-264). Randomness: Philox4x32-10 keyed by `seed`,
+ * counter (stream + query index, 0, 0, 0). Host buffers. */
+DRWC_API int drwc_transition_batch(drwc_ctx* ctx, int n, int N, const float* layers,
+                                   const float* cuboids, uint64_t seed, uint64_t stream,
+                                   float* out_pos);
+
+/* Drop-in for DNNSolverGrad::sample (dnn_solver_gradient.cpp:49-73,
+ * 111-163): per query solve the centre-gradient surface values along axis
+ * (0 = x, 1 = y, 2 = z; WVTX/WVTY/WVTZ), sample a panel with probability
+ * |g_b| / sum|g| and write 5 floats: panel centre (3), sum|g| * sign(g_b),
+ * centre permittivity in the query's own units. axis may be NULL only to get
+ * the reference's error (DRWC_ERR_INVALID, dnn_solver_gradient.cpp:40-47).
+ * Host buffers. */
+DRWC_API int drwc_first_hop_batch(drwc_ctx* ctx, int n, int N, const float* layers,
+                                  const float* cuboids, const int32_t* axis, uint64_t seed,
+                                  uint64_t stream, float* out);
+
+/* ---- structures and the FRW walk (the closed walker's role) --------------- */
+typedef struct drwc_box {
+    double lo[3];
+    double hi[3];
+    int32_t net;   /* conductor net id in [0, n_nets) */
+    int32_t pad_;
+} drwc_box;
+
+typedef struct drwc_diel_box {
+    double lo[3];
+    double hi[3];
+    double eps;    /* relative permittivity, overrides the layers inside */
+} drwc_diel_box;
+
+typedef struct drwc_structure {
+    int32_t n_boxes;          /* conductor boxes */
+    int32_t n_nets;           /* nets; ground (the enclosure) is net n_nets */
+    const drwc_box* boxes;
+    int32_t n_layers;         /* stratified dielectric, sorted by zlo */
+    int32_t n_diel;           /* dielectric blocks (first containing wins) */
+    const double* layer_zlo;  /* layer l covers [zlo[l], zlo[l+1]) */
+    const double* layer_eps;
+    const drwc_diel_box* diel;
+    double encl_lo[3];        /* grounded enclosure */
+    double encl_hi[3];
+} drwc_structure;
+
+typedef struct drwc_job_params {
+    int32_t master;           /* master net */
+    int32_t N;                /* cube resolution of every hop */
+    double gauss_offset;      /* Gaussian surface offset from the master (um) */
+    double stop_dist;         /* absorption distance (um) */
+    double p_tol;             /* self-capacitance relative 1-sigma target (-p) */
+    double c_tol;             /* coupling relative 1-sigma target (-c) */
+    double c_ratio;           /* the largest couplings (ground included) that make up
+                                 this fraction of the summed coupling magnitude must
+                                 each meet c_tol (--c-ratio) */
+    int64_t min_walks;        /* walks before the first convergence check */
+    int64_t max_walks;        /* hard cap */
+    int64_t batch_walks;      /* walks per device batch between checks */
+    int32_t max_hops;         /* per walk; a walk reaching it is "lost" */
+    int32_t pad_;
+    uint64_t seed;
+    drwc_fdm_opts fdm;        /* per-hop solve knobs */
+} drwc_job_params;
+DRWC_API void drwc_job_params_default(drwc_job_params* p);
+
+typedef struct drwc_job_result {
+    int32_t n_entries;        /* n_nets + 1 (last = ground) */
+    int32_t converged;        /* 1 when -p/-c/--c-ratio were met */
+    int64_t walks;
+    int64_t hops;
+    int64_t lost;             /* walks cut at max_hops */
+    double seconds;           /* job wall time on the device */
+    double cap[DRWC_MAX_NETS + 1];     /* fF, row of the master */
+    double stderr_[DRWC_MAX_NETS + 1]; /* 1-sigma standard error, fF */
+} drwc_job_result;
+
+/* A prepared job: the structure validated and uploaded once (conductor boxes,
+ * dielectric layers and blocks, a uniform grid of conductor boxes for the
+ * nearest-conductor search), the Gaussian surface of the master built. */
+typedef struct drwc_job drwc_job;
+DRWC_API int drwc_job_create(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
+                             drwc_job** out);
+DRWC_API int drwc_job_destroy(drwc_job* job);
+/* Launch walks [walk0, walk0 + nwalks) on the context stream (async). Per-walk
+ * records go to DEVICE arrays end_net / hops / weight (fF); solver_stats
+ * (DEVICE, nullable, 3 int64) receives total hops, FP32 CG iterations and FP64
+ * residual sweeps of the launch. */
+DRWC_API int drwc_job_walks_device(drwc_job* job, int64_t walk0, int64_t nwalks,
+                                   int32_t* end_net, int32_t* hops, double* weight,
+                                   int64_t* solver_stats);
+/* Bytes of structure data the job uploaded to the device. */
+DRWC_API int drwc_job_h2d_bytes(drwc_job* job, int64_t* bytes);
+
+/* Run one extraction job (master row of the capacitance matrix) to
+ * convergence on the device. Host structure in, host result out. */
+DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
+                          drwc_job_result* out);
+
+/* Run walks [walk0, walk0 + nwalks) of a job and return the per-walk records
+ * (end net, hop count, weight in fF) to host arrays. Same walk ids give the
+ * same records whatever the batch; this is what the parity tests compare.
+ * solver_stats (nullable, 4 int64): total hops, FP32 CG iterations, FP64
+ * residual sweeps and cube cells solved (sum of N^3 over hops). */
+DRWC_API int drwc_frw_walks(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
+                            int64_t walk0, int64_t nwalks, int32_t* end_net, int32_t* hops,
+                            double* weight, int64_t* solver_stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DRWC_H */

@@ -1,0 +1,59 @@
+"""CPU checks of the C-ABI boundary: the library loads and exports every
+entry point include/drwc.h declares (no compute calls: no GPU here)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_symbols():
+    txt = (ROOT / "include" / "drwc.h").read_text()
+    return sorted(set(re.findall(r"DRWC_API\s+[\w\s\*]+?\b(drwc_\w+)\s*\(", txt)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "drwc_ggft_solve" in syms and "drwc_frw_run" in syms
+    from deeprwcap_b200 import abi
+    assert sorted(abi.EXPORTS) == syms
+
+
+def test_library_exports_every_declared_symbol():
+    from deeprwcap_b200 import abi
+    if not abi.LIB_PATH.exists():
+        from deeprwcap_b200 import build
+        build.build()
+    lib = C.CDLL(str(abi.LIB_PATH))
+    for s in declared_symbols():
+        assert hasattr(lib, s), s
+
+
+def test_pure_entry_points_without_device():
+    """Calls that touch no device: version, status strings, defaults and the
+    argument checks that run before any CUDA call."""
+    from deeprwcap_b200 import abi
+    L = abi.load()
+    assert b"sm_100a" in L.drwc_version()
+    assert L.drwc_status_string(0) == b"ok"
+    o = abi.default_fdm_opts()
+    assert o.tol == 1e-10 and o.max_outer == 8
+    p = abi.default_job_params()
+    assert p.N == 16 and p.max_hops == 10000
+    assert L.drwc_ggft_solve(None, 16, None, 0, 0.0, None, None) == 1
+    assert L.drwc_ctx_destroy(None) == 1
+    h = C.c_void_p()
+    rc = L.drwc_ctx_create(0, C.byref(h))
+    assert rc in (0, 5)  # no device in this container -> DRWC_ERR_NO_DEVICE
+    if rc == 0:
+        L.drwc_ctx_destroy(h)
+
+
+def test_product_does_not_import_oracle():
+    """The product package never reaches into oracle/."""
+    for f in (ROOT / "deeprwcap_b200").rglob("*"):
+        if f.suffix in (".py", ".cu", ".cuh", ".cpp", ".h"):
+            txt = f.read_text()
+            assert "oracle" not in re.sub(r"#.*|//.*", "", txt).replace("oracle/_ref", ""), f
