@@ -112,7 +112,7 @@ def load():
     L.drwc_fdm_opts_default.restype = None
     L.drwc_ggft_solve.argtypes = [vp, C.c_int, vp, C.c_int, dbl, vp, C.POINTER(i32)]
     L.drwc_fdm_solve_batch_device.argtypes = [vp, C.c_int, vp, vp, vp, vp,
-                                              C.POINTER(FdmOpts), vp, vp, vp, vp, vp]
+                                              C.POINTER(FdmOpts), vp, vp, vp, vp, vp, vp]
     L.drwc_fdm_solve_batch.argtypes = [vp, C.c_int, vp, vp, vp, vp, C.POINTER(FdmOpts), vp,
                                        vp, vp, vp, vp]
     L.drwc_structure_construction.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.c_int, vp, vp]

@@ -23,8 +23,9 @@ __global__ void __launch_bounds__(Cube<N>::NT)
 fdm_batch_kernel(int nsel, const int32_t* __restrict__ sel, const double* __restrict__ eps,
                  const int64_t* __restrict__ eps_off, const int32_t* __restrict__ code,
                  const int64_t* __restrict__ out_off, double* __restrict__ out,
-                 int32_t* __restrict__ iters, double* __restrict__ relres,
-                 int32_t* __restrict__ status, FdmParams prm, double* __restrict__ scratch_y,
+                 int32_t* __restrict__ iters, int32_t* __restrict__ sweeps,
+                 double* __restrict__ relres, int32_t* __restrict__ status, FdmParams prm,
+                 double* __restrict__ scratch_y,
                  float* __restrict__ scratch_s) {
     extern __shared__ __align__(128) unsigned char smem[];
     using D = Cube<N>;
@@ -45,6 +46,7 @@ fdm_batch_kernel(int nsel, const int32_t* __restrict__ sel, const double* __rest
         }
         if (threadIdx.x == 0) {
             if (iters) iters[c] = st.iters;
+            if (sweeps) sweeps[c] = st.sweeps;
             if (relres) relres[c] = st.relres;
             if (status) status[c] = st.status;
         }
@@ -105,7 +107,7 @@ DRWC_API int drwc_fdm_solve_batch_device(drwc_ctx* ctx, int ncubes, const int32_
                                          const int64_t* eps_off, const double* eps,
                                          const int32_t* code, const drwc_fdm_opts* opts,
                                          const int64_t* out_off, double* out, int32_t* iters,
-                                         double* relres, int32_t* status) {
+                                         int32_t* sweeps, double* relres, int32_t* status) {
     if (!ctx || ncubes < 0 || (ncubes > 0 && (!N || !eps_off || !eps || !out_off || !out)))
         return DRWC_ERR_INVALID;
     if (ncubes == 0) return DRWC_OK;
@@ -172,7 +174,7 @@ DRWC_API int drwc_fdm_solve_batch_device(drwc_ctx* ctx, int ncubes, const int32_
             FdmParams prm = make_params(opts, NC);
             fdm_batch_kernel<NC><<<grid, D::NT, D::kSmemBytes, ctx->stream>>>(
                 g.count, d_sel + g.first, eps, d_eoff, code ? d_code : nullptr, d_ooff, out,
-                iters, relres, status, prm, sy, sf);
+                iters, sweeps, relres, status, prm, sy, sf);
             return launch_check(ctx);
         });
         if (rc) return rc;
@@ -206,11 +208,12 @@ DRWC_API int drwc_fdm_solve_batch(drwc_ctx* ctx, int ncubes, const int32_t* N,
         DRWC_CUDA_TRY(cudaMemcpyAsync(d_in, eps, ein * sizeof(double), cudaMemcpyHostToDevice,
                                       ctx->stream));
     }
-    int32_t* d_it = (int32_t*)d_res;
+    // [relres: ncubes doubles][iters: ncubes int32][status: ncubes int32]
+    double* d_rr = (double*)d_res;
+    int32_t* d_it = (int32_t*)(d_rr + ncubes);
     int32_t* d_st = d_it + ncubes;
-    double* d_rr = (double*)(d_st + ncubes + (ncubes & 1));
     int rc = drwc_fdm_solve_batch_device(ctx, ncubes, N, eps_off, (const double*)d_in, code, opts,
-                                         out_off, (double*)d_out, d_it, d_rr, d_st);
+                                         out_off, (double*)d_out, d_it, nullptr, d_rr, d_st);
     if (rc) return rc;
     std::vector<int32_t> st(ncubes);
     {

@@ -110,14 +110,16 @@ DRWC_API int drwc_ggft_solve(drwc_ctx* ctx, int N, const double* eps, int code,
  * the context stream. Cube c has resolution N[c], permittivity at
  * eps + eps_off[c] (N^3 doubles), solver code code[c] (NULL: all GFT), and
  * writes 6*N^2 doubles at out + out_off[c]. N, eps_off, code and out_off are
- * HOST arrays (the library groups cubes by N). iters / relres / status are
- * per-cube DEVICE outputs (nullable): status 0 = converged, 1 = not
- * converged, 2 = invalid permittivity (non-positive or non-finite). */
+ * HOST arrays (the library groups cubes by N). iters (FP32 CG iterations),
+ * sweeps (FP64 residual evaluations), relres and status are per-cube DEVICE
+ * outputs (nullable): status 0 = converged, 1 = not converged, 2 = invalid
+ * permittivity (non-positive or non-finite). */
 DRWC_API int drwc_fdm_solve_batch_device(drwc_ctx* ctx, int ncubes, const int32_t* N,
                                          const int64_t* eps_off, const double* eps,
                                          const int32_t* code, const drwc_fdm_opts* opts,
                                          const int64_t* out_off, double* out,
-                                         int32_t* iters, double* relres, int32_t* status);
+                                         int32_t* iters, int32_t* sweeps, double* relres,
+                                         int32_t* status);
 
 /* Same, host buffers (eps/out/iters/relres/status on the host); synchronous. */
 DRWC_API int drwc_fdm_solve_batch(drwc_ctx* ctx, int ncubes, const int32_t* N,
