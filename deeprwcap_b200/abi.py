@@ -40,6 +40,7 @@ EXPORTS = [
     "drwc_fdm_solve_batch", "drwc_structure_construction", "drwc_transition_batch",
     "drwc_first_hop_batch", "drwc_job_params_default", "drwc_frw_run", "drwc_frw_walks",
     "drwc_job_create", "drwc_job_destroy", "drwc_job_walks_device", "drwc_job_h2d_bytes",
+    "drwc_fdm_solve_noalloc",
 ]
 
 
@@ -130,6 +131,8 @@ def load():
     L.drwc_job_destroy.argtypes = [vp]
     L.drwc_job_walks_device.argtypes = [vp, i64, i64, vp, vp, vp, vp]
     L.drwc_job_h2d_bytes.argtypes = [vp, C.POINTER(i64)]
+    L.drwc_fdm_solve_noalloc.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.POINTER(FdmOpts), vp,
+                                         vp, vp]
     _lib = L
     return L
 

@@ -128,6 +128,25 @@ DRWC_API int drwc_fdm_solve_batch(drwc_ctx* ctx, int ncubes, const int32_t* N,
                                   const int64_t* out_off, double* out,
                                   int32_t* iters, double* relres, int32_t* status);
 
+/* Same-N batch with no device allocation. No counterpart in the reference:
+ * it exists for callers that cannot allocate device memory when they call in
+ * (an application that owns all GPU memory through its own pool and forbids
+ * later driver allocations, or a latency-critical loop where a cudaMalloc and
+ * its implicit synchronisation are not allowed). Cube c reads N^3 doubles at
+ * eps + c*N^3 and writes 6*N^2 doubles at out + c*6*N^2; code (nullable: all
+ * GFT), iters and status (nullable) are DEVICE arrays of ncubes entries, as
+ * in drwc_fdm_solve_batch_device. Runs async on the context stream. Solver
+ * scratch comes from a fixed 16 MiB static device array in the library
+ * (12 bytes per cell per resident CTA; every GPU that loads the library holds
+ * it until exit); N outside [DRWC_N_MIN, DRWC_N_MAX] is rejected with
+ * DRWC_ERR_INVALID. The first call on a device sets up (looks up the array's
+ * device address, sets kernel attributes) and should come before any stream
+ * capture. Calls share the array: calls that overlap on the GPU race, so
+ * issue them on one stream. */
+DRWC_API int drwc_fdm_solve_noalloc(drwc_ctx* ctx, int N, int ncubes, const double* eps,
+                                    const int32_t* code, const drwc_fdm_opts* opts, double* out,
+                                    int32_t* iters, int32_t* status);
+
 /* ---- dnnsolver replacements ------------------------------------------------- */
 /* Drop-in for DNNSolver::structureConstruction (dnn_solver.cpp:252-300) with
  * fill_structure_kernel (cuda_kernels.cu:21-84): n queries of 30 layer floats
