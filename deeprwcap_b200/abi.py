@@ -14,7 +14,7 @@ from pathlib import Path
 import numpy as np
 
 PKG = Path(__file__).resolve().parent
-LIB_PATH = PKG / "libdrwc.so"
+LIB_PATH = Path(os.environ.get("DRWC_LIBRARY", str(PKG / "libdrwc.so")))
 
 MAX_NETS = 256
 MAX_LAYERS = 15

@@ -20,12 +20,14 @@ from pathlib import Path
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
-BUILD = PKG / "_build"
-LIB = PKG / "libdrwc.so"
+BUILD = Path(os.environ.get("DRWC_BUILD_DIR", str(PKG / "_build")))
+LIB = Path(os.environ.get("DRWC_LIBRARY", str(PKG / "libdrwc.so")))
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr",
               "-Xcompiler", "-fPIC,-fvisibility=hidden", "-I", str(ROOT / "include")]
+# Extra -D flags (tuning sweeps build variants into another folder with these).
+EXTRA = os.environ.get("DRWC_NVCC_DEFINES", "").split()
 
 
 def nvcc() -> str:
@@ -44,7 +46,7 @@ def _compile(src: Path, verbose: bool, ptxas_v: bool) -> tuple[Path, str]:
     newest = max([src.stat().st_mtime] + [h.stat().st_mtime for h in _headers()])
     if obj.exists() and obj.stat().st_mtime >= newest and not ptxas_v:
         return obj, ""
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *EXTRA, "-c", str(src), "-o", str(obj)]
     if ptxas_v:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

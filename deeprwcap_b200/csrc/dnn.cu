@@ -111,9 +111,9 @@ query_kernel(int n, const float* __restrict__ layers, const float* __restrict__ 
             code = a == 0 ? DRWC_WVTX : a == 1 ? DRWC_WVTY : DRWC_WVTZ;
         }
         FdmStats st;
-        cube_solve<N>(sm, es, ys, ss, code, prm, &st);
+        cube_solve<N>(sm, EpsGlobal{es}, ys, ss, code, prm, &st);
         double* w = reinterpret_cast<double*>(sm.stage());  // 6N^2 doubles over p|cx|cy|cz
-        for_each_panel<N>(es, ys, [&](int b, double v) { w[b] = v; });
+        for_each_panel<N>(EpsGlobal{es}, ys, [&](int b, double v) { w[b] = v; });
         __syncthreads();
         const double u = philox_uniform2(seed, stream + (uint64_t)q, 0, 0).x;
         double tot = 0.0;
@@ -128,7 +128,7 @@ query_kernel(int n, const float* __restrict__ layers, const float* __restrict__ 
                 o[0] = pos[0]; o[1] = pos[1]; o[2] = pos[2];
                 if (GRAD) {
                     o[3] = (float)(w[b] < 0.0 ? -tot : tot);
-                    o[4] = (float)(center_diel<N>(es, code) * (double)m);
+                    o[4] = (float)(center_diel<N>(EpsGlobal{es}, code) * (double)m);
                 }
             }
             if (status) status[q] = b < 0 ? 2 : st.status;

@@ -19,7 +19,7 @@ namespace drwc {
 // Per-cube input is FP64 permittivity in global memory, read by the set-up
 // passes of cube_solve and by its FP64 residual sweeps.
 template <int N>
-__global__ void __launch_bounds__(Cube<N>::NT)
+__global__ void __launch_bounds__(Cube<N>::NT, CubeTraits<N>::kMinBlocks)
 fdm_batch_kernel(int nsel, const int32_t* __restrict__ sel, const double* __restrict__ eps,
                  const int64_t* __restrict__ eps_off, const int32_t* __restrict__ code,
                  const int64_t* __restrict__ out_off, double* __restrict__ out,
@@ -37,12 +37,12 @@ fdm_batch_kernel(int nsel, const int32_t* __restrict__ sel, const double* __rest
         const double* e = eps + eps_off[c];
         const int cd = code ? code[c] : DRWC_GFT;
         FdmStats st;
-        cube_solve<N>(sm, e, ys, ss, cd, prm, &st);
+        cube_solve<N>(sm, EpsGlobal{e}, ys, ss, cd, prm, &st);
         double* o = out + out_off[c];
         if (st.status == 2) {
             for (int b = threadIdx.x; b < 6 * D::NN; b += blockDim.x) o[b] = 0.0;
         } else {
-            for_each_panel<N>(e, ys, [&](int b, double v) { o[b] = v; });
+            for_each_panel<N>(EpsGlobal{e}, ys, [&](int b, double v) { o[b] = v; });
         }
         if (threadIdx.x == 0) {
             if (iters) iters[c] = st.iters;

@@ -121,15 +121,58 @@ DRWC_DEV double block_sum_d(double v, double* red, int slot) {
     return s;
 }
 
+// ----------------------------------------------------------- permittivity
+// Where a cube's permittivity comes from. Both sources give the FP64 value of
+// a cell, the FP64 conductance g = e_p e_q / (e_p + e_q) of a face link and
+// its FP32 counterpart for the inner solve.
+//
+// EpsGlobal: an arbitrary FP64 array in global memory (the ggft drop-in and
+// the batched solver); conductances are computed per use.
+struct EpsGlobal {
+    const double* __restrict__ eps;
+    DRWC_DEV double e64(int c) const { return eps[c]; }
+    DRWC_DEV float e32(int c) const { return (float)eps[c]; }
+    DRWC_DEV double g64(int c, int q) const {
+        const double a = eps[c], b = eps[q];
+        return a * b / (a + b);
+    }
+    DRWC_DEV float g32(int c, int q) const {
+        const float a = (float)eps[c], b = (float)eps[q];
+        return a * b / (a + b);
+    }
+    DRWC_DEV bool valid(int c) const {
+        const double v = eps[c];
+        return v > 0.0 && isfinite(v);
+    }
+};
+
+// EpsPalette: piecewise-constant structures (the walker). Each cell holds a
+// material id (shared memory, 1 byte); the job's palette of permittivities
+// and the table of pair conductances g(m, m') are precomputed once per job,
+// so set-up and FP64 sweeps need neither divisions nor global loads.
+struct EpsPalette {
+    const uint8_t* mat;     // N^3 material ids (shared memory)
+    const double* pal;      // P permittivities (shared memory)
+    const double* pair64;   // P x P conductances (shared memory)
+    const float* pair32;    // P x P, FP32
+    int P;
+    DRWC_DEV double e64(int c) const { return pal[mat[c]]; }
+    DRWC_DEV float e32(int c) const { return (float)pal[mat[c]]; }
+    DRWC_DEV double g64(int c, int q) const { return pair64[mat[c] * P + mat[q]]; }
+    DRWC_DEV float g32(int c, int q) const { return pair32[mat[c] * P + mat[q]]; }
+    DRWC_DEV bool valid(int c) const { return true; }  // palette checked on the host
+};
+
 // ------------------------------------------------------------ right-hand side
 // Centre sources of ggft_solver.cpp:137-274 (unit source / centre gradient,
 // h = 2/N). Written by thread 0 into smem as (cell, value) pairs.
-template <int N>
-DRWC_DEV void build_rhs(const double* __restrict__ eps, int code, const CubeSmem<N>& sm) {
+template <int N, class E>
+DRWC_DEV void build_rhs(const E& eps, int code, const CubeSmem<N>& sm) {
     if (threadIdx.x != 0) return;
     const double h = 2.0 / N;
     const int c = N / 2;
     auto id = [](int i, int j, int k) { return i + j * N + k * N * N; };
+    auto Ev = [&](int cell) { return eps.e64(cell); };
     int n = 0;
     if (N % 2) {
         const int zzz = id(c, c, c);
@@ -138,24 +181,23 @@ DRWC_DEV void build_rhs(const double* __restrict__ eps, int code, const CubeSmem
         } else {
             const int stride = code == DRWC_WVTZ ? N * N : code == DRWC_WVTX ? 1 : N;
             const int pp = zzz + stride, mm = zzz - stride;
-            const double d_plus = eps[pp] + eps[zzz];
-            const double d_minus = -(eps[zzz] + eps[mm]);
-            sm.rhs_idx[0] = pp;  sm.rhs_val[0] = eps[pp] / d_plus / h;
-            sm.rhs_idx[1] = zzz; sm.rhs_val[1] = eps[zzz] * (1. / d_plus + 1. / d_minus) / h;
-            sm.rhs_idx[2] = mm;  sm.rhs_val[2] = eps[mm] / d_minus / h;
+            const double d_plus = Ev(pp) + Ev(zzz);
+            const double d_minus = -(Ev(zzz) + Ev(mm));
+            sm.rhs_idx[0] = pp;  sm.rhs_val[0] = Ev(pp) / d_plus / h;
+            sm.rhs_idx[1] = zzz; sm.rhs_val[1] = Ev(zzz) * (1. / d_plus + 1. / d_minus) / h;
+            sm.rhs_idx[2] = mm;  sm.rhs_val[2] = Ev(mm) / d_minus / h;
             n = 3;
         }
     } else {
         const int zzz = id(c, c, c), zmz = id(c, c - 1, c), zzm = id(c, c, c - 1),
                   zmm = id(c, c - 1, c - 1), mzz = id(c - 1, c, c), mmz = id(c - 1, c - 1, c),
                   mzm = id(c - 1, c, c - 1), mmm = id(c - 1, c - 1, c - 1);
-        const double dsum = eps[zzz] + eps[zmz] + eps[zzm] + eps[zmm] + eps[mzz] + eps[mmz] +
-                            eps[mzm] + eps[mmm];
+        const double dsum = Ev(zzz) + Ev(zmz) + Ev(zzm) + Ev(zmm) + Ev(mzz) + Ev(mmz) + Ev(mzm) + Ev(mmm);
         if (code == DRWC_GFT) {
             const int cells[8] = {zzz, mzz, zmz, zzm, mmz, mzm, zmm, mmm};
             for (int t = 0; t < 8; ++t) {
                 sm.rhs_idx[t] = cells[t];
-                sm.rhs_val[t] = eps[cells[t]] / dsum;
+                sm.rhs_val[t] = Ev(cells[t]) / dsum;
             }
         } else {
             int plus[4], minus[4];
@@ -163,21 +205,21 @@ DRWC_DEV void build_rhs(const double* __restrict__ eps, int code, const CubeSmem
             if (code == DRWC_WVTZ) {
                 plus[0] = zzz; plus[1] = mzz; plus[2] = zmz; plus[3] = mmz;
                 minus[0] = zzm; minus[1] = mzm; minus[2] = zmm; minus[3] = mmm;
-                d_minus = -(eps[zzm] + eps[mzm] + eps[zmm] + eps[mmm]);
+                d_minus = -(Ev(zzm) + Ev(mzm) + Ev(zmm) + Ev(mmm));
             } else if (code == DRWC_WVTX) {
                 plus[0] = zzz; plus[1] = zmz; plus[2] = zzm; plus[3] = zmm;
                 minus[0] = mzz; minus[1] = mmz; minus[2] = mzm; minus[3] = mmm;
-                d_minus = -(eps[mzz] + eps[mmz] + eps[mzm] + eps[mmm]);
+                d_minus = -(Ev(mzz) + Ev(mmz) + Ev(mzm) + Ev(mmm));
             } else {
                 plus[0] = zzz; plus[1] = mzz; plus[2] = zzm; plus[3] = mzm;
                 minus[0] = zmz; minus[1] = mmz; minus[2] = zmm; minus[3] = mmm;
-                d_minus = -(eps[zmz] + eps[mmz] + eps[zmm] + eps[mmm]);
+                d_minus = -(Ev(zmz) + Ev(mmz) + Ev(zmm) + Ev(mmm));
             }
             for (int t = 0; t < 4; ++t) {
                 sm.rhs_idx[t] = plus[t];
-                sm.rhs_val[t] = eps[plus[t]] / dsum / h * 2;
+                sm.rhs_val[t] = Ev(plus[t]) / dsum / h * 2;
                 sm.rhs_idx[4 + t] = minus[t];
-                sm.rhs_val[4 + t] = eps[minus[t]] * (1. / dsum + 1. / d_minus) / h * 2;
+                sm.rhs_val[4 + t] = Ev(minus[t]) * (1. / dsum + 1. / d_minus) / h * 2;
             }
         }
         n = 8;
@@ -185,46 +227,55 @@ DRWC_DEV void build_rhs(const double* __restrict__ eps, int code, const CubeSmem
     sm.flags[0] = n;
 }
 
-template <int N>
-DRWC_DEV double rhs_at(const CubeSmem<N>& sm, int cell) {
-    double v = 0.0;
-    const int n = sm.flags[0];
-    for (int t = 0; t < n; ++t)
-        if (sm.rhs_idx[t] == cell) v = sm.rhs_val[t];
-    return v;
-}
-
 // Permittivity the first-hop weight is scaled by (ggft_solver.cpp:649-671):
 // odd N the centre cell, even N the mean of the four centre cells on the
 // minus side of the gradient axis.
-template <int N>
-DRWC_DEV double center_diel(const double* __restrict__ eps, int code) {
+template <int N, class E>
+DRWC_DEV double center_diel(const E& eps, int code) {
     const int c = N / 2;
     auto id = [](int i, int j, int k) { return i + j * N + k * N * N; };
-    if ((N % 2) || code == DRWC_GFT) return eps[id(c, c, c)];
+    auto V = [&](int cell) { return eps.e64(cell); };
+    if ((N % 2) || code == DRWC_GFT) return V(id(c, c, c));
     if (code == DRWC_WVTZ)
-        return (eps[id(c, c, c - 1)] + eps[id(c - 1, c - 1, c - 1)] + eps[id(c, c - 1, c - 1)] +
-                eps[id(c - 1, c, c - 1)]) / 4;
+        return (V(id(c, c, c - 1)) + V(id(c - 1, c - 1, c - 1)) + V(id(c, c - 1, c - 1)) +
+                V(id(c - 1, c, c - 1))) / 4;
     if (code == DRWC_WVTX)
-        return (eps[id(c - 1, c, c)] + eps[id(c - 1, c - 1, c)] + eps[id(c - 1, c, c - 1)] +
-                eps[id(c - 1, c - 1, c - 1)]) / 4;
-    return (eps[id(c, c - 1, c)] + eps[id(c - 1, c - 1, c)] + eps[id(c, c - 1, c - 1)] +
-            eps[id(c - 1, c - 1, c - 1)]) / 4;
+        return (V(id(c - 1, c, c)) + V(id(c - 1, c - 1, c)) + V(id(c - 1, c, c - 1)) +
+                V(id(c - 1, c - 1, c - 1))) / 4;
+    return (V(id(c, c - 1, c)) + V(id(c - 1, c - 1, c)) + V(id(c, c - 1, c - 1)) +
+            V(id(c - 1, c - 1, c - 1))) / 4;
 }
 
+#ifndef DRWC_PREGS_MAX_N
+#define DRWC_PREGS_MAX_N 16
+#endif
+#ifndef DRWC_MIN_BLOCKS_256
+#define DRWC_MIN_BLOCKS_256 2
+#endif
+
+template <int N>
+struct CubeTraits {
+    // Keep the thread's own column of p in registers too (saves three shared
+    // loads per cell and iteration) when the register file allows it.
+    static constexpr bool kPRegs = N <= DRWC_PREGS_MAX_N;
+    // Resident CTAs per SM the register allocation is sized for.
+    static constexpr int kMinBlocks = Cube<N>::NT <= 256 ? DRWC_MIN_BLOCKS_256 : 1;
+};
+
 // --------------------------------------------------------------- the solver
-// eps:  N^3 FP64 permittivity in global memory (cell i + j*N + k*N*N).
+// eps:  permittivity source (EpsGlobal / EpsPalette), cell i + j*N + k*N*N.
 // ys:   N^3 doubles of global scratch (the FP64 solution y of K y = e).
 // ss:   N^3 floats of global scratch (the Jacobi scale S).
 // On return (all threads) ys holds y and the stats are filled; shared memory
 // p/cx/cy/cz are free for the caller.
-template <int N>
-__device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const double* __restrict__ eps,
+template <int N, class E>
+__device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const E eps,
                                         double* __restrict__ ys, float* __restrict__ ss, int code,
                                         const FdmParams& prm, FdmStats* st) {
     using D = Cube<N>;
     constexpr int NN = D::NN;
     constexpr int NW = D::NW;
+    constexpr bool PR = CubeTraits<N>::kPRegs;
     const int t = threadIdx.x;
     const bool active = t < NN;
     const int i = t % N, j = t / N;
@@ -246,16 +297,15 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const double* __r
 #pragma unroll 1
         for (int k = 0; k < N; ++k) {
             const int c = base + k * NN;
-            const double e64 = eps[c];
-            bad |= !(e64 > 0.0) || !isfinite(e64);
-            const float ec = (float)e64;
+            bad |= !eps.valid(c);
+            const float ec = eps.e32(c);
             float d = 0.f;
-            d += (i + 1 < N) ? ec * (float)eps[c + 1] / (ec + (float)eps[c + 1]) : ec;
-            d += (i > 0) ? ec * (float)eps[c - 1] / (ec + (float)eps[c - 1]) : ec;
-            d += (j + 1 < N) ? ec * (float)eps[c + N] / (ec + (float)eps[c + N]) : ec;
-            d += (j > 0) ? ec * (float)eps[c - N] / (ec + (float)eps[c - N]) : ec;
-            d += (k + 1 < N) ? ec * (float)eps[c + NN] / (ec + (float)eps[c + NN]) : ec;
-            d += (k > 0) ? ec * (float)eps[c - NN] / (ec + (float)eps[c - NN]) : ec;
+            d += (i + 1 < N) ? eps.g32(c, c + 1) : ec;
+            d += (i > 0) ? eps.g32(c, c - 1) : ec;
+            d += (j + 1 < N) ? eps.g32(c, c + N) : ec;
+            d += (j > 0) ? eps.g32(c, c - N) : ec;
+            d += (k + 1 < N) ? eps.g32(c, c + NN) : ec;
+            d += (k > 0) ? eps.g32(c, c - NN) : ec;
             ss[c] = rsqrtf(d);
             ys[c] = 0.0;
         }
@@ -271,66 +321,58 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const double* __r
 #pragma unroll 1
         for (int k = 0; k < N; ++k) {
             const int c = base + k * NN;
-            const float ec = (float)eps[c];
             const float sc = ss[c];
             float vx = 0.f, vy = 0.f, vz = 0.f;
-            if (i + 1 < N) { const float eq = (float)eps[c + 1]; vx = ec * eq / (ec + eq) * sc * ss[c + 1]; }
-            if (j + 1 < N) { const float eq = (float)eps[c + N]; vy = ec * eq / (ec + eq) * sc * ss[c + N]; }
-            if (k + 1 < N) { const float eq = (float)eps[c + NN]; vz = ec * eq / (ec + eq) * sc * ss[c + NN]; }
+            if (i + 1 < N) vx = eps.g32(c, c + 1) * sc * ss[c + 1];
+            if (j + 1 < N) vy = eps.g32(c, c + N) * sc * ss[c + N];
+            if (k + 1 < N) vz = eps.g32(c, c + NN) * sc * ss[c + NN];
             sm.cx[c] = vx; sm.cy[c] = vy; sm.cz[c] = vz;
         }
     }
     // ||e|| (FP64) from the rhs table
     double enorm2 = 0.0;
-    for (int q = 0; q < sm.flags[0]; ++q) enorm2 += sm.rhs_val[q] * sm.rhs_val[q];
+    const int nrhs = sm.flags[0];
+    for (int q = 0; q < nrhs; ++q) enorm2 += sm.rhs_val[q] * sm.rhs_val[q];
     const double enorm = sqrt(enorm2);
 
-    float r[N], x[N], q[N];
+    float r[N], x[N], q[N], pr[PR ? N : 1];
+    // Sweep 0: y = 0, so e - K y = e (non-zero only at the centre source).
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) r[k] = 0.f;
+        for (int v = 0; v < nrhs; ++v) {
+            const int cell = sm.rhs_idx[v];
+            if (cell % NN == base) {
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                    if (cell / NN == k) r[k] = (float)((double)ss[cell] * sm.rhs_val[v]);
+            }
+        }
+    }
     int total_inner = 0, outer = 0;
     double relres = 1.0;
     int status = 1;
 #pragma unroll 1
-    for (outer = 0; outer <= prm.max_outer; ++outer) {
-        // ---- FP64 residual r64 = e - K y, inner rhs b = S r64 (FP32 regs)
-        __syncthreads();  // ys writes of the previous sweep visible
-        double rn2 = 0.0;
-        if (active) {
-#pragma unroll
-            for (int k = 0; k < N; ++k) {
-                const int c = base + k * NN;
-                const double ec = eps[c];
-                const double yc = ys[c];
-                double diag = 0.0, off = 0.0;
-                if (i + 1 < N) { const double eq = eps[c + 1]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c + 1]; } else diag += ec;
-                if (i > 0) { const double eq = eps[c - 1]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c - 1]; } else diag += ec;
-                if (j + 1 < N) { const double eq = eps[c + N]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c + N]; } else diag += ec;
-                if (j > 0) { const double eq = eps[c - N]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c - N]; } else diag += ec;
-                if (k + 1 < N) { const double eq = eps[c + NN]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c + NN]; } else diag += ec;
-                if (k > 0) { const double eq = eps[c - NN]; const double g = ec * eq / (ec + eq); diag += g; off += g * ys[c - NN]; } else diag += ec;
-                const double r64 = rhs_at<N>(sm, c) - (diag * yc - off);
-                rn2 += r64 * r64;
-                r[k] = (float)((double)ss[c] * r64);
-            }
-        }
-        rn2 = block_sum_d<NW>(rn2, sm.red, 0);
-        relres = sqrt(rn2) / enorm;
-        if (relres <= prm.tol) { status = 0; break; }
-        if (outer == prm.max_outer) break;
-
-        // ---- FP32 CG on K~ d = b, d in x[], starting from 0
+    for (outer = 0; outer < prm.max_outer; ++outer) {
+        // ---- FP32 CG on K~ d = b, d in x[], starting from 0. The reduction
+        //      it needs is set so this sweep brings ||e - K y|| to about half
+        //      the target (no deeper than inner_tol per sweep).
         float rr = 0.f;
 #pragma unroll
         for (int k = 0; k < N; ++k) {
             x[k] = 0.f;
             if (active) {
                 sm.p[base + k * NN] = r[k];
+                if constexpr (PR) pr[k] = r[k];
                 rr += r[k] * r[k];
             } else {
                 r[k] = 0.f;
+                if constexpr (PR) pr[k] = 0.f;
             }
         }
         rr = block_sum_f<NW>(rr, sm.red, 1);  // barrier also publishes p
-        const float stop2 = rr * prm.inner_tol * prm.inner_tol;
+        const float want = fmaxf(prm.inner_tol, (float)(0.5 * prm.tol / relres));
+        const float stop2 = rr * want * want;
         int it = 0;
 #pragma unroll 1
         for (it = 0; it < prm.max_inner && rr > stop2; ++it) {
@@ -338,11 +380,13 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const double* __r
             float pq = 0.f;
             if (active) {
                 float pm = 0.f, czm = 0.f;
-                float pc = sm.p[base];
+                float pc = PR ? pr[0] : sm.p[base];
 #pragma unroll
                 for (int k = 0; k < N; ++k) {
                     const int c = base + k * NN;
-                    const float pn = (k + 1 < N) ? sm.p[c + NN] : 0.f;
+                    float pn;
+                    if constexpr (PR) pn = (k + 1 < N) ? pr[(k + 1) % N] : 0.f;
+                    else pn = (k + 1 < N) ? sm.p[c + NN] : 0.f;
                     const float czc = sm.cz[c];
                     const float nb = sm.cx[c - 1] * sm.p[c - 1] + sm.cx[c] * sm.p[c + 1] +
                                      sm.cy[c - N] * sm.p[c - N] + sm.cy[c] * sm.p[c + N] +
@@ -359,7 +403,8 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const double* __r
 #pragma unroll
                 for (int k = 0; k < N; ++k) {
                     const int c = base + k * NN;
-                    x[k] += alpha * sm.p[c];
+                    if constexpr (PR) x[k] += alpha * pr[k];
+                    else x[k] += alpha * sm.p[c];
                     r[k] -= alpha * q[k];
                     rr2 += r[k] * r[k];
                 }
@@ -371,7 +416,12 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const double* __r
 #pragma unroll
                 for (int k = 0; k < N; ++k) {
                     const int c = base + k * NN;
-                    sm.p[c] = r[k] + beta * sm.p[c];
+                    if constexpr (PR) {
+                        pr[k] = r[k] + beta * pr[k];
+                        sm.p[c] = pr[k];
+                    } else {
+                        sm.p[c] = r[k] + beta * sm.p[c];
+                    }
                 }
             }
             __syncthreads();
@@ -385,18 +435,45 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const double* __r
                 ys[c] += (double)ss[c] * (double)x[k];
             }
         }
+        __syncthreads();  // y of the neighbours visible
+        // ---- FP64 residual r64 = e - K y, next inner rhs b = S r64 (FP32 regs)
+        double rn2 = 0.0;
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                const int c = base + k * NN;
+                const double ec = eps.e64(c);
+                const double yc = ys[c];
+                double diag = 0.0, off = 0.0;
+                if (i + 1 < N) { const double g = eps.g64(c, c + 1); diag += g; off += g * ys[c + 1]; } else diag += ec;
+                if (i > 0) { const double g = eps.g64(c, c - 1); diag += g; off += g * ys[c - 1]; } else diag += ec;
+                if (j + 1 < N) { const double g = eps.g64(c, c + N); diag += g; off += g * ys[c + N]; } else diag += ec;
+                if (j > 0) { const double g = eps.g64(c, c - N); diag += g; off += g * ys[c - N]; } else diag += ec;
+                if (k + 1 < N) { const double g = eps.g64(c, c + NN); diag += g; off += g * ys[c + NN]; } else diag += ec;
+                if (k > 0) { const double g = eps.g64(c, c - NN); diag += g; off += g * ys[c - NN]; } else diag += ec;
+                double e_c = 0.0;
+                for (int v = 0; v < nrhs; ++v)
+                    if (sm.rhs_idx[v] == c) e_c = sm.rhs_val[v];
+                const double r64 = e_c - (diag * yc - off);
+                rn2 += r64 * r64;
+                r[k] = (float)((double)ss[c] * r64);
+            }
+        }
+        rn2 = block_sum_d<NW>(rn2, sm.red, 0);
+        relres = sqrt(rn2) / enorm;
+        if (relres <= prm.tol) { status = 0; ++outer; break; }
     }
     st->status = status;
     st->iters = total_inner;
-    st->sweeps = outer + 1;
+    st->sweeps = outer;
     st->relres = relres;
     __syncthreads();
 }
 
 // Surface values gft[b] = eps_c * y_c under panel b (ggft panel order,
 // ggft_solver.h:65-77). Cooperative over the CTA; writes through `put(b, v)`.
-template <int N, class Put>
-DRWC_DEV void for_each_panel(const double* __restrict__ eps, const double* __restrict__ ys, Put put) {
+template <int N, class E, class Put>
+DRWC_DEV void for_each_panel(const E& eps, const double* __restrict__ ys, Put put) {
     constexpr int NN = N * N;
     for (int b = threadIdx.x; b < 6 * NN; b += blockDim.x) {
         const int f = b / NN, tt = b % NN;
@@ -410,7 +487,7 @@ DRWC_DEV void for_each_panel(const double* __restrict__ eps, const double* __res
             case 4: c = a * N + bb * NN; break;                   // x-: (0,j,k)
             default: c = (N - 1) + a * N + bb * NN; break;        // x+
         }
-        put(b, eps[c] * ys[c]);
+        put(b, eps.e64(c) * ys[c]);
     }
 }
 

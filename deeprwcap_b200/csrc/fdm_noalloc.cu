@@ -48,12 +48,12 @@ fdm_noalloc_kernel(int ncubes, const double* __restrict__ eps, const int32_t* __
         const double* e = eps + (size_t)c * D::NNN;
         const int cd = code ? code[c] : DRWC_GFT;
         FdmStats st;
-        cube_solve<N>(sm, e, ys, ss, cd, prm, &st);
+        cube_solve<N>(sm, EpsGlobal{e}, ys, ss, cd, prm, &st);
         double* o = out + (size_t)c * 6 * D::NN;
         if (st.status == 2) {
             for (int b = threadIdx.x; b < 6 * D::NN; b += blockDim.x) o[b] = 0.0;
         } else {
-            for_each_panel<N>(e, ys, [&](int b, double v) { o[b] = v; });
+            for_each_panel<N>(EpsGlobal{e}, ys, [&](int b, double v) { o[b] = v; });
         }
         if (threadIdx.x == 0) {
             if (iters) iters[c] = st.iters;

@@ -40,13 +40,20 @@ FdmParams make_params(const drwc_fdm_opts* o, int N);
 constexpr double kEps0FfPerUm = 8.8541878128e-3;  // vacuum permittivity, fF/um
 constexpr int kBruteBoxes = 16;                  // <= this many boxes: scan all
 
+constexpr int kMaxMaterials = 32;              // distinct permittivities per structure
+
 struct DevGeom {
     int n_boxes, n_nets, n_layers, n_diel;
     const double* box;      // n_boxes x 6 (lo xyz, hi xyz)
     const int* net;         // n_boxes
     const double* zlo;      // n_layers
-    const double* leps;     // n_layers
-    const double* diel;     // n_diel x 7
+    const int* lmat;        // n_layers material ids
+    const double* diel;     // n_diel x 7 (eps slot unused on the device)
+    const int* dmat;        // n_diel material ids
+    const double* pal;      // n_mat distinct permittivities
+    const double* pair64;   // n_mat x n_mat conductances e e' / (e + e')
+    const float* pair32;
+    int n_mat;
     double encl_lo[3], encl_hi[3];
     // uniform grid over the enclosure (CSR cell -> boxes)
     int gdim[3];
@@ -151,33 +158,53 @@ DRWC_DEV void nearest(const DevGeom& g, const double r[3], double* d_out, int* n
     }
 }
 
-DRWC_DEV double eps_at(const DevGeom& g, const double p[3]) {
+// Material id at a point: first containing dielectric block, else the last
+// stratified layer with zlo <= z (layer 0 below all of them).
+DRWC_DEV int mat_at(const DevGeom& g, const double p[3]) {
     for (int b = 0; b < g.n_diel; ++b) {
         const double* D = g.diel + 7 * b;
         if (p[0] >= D[0] && p[0] <= D[3] && p[1] >= D[1] && p[1] <= D[4] && p[2] >= D[2] &&
             p[2] <= D[5])
-            return D[6];
+            return g.dmat[b];
     }
-    if (g.n_layers <= 0) return 1.0;
+    if (g.n_layers <= 0) return 0;
     int li = 0;
     for (int l = 0; l < g.n_layers; ++l) {
         if (p[2] >= g.zlo[l]) li = l;
         else break;
     }
-    return g.leps[li];
+    return g.lmat[li];
+}
+
+// Cell-centre offsets (2i+1)/N - 1, rounded exactly as the CPU walk computes them.
+template <int N>
+DRWC_DEV void centre_offsets(double* tco) {
+    for (int i = threadIdx.x; i < N; i += blockDim.x)
+        tco[i] = dsub(ddiv(dadd(dmul(2.0, (double)i), 1.0), (double)N), 1.0);
 }
 
 template <int N>
-DRWC_DEV void voxelise(const DevGeom& g, const double c[3], double a, double* es) {
+DRWC_DEV void voxelise(const DevGeom& g, const double c[3], double a, const double* tco,
+                       uint8_t* mat) {
     for (int v = threadIdx.x; v < N * N * N; v += blockDim.x) {
         const int i = v % N, j = (v / N) % N, k = v / (N * N);
         double p[3];
-        p[0] = dadd(c[0], dmul(a, dsub(ddiv(dadd(dmul(2.0, (double)i), 1.0), (double)N), 1.0)));
-        p[1] = dadd(c[1], dmul(a, dsub(ddiv(dadd(dmul(2.0, (double)j), 1.0), (double)N), 1.0)));
-        p[2] = dadd(c[2], dmul(a, dsub(ddiv(dadd(dmul(2.0, (double)k), 1.0), (double)N), 1.0)));
-        es[v] = eps_at(g, p);
+        p[0] = dadd(c[0], dmul(a, tco[i]));
+        p[1] = dadd(c[1], dmul(a, tco[j]));
+        p[2] = dadd(c[2], dmul(a, tco[k]));
+        mat[v] = (uint8_t)mat_at(g, p);
     }
 }
+
+// Shared memory beyond the solver's: material ids, cell-centre offsets, the
+// palette and its pair-conductance tables.
+template <int N>
+struct WalkSmem {
+    static size_t bytes(int P) {
+        return Cube<N>::kSmemBytes + ((size_t)N * N * N + 15) / 16 * 16 + 8 * N + 8 * P +
+               8 * (size_t)P * P + 4 * (size_t)P * P + 16;
+    }
+};
 
 struct WalkState {
     double r[3];
@@ -192,21 +219,34 @@ struct WalkState {
 };
 
 template <int N>
-__global__ void __launch_bounds__(Cube<N>::NT)
-walk_kernel(DevGeom g, Gauss G, WalkParams P, long long walk0, long long nwalks,
+__global__ void __launch_bounds__(Cube<N>::NT, CubeTraits<N>::kMinBlocks)
+walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
             unsigned long long* __restrict__ next, unsigned long long* __restrict__ stats,
             int32_t* __restrict__ end_out,
             int32_t* __restrict__ hops_out, double* __restrict__ w_out,
-            double* __restrict__ scratch_e, double* __restrict__ scratch_y,
-            float* __restrict__ scratch_s) {
+            double* __restrict__ scratch_y, float* __restrict__ scratch_s) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ WalkState S;
     using D = Cube<N>;
     constexpr int M = 6 * D::NN;
     const CubeSmem<N> sm = CubeSmem<N>::carve(smem);
-    double* es = scratch_e + (size_t)blockIdx.x * D::NNN;
+    const int P = g.n_mat;
+    unsigned char* xs = smem + D::kSmemBytes;
+    uint8_t* mat = xs;
+    double* tco = reinterpret_cast<double*>(xs + ((size_t)D::NNN + 15) / 16 * 16);
+    double* pal = tco + N;
+    double* pair64 = pal + P;
+    float* pair32 = reinterpret_cast<float*>(pair64 + P * P);
+    for (int v = threadIdx.x; v < P; v += blockDim.x) pal[v] = g.pal[v];
+    for (int v = threadIdx.x; v < P * P; v += blockDim.x) {
+        pair64[v] = g.pair64[v];
+        pair32[v] = g.pair32[v];
+    }
+    centre_offsets<N>(tco);
+    const EpsPalette E{mat, pal, pair64, pair32, P};
     double* ys = scratch_y + (size_t)blockIdx.x * D::NNN;
     float* ss = scratch_s + (size_t)blockIdx.x * D::NNN;
+    __syncthreads();
     const int t = threadIdx.x;
     unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0;
     for (;;) {
@@ -217,8 +257,8 @@ walk_kernel(DevGeom g, Gauss G, WalkParams P, long long walk0, long long nwalks,
         const uint64_t w = (uint64_t)(walk0 + idx);
         // ---- start point on the Gaussian surface
         if (t == 0) {
-            const double2 u = philox_uniform2(P.seed, w, 0, 0);
-            const double2 v = philox_uniform2(P.seed, w, 0, 1);
+            const double2 u = philox_uniform2(W.seed, w, 0, 0);
+            const double2 v = philox_uniform2(W.seed, w, 0, 1);
             const double target = dmul(u.x, G.total);
             double run = 0.0;
             int f = 5;
@@ -248,8 +288,8 @@ walk_kernel(DevGeom g, Gauss G, WalkParams P, long long walk0, long long nwalks,
                 if (t == 0) {
                     S.a = d;
                     S.net = net;
-                    if (d < P.stop) S.done = 1;
-                    else if (S.hops >= P.max_hops) { S.done = 1; S.net = -1; }
+                    if (d < W.stop) S.done = 1;
+                    else if (S.hops >= W.max_hops) { S.done = 1; S.net = -1; }
                 }
             }
             __syncthreads();
@@ -258,15 +298,15 @@ walk_kernel(DevGeom g, Gauss G, WalkParams P, long long walk0, long long nwalks,
             const double a = S.a;
             const bool first = S.hops == 0;
             const int code = first ? S.code : DRWC_GFT;
-            voxelise<N>(g, c, a, es);
+            voxelise<N>(g, c, a, tco, mat);
             __syncthreads();
             FdmStats st;
-            cube_solve<N>(sm, es, ys, ss, code, P.prm, &st);
+            cube_solve<N>(sm, E, ys, ss, code, W.prm, &st);
             double* wv = reinterpret_cast<double*>(sm.stage());
-            for_each_panel<N>(es, ys, [&](int b, double v) { wv[b] = v; });
+            for_each_panel<N>(E, ys, [&](int b, double v) { wv[b] = v; });
             __syncthreads();
-            const double2 u = first ? philox_uniform2(P.seed, w, 0, 1)
-                                    : philox_uniform2(P.seed, w, (uint32_t)S.hops, 0);
+            const double2 u = first ? philox_uniform2(W.seed, w, 0, 1)
+                                    : philox_uniform2(W.seed, w, (uint32_t)S.hops, 0);
             const double ud = first ? u.y : u.x;
             double tot = 0.0;
             const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
@@ -280,7 +320,7 @@ walk_kernel(DevGeom g, Gauss G, WalkParams P, long long walk0, long long nwalks,
                 } else {
                     if (first) {
                         const double sg = wv[b] < 0.0 ? -1.0 : 1.0;
-                        const double eps_w = center_diel<N>(es, code);
+                        const double eps_w = center_diel<N>(E, code);
                         double om = dmul(-S.sgn_out, G.total);
                         om = dmul(om, eps_w);
                         om = dmul(om, tot);
@@ -357,8 +397,9 @@ __global__ void hop_sum_kernel(long long nw, const int32_t* __restrict__ hops,
 
 // ------------------------------------------------------------------ host side
 struct HostGeom {
-    std::vector<double> box, zlo, leps, diel;
-    std::vector<int> net, gstart, gitems;
+    std::vector<double> box, zlo, diel, pal, pair64;
+    std::vector<float> pair32;
+    std::vector<int> net, gstart, gitems, lmat, dmat;
     DevGeom dev{};
     void* dbuf = nullptr;
 };
@@ -399,7 +440,30 @@ static int upload_geom(drwc_ctx* ctx, const drwc_structure* s, HostGeom* h) {
         h->net[b] = s->boxes[b].net;
     }
     h->zlo.assign(s->layer_zlo, s->layer_zlo + s->n_layers);
-    h->leps.assign(s->layer_eps, s->layer_eps + s->n_layers);
+    // material palette: distinct permittivities of layers and blocks
+    h->pal.clear();
+    auto mat_of = [&](double e) {
+        for (size_t m = 0; m < h->pal.size(); ++m)
+            if (h->pal[m] == e) return (int)m;
+        h->pal.push_back(e);
+        return (int)h->pal.size() - 1;
+    };
+    h->lmat.resize(s->n_layers);
+    for (int l = 0; l < s->n_layers; ++l) h->lmat[l] = mat_of(s->layer_eps[l]);
+    if (s->n_layers == 0) mat_of(1.0);  // vacuum when no layer is given
+    h->dmat.resize(s->n_diel);
+    for (int d = 0; d < s->n_diel; ++d) h->dmat[d] = mat_of(s->diel[d].eps);
+    const int P = (int)h->pal.size();
+    if (P > kMaxMaterials) return DRWC_ERR_GEOMETRY;
+    h->pair64.resize((size_t)P * P);
+    h->pair32.resize((size_t)P * P);
+    for (int a = 0; a < P; ++a)
+        for (int b = 0; b < P; ++b) {
+            const double e1 = h->pal[a], e2 = h->pal[b];
+            h->pair64[a * P + b] = e1 * e2 / (e1 + e2);
+            const float f1 = (float)e1, f2 = (float)e2;
+            h->pair32[a * P + b] = f1 * f2 / (f1 + f2);
+        }
     h->diel.resize(7 * s->n_diel);
     for (int d = 0; d < s->n_diel; ++d) {
         for (int a = 0; a < 3; ++a) {
@@ -456,7 +520,10 @@ static int upload_geom(drwc_ctx* ctx, const drwc_structure* s, HostGeom* h) {
     auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
     const size_t o_box = take(h->box.size() * 8), o_net = take(h->net.size() * 4),
                  o_zlo = take(std::max<size_t>(1, h->zlo.size()) * 8),
-                 o_leps = take(std::max<size_t>(1, h->leps.size()) * 8),
+                 o_lmat = take(std::max<size_t>(1, h->lmat.size()) * 4),
+                 o_dmat = take(std::max<size_t>(1, h->dmat.size()) * 4),
+                 o_pal = take(h->pal.size() * 8), o_p64 = take(h->pair64.size() * 8),
+                 o_p32 = take(h->pair32.size() * 4),
                  o_diel = take(std::max<size_t>(1, h->diel.size()) * 8),
                  o_gs = take(h->gstart.size() * 4), o_gi = take(h->gitems.size() * 4);
     void* d = nullptr;
@@ -466,7 +533,11 @@ static int upload_geom(drwc_ctx* ctx, const drwc_structure* s, HostGeom* h) {
     std::memcpy(hb.data() + o_box, h->box.data(), h->box.size() * 8);
     std::memcpy(hb.data() + o_net, h->net.data(), h->net.size() * 4);
     if (!h->zlo.empty()) std::memcpy(hb.data() + o_zlo, h->zlo.data(), h->zlo.size() * 8);
-    if (!h->leps.empty()) std::memcpy(hb.data() + o_leps, h->leps.data(), h->leps.size() * 8);
+    if (!h->lmat.empty()) std::memcpy(hb.data() + o_lmat, h->lmat.data(), h->lmat.size() * 4);
+    if (!h->dmat.empty()) std::memcpy(hb.data() + o_dmat, h->dmat.data(), h->dmat.size() * 4);
+    std::memcpy(hb.data() + o_pal, h->pal.data(), h->pal.size() * 8);
+    std::memcpy(hb.data() + o_p64, h->pair64.data(), h->pair64.size() * 8);
+    std::memcpy(hb.data() + o_p32, h->pair32.data(), h->pair32.size() * 4);
     if (!h->diel.empty()) std::memcpy(hb.data() + o_diel, h->diel.data(), h->diel.size() * 8);
     std::memcpy(hb.data() + o_gs, h->gstart.data(), h->gstart.size() * 4);
     std::memcpy(hb.data() + o_gi, h->gitems.data(), h->gitems.size() * 4);
@@ -480,7 +551,12 @@ static int upload_geom(drwc_ctx* ctx, const drwc_structure* s, HostGeom* h) {
     g.box = (const double*)(base + o_box);
     g.net = (const int*)(base + o_net);
     g.zlo = (const double*)(base + o_zlo);
-    g.leps = (const double*)(base + o_leps);
+    g.lmat = (const int*)(base + o_lmat);
+    g.dmat = (const int*)(base + o_dmat);
+    g.pal = (const double*)(base + o_pal);
+    g.pair64 = (const double*)(base + o_p64);
+    g.pair32 = (const float*)(base + o_p32);
+    g.n_mat = (int)h->pal.size();
     g.diel = (const double*)(base + o_diel);
     for (int a = 0; a < 3; ++a) {
         g.encl_lo[a] = s->encl_lo[a];
@@ -537,22 +613,25 @@ static int gauss_build(const drwc_structure* s, const drwc_job_params* p, Gauss*
     return DRWC_OK;
 }
 
-struct WalkShape { int per_sm = 0; };
-
+// Resident CTAs per SM for a given palette size (the shared-memory request
+// grows with it); the attribute is set once for the largest palette.
 template <int N>
-static int walk_shape(WalkShape* s) {
-    static WalkShape cached;
-    if (!cached.per_sm) {
-        using D = Cube<N>;
+static int walk_shape(int P, int* per_sm) {
+    static bool attr = false;
+    static int cache[kMaxMaterials + 1] = {0};
+    if (!attr) {
         DRWC_CUDA_TRY(cudaFuncSetAttribute(walk_kernel<N>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)D::kSmemBytes));
-        int nb = 0;
-        DRWC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, walk_kernel<N>, D::NT,
-                                                                    D::kSmemBytes));
-        cached.per_sm = nb < 1 ? 1 : nb;
+                                           (int)WalkSmem<N>::bytes(kMaxMaterials)));
+        attr = true;
     }
-    *s = cached;
+    if (!cache[P]) {
+        int nb = 0;
+        DRWC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &nb, walk_kernel<N>, Cube<N>::NT, WalkSmem<N>::bytes(P)));
+        cache[P] = nb < 1 ? 1 : nb;
+    }
+    *per_sm = cache[P];
     return DRWC_OK;
 }
 
@@ -570,19 +649,19 @@ static int launch_walks(drwc_ctx* ctx, const HostGeom& hg, const Gauss& G, const
     return dispatch_N(P.N, [&](auto nc) -> int {
         constexpr int NC = decltype(nc)::value;
         using D = Cube<NC>;
-        WalkShape sh;
-        int rc = walk_shape<NC>(&sh);
+        const int nmat = hg.dev.n_mat;
+        int per_sm = 0;
+        int rc = walk_shape<NC>(nmat, &per_sm);
         if (rc) return rc;
-        const int grid = (int)std::min<long long>(nw, (long long)sh.per_sm * ctx->sm_count);
+        const int grid = (int)std::min<long long>(nw, (long long)per_sm * ctx->sm_count);
         void* scratch = nullptr;
-        rc = ws_get(ctx, WS_SCRATCH, (size_t)grid * D::NNN * 20, &scratch);
+        rc = ws_get(ctx, WS_SCRATCH, (size_t)grid * D::NNN * 12, &scratch);
         if (rc) return rc;
-        double* se = (double*)scratch;
-        double* sy = se + (size_t)grid * D::NNN;
+        double* sy = (double*)scratch;
         float* sf = (float*)(sy + (size_t)grid * D::NNN);
         DRWC_CUDA_TRY(cudaMemsetAsync(wb.counter, 0, 8 * sizeof(unsigned long long), ctx->stream));
-        walk_kernel<NC><<<grid, D::NT, D::kSmemBytes, ctx->stream>>>(
-            hg.dev, G, P, walk0, nw, wb.counter, wb.counter + 2, wb.end, wb.hops, wb.w, se, sy, sf);
+        walk_kernel<NC><<<grid, D::NT, WalkSmem<NC>::bytes(nmat), ctx->stream>>>(
+            hg.dev, G, P, walk0, nw, wb.counter, wb.counter + 2, wb.end, wb.hops, wb.w, sy, sf);
         return launch_check(ctx);
     });
 }
@@ -677,11 +756,14 @@ DRWC_API int drwc_job_create(drwc_ctx* ctx, const drwc_structure* s, const drwc_
     const ptrdiff_t shift = (unsigned char*)own - (unsigned char*)j->hg.dbuf;
     DevGeom& g = j->hg.dev;
     auto mv = [&](auto*& ptr) { ptr = (std::remove_reference_t<decltype(ptr)>)((const unsigned char*)ptr + shift); };
-    mv(g.box); mv(g.net); mv(g.zlo); mv(g.leps); mv(g.diel); mv(g.gstart); mv(g.gitems);
+    mv(g.box); mv(g.net); mv(g.zlo); mv(g.lmat); mv(g.dmat); mv(g.diel); mv(g.pal);
+    mv(g.pair64); mv(g.pair32); mv(g.gstart); mv(g.gitems);
     j->hg.dbuf = own;
     j->n_entries = s->n_nets + 1;
     j->h2d_bytes = (int64_t)(j->hg.box.size() * 8 + j->hg.net.size() * 4 + j->hg.zlo.size() * 8 +
-                             j->hg.leps.size() * 8 + j->hg.diel.size() * 8 +
+                             j->hg.lmat.size() * 4 + j->hg.dmat.size() * 4 +
+                             j->hg.pal.size() * 8 + j->hg.pair64.size() * 12 +
+                             j->hg.diel.size() * 8 +
                              j->hg.gstart.size() * 4 + j->hg.gitems.size() * 4);
     DRWC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     *out = j;
