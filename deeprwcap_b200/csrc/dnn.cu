@@ -90,7 +90,8 @@ query_kernel(int n, const float* __restrict__ layers, const float* __restrict__ 
              const int32_t* __restrict__ axis, uint64_t seed, uint64_t stream, FdmParams prm,
              double* __restrict__ scratch_e, double* __restrict__ scratch_y,
              float* __restrict__ scratch_s, float* __restrict__ out, int32_t* __restrict__ status) {
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char drwc_dyn_smem[];
+    unsigned char* smem = drwc_dyn_smem;
     __shared__ float lay[2 * kL], cub[7 * kC];
     using D = Cube<N>;
     const CubeSmem<N> sm = CubeSmem<N>::carve(smem);
@@ -111,7 +112,7 @@ query_kernel(int n, const float* __restrict__ layers, const float* __restrict__ 
             code = a == 0 ? DRWC_WVTX : a == 1 ? DRWC_WVTY : DRWC_WVTZ;
         }
         FdmStats st;
-        cube_solve<N>(sm, EpsGlobal{es}, ys, ss, code, prm, &st);
+        cube_solve<N>(EpsGlobal{es}, ys, ss, code, prm, &st);
         double* w = reinterpret_cast<double*>(sm.stage());  // 6N^2 doubles over p|cx|cy|cz
         for_each_panel<N>(EpsGlobal{es}, ys, [&](int b, double v) { w[b] = v; });
         __syncthreads();

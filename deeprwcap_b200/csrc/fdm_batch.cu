@@ -27,7 +27,8 @@ fdm_batch_kernel(int nsel, const int32_t* __restrict__ sel, const double* __rest
                  double* __restrict__ relres, int32_t* __restrict__ status, FdmParams prm,
                  double* __restrict__ scratch_y,
                  float* __restrict__ scratch_s) {
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char drwc_dyn_smem[];
+    unsigned char* smem = drwc_dyn_smem;
     using D = Cube<N>;
     const CubeSmem<N> sm = CubeSmem<N>::carve(smem);
     double* ys = scratch_y + (size_t)blockIdx.x * D::NNN;
@@ -37,7 +38,7 @@ fdm_batch_kernel(int nsel, const int32_t* __restrict__ sel, const double* __rest
         const double* e = eps + eps_off[c];
         const int cd = code ? code[c] : DRWC_GFT;
         FdmStats st;
-        cube_solve<N>(sm, EpsGlobal{e}, ys, ss, cd, prm, &st);
+        cube_solve<N>(EpsGlobal{e}, ys, ss, cd, prm, &st);
         double* o = out + out_off[c];
         if (st.status == 2) {
             for (int b = threadIdx.x; b < 6 * D::NN; b += blockDim.x) o[b] = 0.0;

@@ -9,8 +9,9 @@
 // update_ek (:137-274).
 //
 // One CTA owns one cube; the whole FP32 iteration state stays on chip:
-//   thread t < N^2 owns the z-column (i, j) = (t % N, t / N) and keeps its
-//   N cells of r, x and q = K~p in registers (fully unrolled over k);
+//   each z-column (i, j) is owned by one thread, or by two threads that own
+//   its lower and upper halves (N^2 or 2N^2 threads); a thread keeps its
+//   cells of r, x, q = K~p (and p) in registers (fully unrolled over k);
 //   shared memory holds the search direction p and the three scaled link
 //   coefficients cx, cy, cz (cell -> +x/+y/+z neighbour), each padded with N
 //   zero guard cells on both ends so the 7-point stencil needs no branches:
@@ -43,11 +44,22 @@ struct FdmStats {
     int status;      // 0 converged, 1 not converged, 2 invalid permittivity
 };
 
+#ifndef DRWC_CG_ONE_REDUCTION
+#define DRWC_CG_ONE_REDUCTION 0
+#endif
+#ifndef DRWC_SPLIT_MAX_N
+#define DRWC_SPLIT_MAX_N 0
+#endif
+
 template <int N>
 struct Cube {
     static constexpr int NN = N * N;
     static constexpr int NNN = N * N * N;
-    static constexpr int NT = ((NN + 31) / 32) * 32;  // threads per CTA
+    // Threads per z-column: two (each owning half of the column) while 2*N^2
+    // threads fit in a CTA, else one.
+    static constexpr int SPLIT = (N <= DRWC_SPLIT_MAX_N && 2 * NN <= 1024) ? 2 : 1;
+    static constexpr int KH = (N + SPLIT - 1) / SPLIT;    // cells per thread
+    static constexpr int NT = ((SPLIT * NN + 31) / 32) * 32;  // threads per CTA
     static constexpr int NW = NT / 32;
     static constexpr int PAD = N;                      // guard cells per side
     static constexpr int LEN = NNN + 2 * PAD;
@@ -106,6 +118,28 @@ DRWC_DEV float block_sum_f(float v, double* red, int slot) {
 #pragma unroll
     for (int w = 0; w < NW; ++w) s += red[slot * NW + w];
     return (float)s;
+}
+
+// Two sums in one barrier (slot s uses red[2*s*NW .. 2*s*NW + 2*NW)).
+template <int NW>
+DRWC_DEV float2 block_sum_f2(float a, float b, double* red, int slot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    float2* r2 = reinterpret_cast<float2*>(red) + slot * NW;
+    if (lane == 0) r2[warp] = make_float2(a, b);
+    __syncthreads();
+    float sa = 0.f, sb = 0.f;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) {
+        const float2 v = r2[w];
+        sa += v.x;
+        sb += v.y;
+    }
+    return make_float2(sa, sb);
 }
 
 template <int NW>
@@ -249,8 +283,8 @@ DRWC_DEV double center_diel(const E& eps, int code) {
 #ifndef DRWC_PREGS_MAX_N
 #define DRWC_PREGS_MAX_N 16
 #endif
-#ifndef DRWC_MIN_BLOCKS_256
-#define DRWC_MIN_BLOCKS_256 2
+#ifndef DRWC_MIN_BLOCKS_SMALL
+#define DRWC_MIN_BLOCKS_SMALL 2
 #endif
 
 template <int N>
@@ -258,8 +292,9 @@ struct CubeTraits {
     // Keep the thread's own column of p in registers too (saves three shared
     // loads per cell and iteration) when the register file allows it.
     static constexpr bool kPRegs = N <= DRWC_PREGS_MAX_N;
-    // Resident CTAs per SM the register allocation is sized for.
-    static constexpr int kMinBlocks = Cube<N>::NT <= 256 ? DRWC_MIN_BLOCKS_256 : 1;
+    // Resident CTAs per SM the register allocation is sized for (N <= 16;
+    // larger cubes run one CTA per SM, bounded by shared memory).
+    static constexpr int kMinBlocks = N <= 16 ? DRWC_MIN_BLOCKS_SMALL : 1;
 };
 
 // --------------------------------------------------------------- the solver
@@ -268,18 +303,36 @@ struct CubeTraits {
 // ss:   N^3 floats of global scratch (the Jacobi scale S).
 // On return (all threads) ys holds y and the stats are filled; shared memory
 // p/cx/cy/cz are free for the caller.
+#ifndef DRWC_SOLVE_INLINE
+#define DRWC_SOLVE_INLINE 0
+#endif
+#if DRWC_SOLVE_INLINE
+#define DRWC_SOLVE_ATTR __device__ __forceinline__
+#else
+#define DRWC_SOLVE_ATTR __device__ __noinline__
+#endif
+
+// The kernel's dynamic shared memory; the cube's arrays sit at its start.
+// Carving them from this symbol (not from pointers handed in) lets the
+// compiler address them as shared memory.
+extern __shared__ __align__(128) unsigned char drwc_dyn_smem[];
+
 template <int N, class E>
-__device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const E eps,
-                                        double* __restrict__ ys, float* __restrict__ ss, int code,
-                                        const FdmParams& prm, FdmStats* st) {
+DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __restrict__ ss,
+                                int code, const FdmParams& prm, FdmStats* st) {
+    const CubeSmem<N> sm = CubeSmem<N>::carve(drwc_dyn_smem);
     using D = Cube<N>;
     constexpr int NN = D::NN;
     constexpr int NW = D::NW;
+    constexpr int KH = D::KH;
     constexpr bool PR = CubeTraits<N>::kPRegs;
     const int t = threadIdx.x;
-    const bool active = t < NN;
-    const int i = t % N, j = t / N;
-    const int base = active ? t : 0;
+    const bool active = t < D::SPLIT * NN;
+    const int col = active ? t % NN : 0;
+    const int i = col % N, j = col / N;
+    const int k0 = active ? (t / NN) * KH : 0;       // first k of this thread's cells
+    const int kend = active ? min(k0 + KH, N) : 0;    // one past the last k
+    auto own = [&](int kk) { return k0 + kk < kend; };
 
     // ---- setup 1: validity, Jacobi scale S = diag(K)^-1/2 (FP32), y = 0,
     //      guards zeroed, right-hand side.
@@ -292,11 +345,11 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const E eps,
     }
     build_rhs<N>(eps, code, sm);
     __syncthreads();
-    if (active) {
+    {
         bool bad = false;
 #pragma unroll 1
-        for (int k = 0; k < N; ++k) {
-            const int c = base + k * NN;
+        for (int k = k0; k < kend; ++k) {
+            const int c = col + k * NN;
             bad |= !eps.valid(c);
             const float ec = eps.e32(c);
             float d = 0.f;
@@ -317,35 +370,34 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const E eps,
         return;
     }
     // ---- setup 2: scaled link coefficients cx/cy/cz = g * S_p * S_q.
-    if (active) {
 #pragma unroll 1
-        for (int k = 0; k < N; ++k) {
-            const int c = base + k * NN;
-            const float sc = ss[c];
-            float vx = 0.f, vy = 0.f, vz = 0.f;
-            if (i + 1 < N) vx = eps.g32(c, c + 1) * sc * ss[c + 1];
-            if (j + 1 < N) vy = eps.g32(c, c + N) * sc * ss[c + N];
-            if (k + 1 < N) vz = eps.g32(c, c + NN) * sc * ss[c + NN];
-            sm.cx[c] = vx; sm.cy[c] = vy; sm.cz[c] = vz;
-        }
+    for (int k = k0; k < kend; ++k) {
+        const int c = col + k * NN;
+        const float sc = ss[c];
+        float vx = 0.f, vy = 0.f, vz = 0.f;
+        if (i + 1 < N) vx = eps.g32(c, c + 1) * sc * ss[c + 1];
+        if (j + 1 < N) vy = eps.g32(c, c + N) * sc * ss[c + N];
+        if (k + 1 < N) vz = eps.g32(c, c + NN) * sc * ss[c + NN];
+        sm.cx[c] = vx; sm.cy[c] = vy; sm.cz[c] = vz;
     }
     // ||e|| (FP64) from the rhs table
     double enorm2 = 0.0;
     const int nrhs = sm.flags[0];
-    for (int q = 0; q < nrhs; ++q) enorm2 += sm.rhs_val[q] * sm.rhs_val[q];
+    for (int v = 0; v < nrhs; ++v) enorm2 += sm.rhs_val[v] * sm.rhs_val[v];
     const double enorm = sqrt(enorm2);
 
-    float r[N], x[N], q[N], pr[PR ? N : 1];
+    float r[KH], x[KH], q[KH], pr[(PR || DRWC_CG_ONE_REDUCTION) ? KH : 1];
     // Sweep 0: y = 0, so e - K y = e (non-zero only at the centre source).
-    if (active) {
 #pragma unroll
-        for (int k = 0; k < N; ++k) r[k] = 0.f;
+    for (int kk = 0; kk < KH; ++kk) r[kk] = 0.f;
+    if (active) {
         for (int v = 0; v < nrhs; ++v) {
             const int cell = sm.rhs_idx[v];
-            if (cell % NN == base) {
+            if (cell % NN == col) {
 #pragma unroll
-                for (int k = 0; k < N; ++k)
-                    if (cell / NN == k) r[k] = (float)((double)ss[cell] * sm.rhs_val[v]);
+                for (int kk = 0; kk < KH; ++kk)
+                    if (own(kk) && cell / NN == k0 + kk)
+                        r[kk] = (float)((double)ss[cell] * sm.rhs_val[v]);
             }
         }
     }
@@ -359,17 +411,75 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const E eps,
         //      the target (no deeper than inner_tol per sweep).
         float rr = 0.f;
 #pragma unroll
-        for (int k = 0; k < N; ++k) {
-            x[k] = 0.f;
-            if (active) {
-                sm.p[base + k * NN] = r[k];
-                if constexpr (PR) pr[k] = r[k];
-                rr += r[k] * r[k];
+        for (int kk = 0; kk < KH; ++kk) {
+            x[kk] = 0.f;
+            if (own(kk)) {
+                sm.p[col + (k0 + kk) * NN] = r[kk];
+                rr += r[kk] * r[kk];
             } else {
-                r[k] = 0.f;
-                if constexpr (PR) pr[k] = 0.f;
+                r[kk] = 0.f;
+            }
+            if constexpr (PR) pr[kk] = r[kk];
+        }
+#if DRWC_CG_ONE_REDUCTION
+        // Chronopoulos-Gear CG: one fused reduction (r.r, w.r) and two
+        // barriers per iteration; p and s = K~p live only in registers and
+        // the stencil runs on r, which is the vector shared through smem.
+        (void)rr;
+        float sv[KH], gamma_old = 1.f, alpha_old = 1.f, stop2 = 0.f;
+        int it = 0;
+#pragma unroll 1
+        for (it = 0; it <= prm.max_inner; ++it) {
+            __syncthreads();  // r published
+            float gam = 0.f, del = 0.f;
+            if (active) {
+                float rm = k0 > 0 ? sm.p[col + (k0 - 1) * NN] : 0.f;
+                float czm = k0 > 0 ? sm.cz[col + (k0 - 1) * NN] : 0.f;
+                float rc = r[0];
+#pragma unroll
+                for (int kk = 0; kk < KH; ++kk) {
+                    const int k = k0 + kk;
+                    const int c = col + k * NN;
+                    float rn;
+                    if (kk + 1 < KH) rn = r[(kk + 1) % KH];
+                    else rn = (k + 1 < N) ? sm.p[c + NN] : 0.f;
+                    if (own(kk)) {
+                        const float czc = sm.cz[c];
+                        const float nb = sm.cx[c - 1] * sm.p[c - 1] + sm.cx[c] * sm.p[c + 1] +
+                                         sm.cy[c - N] * sm.p[c - N] + sm.cy[c] * sm.p[c + N] +
+                                         czm * rm + czc * rn;
+                        q[kk] = rc - nb;  // w = K~ r
+                        gam += rc * rc;
+                        del += q[kk] * rc;
+                        czm = czc;
+                    } else {
+                        q[kk] = 0.f;
+                    }
+                    rm = rc; rc = rn;
+                }
+            }
+            const float2 gd = block_sum_f2<NW>(gam, del, sm.red, it & 1);
+            if (it == 0) {
+                const float want = fmaxf(prm.inner_tol, (float)(0.5 * prm.tol / relres));
+                stop2 = gd.x * want * want;
+            }
+            if (gd.x <= stop2 || it == prm.max_inner) break;
+            const float beta = it == 0 ? 0.f : gd.x / gamma_old;
+            const float alpha = gd.x / (gd.y - beta * gd.x / alpha_old);
+            gamma_old = gd.x;
+            alpha_old = alpha;
+#pragma unroll
+            for (int kk = 0; kk < KH; ++kk) {
+                if (own(kk)) {
+                    pr[kk] = (it == 0 ? 0.f : beta * pr[kk]) + r[kk];
+                    sv[kk] = (it == 0 ? 0.f : beta * sv[kk]) + q[kk];
+                    x[kk] += alpha * pr[kk];
+                    r[kk] -= alpha * sv[kk];
+                    sm.p[col + (k0 + kk) * NN] = r[kk];
+                }
             }
         }
+#else
         rr = block_sum_f<NW>(rr, sm.red, 1);  // barrier also publishes p
         const float want = fmaxf(prm.inner_tol, (float)(0.5 * prm.tol / relres));
         const float stop2 = rr * want * want;
@@ -379,85 +489,99 @@ __device__ __noinline__ void cube_solve(const CubeSmem<N>& sm, const E eps,
             // q = K~ p  (K~_pp = 1)
             float pq = 0.f;
             if (active) {
-                float pm = 0.f, czm = 0.f;
-                float pc = PR ? pr[0] : sm.p[base];
+                // z-neighbours across the split come from shared memory
+                float pm = k0 > 0 ? sm.p[col + (k0 - 1) * NN] : 0.f;
+                float czm = k0 > 0 ? sm.cz[col + (k0 - 1) * NN] : 0.f;
+                float pc;
+                if constexpr (PR) pc = pr[0];
+                else pc = sm.p[col + k0 * NN];
 #pragma unroll
-                for (int k = 0; k < N; ++k) {
-                    const int c = base + k * NN;
+                for (int kk = 0; kk < KH; ++kk) {
+                    const int k = k0 + kk;
+                    const int c = col + k * NN;
                     float pn;
-                    if constexpr (PR) pn = (k + 1 < N) ? pr[(k + 1) % N] : 0.f;
-                    else pn = (k + 1 < N) ? sm.p[c + NN] : 0.f;
-                    const float czc = sm.cz[c];
-                    const float nb = sm.cx[c - 1] * sm.p[c - 1] + sm.cx[c] * sm.p[c + 1] +
-                                     sm.cy[c - N] * sm.p[c - N] + sm.cy[c] * sm.p[c + N] +
-                                     czm * pm + czc * pn;
-                    q[k] = pc - nb;
-                    pq += pc * q[k];
-                    pm = pc; pc = pn; czm = czc;
+                    if constexpr (PR) {
+                        if (kk + 1 < KH) pn = pr[(kk + 1) % KH];
+                        else pn = (k + 1 < N) ? sm.p[c + NN] : 0.f;
+                    } else {
+                        pn = (k + 1 < N) ? sm.p[c + NN] : 0.f;
+                    }
+                    if (own(kk)) {
+                        const float czc = sm.cz[c];
+                        const float nb = sm.cx[c - 1] * sm.p[c - 1] + sm.cx[c] * sm.p[c + 1] +
+                                         sm.cy[c - N] * sm.p[c - N] + sm.cy[c] * sm.p[c + N] +
+                                         czm * pm + czc * pn;
+                        q[kk] = pc - nb;
+                        pq += pc * q[kk];
+                        czm = czc;
+                    } else {
+                        q[kk] = 0.f;
+                    }
+                    pm = pc; pc = pn;
                 }
             }
             pq = block_sum_f<NW>(pq, sm.red, 0);
             const float alpha = rr / pq;
             float rr2 = 0.f;
-            if (active) {
 #pragma unroll
-                for (int k = 0; k < N; ++k) {
-                    const int c = base + k * NN;
-                    if constexpr (PR) x[k] += alpha * pr[k];
-                    else x[k] += alpha * sm.p[c];
-                    r[k] -= alpha * q[k];
-                    rr2 += r[k] * r[k];
+            for (int kk = 0; kk < KH; ++kk) {
+                if (own(kk)) {
+                    if constexpr (PR) x[kk] += alpha * pr[kk];
+                    else x[kk] += alpha * sm.p[col + (k0 + kk) * NN];
+                    r[kk] -= alpha * q[kk];
+                    rr2 += r[kk] * r[kk];
                 }
             }
             rr2 = block_sum_f<NW>(rr2, sm.red, 1);
             const float beta = rr2 / rr;
             rr = rr2;
-            if (active) {
 #pragma unroll
-                for (int k = 0; k < N; ++k) {
-                    const int c = base + k * NN;
+            for (int kk = 0; kk < KH; ++kk) {
+                if (own(kk)) {
+                    const int c = col + (k0 + kk) * NN;
                     if constexpr (PR) {
-                        pr[k] = r[k] + beta * pr[k];
-                        sm.p[c] = pr[k];
+                        pr[kk] = r[kk] + beta * pr[kk];
+                        sm.p[c] = pr[kk];
                     } else {
-                        sm.p[c] = r[k] + beta * sm.p[c];
+                        sm.p[c] = r[kk] + beta * sm.p[c];
                     }
                 }
             }
             __syncthreads();
         }
+#endif
         total_inner += it;
         // ---- y += S d
-        if (active) {
 #pragma unroll
-            for (int k = 0; k < N; ++k) {
-                const int c = base + k * NN;
-                ys[c] += (double)ss[c] * (double)x[k];
+        for (int kk = 0; kk < KH; ++kk) {
+            if (own(kk)) {
+                const int c = col + (k0 + kk) * NN;
+                ys[c] += (double)ss[c] * (double)x[kk];
             }
         }
         __syncthreads();  // y of the neighbours visible
         // ---- FP64 residual r64 = e - K y, next inner rhs b = S r64 (FP32 regs)
         double rn2 = 0.0;
-        if (active) {
 #pragma unroll
-            for (int k = 0; k < N; ++k) {
-                const int c = base + k * NN;
-                const double ec = eps.e64(c);
-                const double yc = ys[c];
-                double diag = 0.0, off = 0.0;
-                if (i + 1 < N) { const double g = eps.g64(c, c + 1); diag += g; off += g * ys[c + 1]; } else diag += ec;
-                if (i > 0) { const double g = eps.g64(c, c - 1); diag += g; off += g * ys[c - 1]; } else diag += ec;
-                if (j + 1 < N) { const double g = eps.g64(c, c + N); diag += g; off += g * ys[c + N]; } else diag += ec;
-                if (j > 0) { const double g = eps.g64(c, c - N); diag += g; off += g * ys[c - N]; } else diag += ec;
-                if (k + 1 < N) { const double g = eps.g64(c, c + NN); diag += g; off += g * ys[c + NN]; } else diag += ec;
-                if (k > 0) { const double g = eps.g64(c, c - NN); diag += g; off += g * ys[c - NN]; } else diag += ec;
-                double e_c = 0.0;
-                for (int v = 0; v < nrhs; ++v)
-                    if (sm.rhs_idx[v] == c) e_c = sm.rhs_val[v];
-                const double r64 = e_c - (diag * yc - off);
-                rn2 += r64 * r64;
-                r[k] = (float)((double)ss[c] * r64);
-            }
+        for (int kk = 0; kk < KH; ++kk) {
+            if (!own(kk)) continue;
+            const int k = k0 + kk;
+            const int c = col + k * NN;
+            const double ec = eps.e64(c);
+            const double yc = ys[c];
+            double diag = 0.0, off = 0.0;
+            if (i + 1 < N) { const double g = eps.g64(c, c + 1); diag += g; off += g * ys[c + 1]; } else diag += ec;
+            if (i > 0) { const double g = eps.g64(c, c - 1); diag += g; off += g * ys[c - 1]; } else diag += ec;
+            if (j + 1 < N) { const double g = eps.g64(c, c + N); diag += g; off += g * ys[c + N]; } else diag += ec;
+            if (j > 0) { const double g = eps.g64(c, c - N); diag += g; off += g * ys[c - N]; } else diag += ec;
+            if (k + 1 < N) { const double g = eps.g64(c, c + NN); diag += g; off += g * ys[c + NN]; } else diag += ec;
+            if (k > 0) { const double g = eps.g64(c, c - NN); diag += g; off += g * ys[c - NN]; } else diag += ec;
+            double e_c = 0.0;
+            for (int v = 0; v < nrhs; ++v)
+                if (sm.rhs_idx[v] == c) e_c = sm.rhs_val[v];
+            const double r64 = e_c - (diag * yc - off);
+            rn2 += r64 * r64;
+            r[kk] = (float)((double)ss[c] * r64);
         }
         rn2 = block_sum_d<NW>(rn2, sm.red, 0);
         relres = sqrt(rn2) / enorm;

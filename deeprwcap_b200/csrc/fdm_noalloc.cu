@@ -38,7 +38,8 @@ fdm_noalloc_kernel(int ncubes, const double* __restrict__ eps, const int32_t* __
                    double* __restrict__ out, int32_t* __restrict__ iters,
                    int32_t* __restrict__ status, FdmParams prm,
                    unsigned char* __restrict__ scratch) {
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char drwc_dyn_smem[];
+    unsigned char* smem = drwc_dyn_smem;
     using D = Cube<N>;
     const CubeSmem<N> sm = CubeSmem<N>::carve(smem);
     double* ys = reinterpret_cast<double*>(scratch) + (size_t)blockIdx.x * D::NNN;
@@ -48,7 +49,7 @@ fdm_noalloc_kernel(int ncubes, const double* __restrict__ eps, const int32_t* __
         const double* e = eps + (size_t)c * D::NNN;
         const int cd = code ? code[c] : DRWC_GFT;
         FdmStats st;
-        cube_solve<N>(sm, EpsGlobal{e}, ys, ss, cd, prm, &st);
+        cube_solve<N>(EpsGlobal{e}, ys, ss, cd, prm, &st);
         double* o = out + (size_t)c * 6 * D::NN;
         if (st.status == 2) {
             for (int b = threadIdx.x; b < 6 * D::NN; b += blockDim.x) o[b] = 0.0;

@@ -225,7 +225,8 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
             int32_t* __restrict__ end_out,
             int32_t* __restrict__ hops_out, double* __restrict__ w_out,
             double* __restrict__ scratch_y, float* __restrict__ scratch_s) {
-    extern __shared__ __align__(128) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char drwc_dyn_smem[];
+    unsigned char* smem = drwc_dyn_smem;
     __shared__ WalkState S;
     using D = Cube<N>;
     constexpr int M = 6 * D::NN;
@@ -301,7 +302,7 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
             voxelise<N>(g, c, a, tco, mat);
             __syncthreads();
             FdmStats st;
-            cube_solve<N>(sm, E, ys, ss, code, W.prm, &st);
+            cube_solve<N>(E, ys, ss, code, W.prm, &st);
             double* wv = reinterpret_cast<double*>(sm.stage());
             for_each_panel<N>(E, ys, [&](int b, double v) { wv[b] = v; });
             __syncthreads();
