@@ -52,7 +52,11 @@ class DrwcError(RuntimeError):
 
 class FdmOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("inner_tol", C.c_double),
-                ("max_outer", C.c_int32), ("max_inner", C.c_int32)]
+                ("max_outer", C.c_int32), ("max_inner", C.c_int32),
+                ("warm_start", C.c_int32), ("reserved_", C.c_int32)]
+
+    def __init__(self, tol=1e-10, inner_tol=1e-5, max_outer=8, max_inner=0, warm_start=1):
+        super().__init__(tol, inner_tol, max_outer, max_inner, warm_start, 0)
 
 
 class Box(C.Structure):

@@ -51,6 +51,9 @@ DRWC_API int drwc_ctx_destroy(drwc_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     for (int i = 0; i < 8; ++i)
         if (ctx->ws[i]) cudaFree(ctx->ws[i]);
+    for (int n = 0; n <= DRWC_N_MAX; ++n)
+        for (int c = 0; c < 4; ++c)
+            if (ctx->warm[n][c]) cudaFree(ctx->warm[n][c]);
     if (ctx->pinned) cudaFreeHost(ctx->pinned);
     cudaStreamDestroy(ctx->stream);
     delete ctx;

@@ -159,9 +159,11 @@ static int query_launch(drwc_ctx* ctx, int n, const float* d_lay, const float* d
     double* se = (double*)scratch;
     double* sy = se + (size_t)grid * D::NNN;
     float* sf = (float*)(sy + (size_t)grid * D::NNN);
+    FdmParams prm = make_params(nullptr, N);
+    rc = warm_tables(ctx, N, prm.warm);
+    if (rc) return rc;
     query_kernel<N, GRAD><<<grid, D::NT, D::kSmemBytes, ctx->stream>>>(
-        n, d_lay, d_cub, d_axis, seed, stream, make_params(nullptr, N), se, sy, sf, d_out,
-        d_status);
+        n, d_lay, d_cub, d_axis, seed, stream, prm, se, sy, sf, d_out, d_status);
     return launch_check(ctx);
 }
 

@@ -87,6 +87,7 @@ FdmParams make_params(const drwc_fdm_opts* o, int N) {
     p.inner_tol = (float)(o->inner_tol > 0 ? o->inner_tol : d.inner_tol);
     p.max_outer = o->max_outer > 0 ? o->max_outer : d.max_outer;
     p.max_inner = o->max_inner > 0 ? o->max_inner : 4 * N * N;
+    for (int c = 0; c < 4; ++c) p.warm[c] = nullptr;  // set by the caller (warm_tables)
     return p;
 }
 
@@ -102,6 +103,8 @@ DRWC_API void drwc_fdm_opts_default(drwc_fdm_opts* opts) {
     opts->inner_tol = 1e-5;
     opts->max_outer = 8;
     opts->max_inner = 0;
+    opts->warm_start = 1;
+    opts->reserved_ = 0;
 }
 
 DRWC_API int drwc_fdm_solve_batch_device(drwc_ctx* ctx, int ncubes, const int32_t* N,
@@ -173,6 +176,10 @@ DRWC_API int drwc_fdm_solve_batch_device(drwc_ctx* ctx, int ncubes, const int32_
             double* sy = (double*)scratch;
             float* sf = (float*)(sy + (size_t)grid * D::NNN);
             FdmParams prm = make_params(opts, NC);
+            if (!opts || opts->warm_start) {
+                const int rw = warm_tables(ctx, NC, prm.warm);
+                if (rw) return rw;
+            }
             fdm_batch_kernel<NC><<<grid, D::NT, D::kSmemBytes, ctx->stream>>>(
                 g.count, d_sel + g.first, eps, d_eoff, code ? d_code : nullptr, d_ooff, out,
                 iters, sweeps, relres, status, prm, sy, sf);

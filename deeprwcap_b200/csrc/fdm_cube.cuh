@@ -34,6 +34,12 @@ struct FdmParams {
     float inner_tol;   // relative residual reduction per FP32 sweep
     int max_outer;     // FP64 refinement sweeps
     int max_inner;     // FP32 CG iterations per sweep
+    // Warm start per solver code (GFT, WVTZ, WVTX, WVTY): the cube solution
+    // x = eps .* y of the uniform-permittivity problem (N^3 doubles), or null
+    // for a cold start. ggft starts every solve from the same uniform
+    // solutions (bootstrap_solve, ggft_solver.cpp:83-135, used by
+    // solveWithGuess at :554-560).
+    const double* warm[4];
 };
 
 // Per-cube solve outcome.
@@ -165,6 +171,7 @@ DRWC_DEV double block_sum_d(double v, double* red, int slot) {
 struct EpsGlobal {
     const double* __restrict__ eps;
     DRWC_DEV double e64(int c) const { return eps[c]; }
+    DRWC_DEV double inv64(int c) const { return 1.0 / eps[c]; }
     DRWC_DEV float e32(int c) const { return (float)eps[c]; }
     DRWC_DEV double g64(int c, int q) const {
         const double a = eps[c], b = eps[q];
@@ -187,14 +194,26 @@ struct EpsGlobal {
 struct EpsPalette {
     const uint8_t* mat;     // N^3 material ids (shared memory)
     const double* pal;      // P permittivities (shared memory)
+    const double* palinv;   // P inverse permittivities
     const double* pair64;   // P x P conductances (shared memory)
     const float* pair32;    // P x P, FP32
     int P;
     DRWC_DEV double e64(int c) const { return pal[mat[c]]; }
+    DRWC_DEV double inv64(int c) const { return palinv[mat[c]]; }
     DRWC_DEV float e32(int c) const { return (float)pal[mat[c]]; }
     DRWC_DEV double g64(int c, int q) const { return pair64[mat[c] * P + mat[q]]; }
     DRWC_DEV float g32(int c, int q) const { return pair32[mat[c] * P + mat[q]]; }
     DRWC_DEV bool valid(int c) const { return true; }  // palette checked on the host
+};
+
+// EpsUniform: permittivity 1 everywhere (the warm-start bootstrap).
+struct EpsUniform {
+    DRWC_DEV double e64(int) const { return 1.0; }
+    DRWC_DEV double inv64(int) const { return 1.0; }
+    DRWC_DEV float e32(int) const { return 1.f; }
+    DRWC_DEV double g64(int, int) const { return 0.5; }
+    DRWC_DEV float g32(int, int) const { return 0.5f; }
+    DRWC_DEV bool valid(int) const { return true; }
 };
 
 // ------------------------------------------------------------ right-hand side
@@ -334,8 +353,9 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
     const int kend = active ? min(k0 + KH, N) : 0;    // one past the last k
     auto own = [&](int kk) { return k0 + kk < kend; };
 
-    // ---- setup 1: validity, Jacobi scale S = diag(K)^-1/2 (FP32), y = 0,
-    //      guards zeroed, right-hand side.
+    // ---- setup 1: validity, Jacobi scale S = diag(K)^-1/2 (FP32), y = the
+    //      warm start (or 0), guards zeroed, right-hand side.
+    const double* __restrict__ warm = prm.warm[code & 3];
     if (t == 0) sm.flags[1] = 0;
     for (int g = t; g < D::PAD; g += D::NT) {
         sm.p[-D::PAD + g] = 0.f; sm.p[D::NNN + g] = 0.f;
@@ -360,7 +380,7 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
             d += (k + 1 < N) ? eps.g32(c, c + NN) : ec;
             d += (k > 0) ? eps.g32(c, c - NN) : ec;
             ss[c] = rsqrtf(d);
-            ys[c] = 0.0;
+            ys[c] = warm ? warm[c] * eps.inv64(c) : 0.0;
         }
         if (bad) atomicOr(&sm.flags[1], 1);
     }
@@ -387,25 +407,62 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
     const double enorm = sqrt(enorm2);
 
     float r[KH], x[KH], q[KH], pr[(PR || DRWC_CG_ONE_REDUCTION) ? KH : 1];
-    // Sweep 0: y = 0, so e - K y = e (non-zero only at the centre source).
+    // FP64 residual r64 = e - K y into the next inner rhs b = S r64 (FP32
+    // registers); returns ||r64|| / ||e|| (all threads).
+    auto residual = [&]() -> double {
+        double rn2 = 0.0;
 #pragma unroll
-    for (int kk = 0; kk < KH; ++kk) r[kk] = 0.f;
-    if (active) {
-        for (int v = 0; v < nrhs; ++v) {
-            const int cell = sm.rhs_idx[v];
-            if (cell % NN == col) {
+        for (int kk = 0; kk < KH; ++kk) {
+            if (!own(kk)) { r[kk] = 0.f; continue; }
+            const int k = k0 + kk;
+            const int c = col + k * NN;
+            const double ec = eps.e64(c);
+            const double yc = ys[c];
+            double diag = 0.0, off = 0.0;
+            if (i + 1 < N) { const double g = eps.g64(c, c + 1); diag += g; off += g * ys[c + 1]; } else diag += ec;
+            if (i > 0) { const double g = eps.g64(c, c - 1); diag += g; off += g * ys[c - 1]; } else diag += ec;
+            if (j + 1 < N) { const double g = eps.g64(c, c + N); diag += g; off += g * ys[c + N]; } else diag += ec;
+            if (j > 0) { const double g = eps.g64(c, c - N); diag += g; off += g * ys[c - N]; } else diag += ec;
+            if (k + 1 < N) { const double g = eps.g64(c, c + NN); diag += g; off += g * ys[c + NN]; } else diag += ec;
+            if (k > 0) { const double g = eps.g64(c, c - NN); diag += g; off += g * ys[c - NN]; } else diag += ec;
+            double e_c = 0.0;
+            for (int v = 0; v < nrhs; ++v)
+                if (sm.rhs_idx[v] == c) e_c = sm.rhs_val[v];
+            const double r64 = e_c - (diag * yc - off);
+            rn2 += r64 * r64;
+            r[kk] = (float)((double)ss[c] * r64);
+        }
+        rn2 = block_sum_d<NW>(rn2, sm.red, 0);
+        return sqrt(rn2) / enorm;
+    };
+    int sweeps = 0;
+    double relres = 1.0;
+    if (warm) {
+        // sweep 0 from the warm start (y written above; neighbours visible
+        // after the barrier that follows the coefficient set-up)
+        __syncthreads();
+        relres = residual();
+        sweeps = 1;
+    } else {
+        // y = 0, so e - K y = e (non-zero only at the centre source)
 #pragma unroll
-                for (int kk = 0; kk < KH; ++kk)
-                    if (own(kk) && cell / NN == k0 + kk)
-                        r[kk] = (float)((double)ss[cell] * sm.rhs_val[v]);
+        for (int kk = 0; kk < KH; ++kk) r[kk] = 0.f;
+        if (active) {
+            for (int v = 0; v < nrhs; ++v) {
+                const int cell = sm.rhs_idx[v];
+                if (cell % NN == col) {
+#pragma unroll
+                    for (int kk = 0; kk < KH; ++kk)
+                        if (own(kk) && cell / NN == k0 + kk)
+                            r[kk] = (float)((double)ss[cell] * sm.rhs_val[v]);
+                }
             }
         }
     }
     int total_inner = 0, outer = 0;
-    double relres = 1.0;
-    int status = 1;
+    int status = relres <= prm.tol ? 0 : 1;
 #pragma unroll 1
-    for (outer = 0; outer < prm.max_outer; ++outer) {
+    for (outer = 0; status != 0 && outer < prm.max_outer; ++outer) {
         // ---- FP32 CG on K~ d = b, d in x[], starting from 0. The reduction
         //      it needs is set so this sweep brings ||e - K y|| to about half
         //      the target (no deeper than inner_tol per sweep).
@@ -560,36 +617,13 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
             }
         }
         __syncthreads();  // y of the neighbours visible
-        // ---- FP64 residual r64 = e - K y, next inner rhs b = S r64 (FP32 regs)
-        double rn2 = 0.0;
-#pragma unroll
-        for (int kk = 0; kk < KH; ++kk) {
-            if (!own(kk)) continue;
-            const int k = k0 + kk;
-            const int c = col + k * NN;
-            const double ec = eps.e64(c);
-            const double yc = ys[c];
-            double diag = 0.0, off = 0.0;
-            if (i + 1 < N) { const double g = eps.g64(c, c + 1); diag += g; off += g * ys[c + 1]; } else diag += ec;
-            if (i > 0) { const double g = eps.g64(c, c - 1); diag += g; off += g * ys[c - 1]; } else diag += ec;
-            if (j + 1 < N) { const double g = eps.g64(c, c + N); diag += g; off += g * ys[c + N]; } else diag += ec;
-            if (j > 0) { const double g = eps.g64(c, c - N); diag += g; off += g * ys[c - N]; } else diag += ec;
-            if (k + 1 < N) { const double g = eps.g64(c, c + NN); diag += g; off += g * ys[c + NN]; } else diag += ec;
-            if (k > 0) { const double g = eps.g64(c, c - NN); diag += g; off += g * ys[c - NN]; } else diag += ec;
-            double e_c = 0.0;
-            for (int v = 0; v < nrhs; ++v)
-                if (sm.rhs_idx[v] == c) e_c = sm.rhs_val[v];
-            const double r64 = e_c - (diag * yc - off);
-            rn2 += r64 * r64;
-            r[kk] = (float)((double)ss[c] * r64);
-        }
-        rn2 = block_sum_d<NW>(rn2, sm.red, 0);
-        relres = sqrt(rn2) / enorm;
-        if (relres <= prm.tol) { status = 0; ++outer; break; }
+        relres = residual();
+        ++sweeps;
+        if (relres <= prm.tol) status = 0;
     }
     st->status = status;
     st->iters = total_inner;
-    st->sweeps = outer;
+    st->sweeps = sweeps;
     st->relres = relres;
     __syncthreads();
 }

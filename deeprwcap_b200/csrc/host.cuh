@@ -24,6 +24,8 @@ struct drwc_ctx {
     // pinned host staging
     void* pinned = nullptr;
     size_t pinned_bytes = 0;
+    // uniform-permittivity solutions per N and solver code (warm starts)
+    double* warm[DRWC_N_MAX + 1][4] = {};
 };
 
 namespace drwc {
@@ -89,6 +91,10 @@ inline int launch_check(drwc_ctx* ctx) {
 }
 
 inline bool n_supported(int N) { return N >= DRWC_N_MIN && N <= DRWC_N_MAX; }
+
+// Fills warm[0..3] with the context's uniform-permittivity solutions for N
+// (computed on the device the first time they are asked for). warm.cu.
+int warm_tables(drwc_ctx* ctx, int N, const double* warm[4]);
 
 // Calls f(std::integral_constant<int, N>) for a runtime N in the supported set.
 template <class F>

@@ -201,7 +201,7 @@ DRWC_DEV void voxelise(const DevGeom& g, const double c[3], double a, const doub
 template <int N>
 struct WalkSmem {
     static size_t bytes(int P) {
-        return Cube<N>::kSmemBytes + ((size_t)N * N * N + 15) / 16 * 16 + 8 * N + 8 * P +
+        return Cube<N>::kSmemBytes + ((size_t)N * N * N + 15) / 16 * 16 + 8 * N + 16 * P +
                8 * (size_t)P * P + 4 * (size_t)P * P + 16;
     }
 };
@@ -236,15 +236,19 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
     uint8_t* mat = xs;
     double* tco = reinterpret_cast<double*>(xs + ((size_t)D::NNN + 15) / 16 * 16);
     double* pal = tco + N;
-    double* pair64 = pal + P;
+    double* palinv = pal + P;
+    double* pair64 = palinv + P;
     float* pair32 = reinterpret_cast<float*>(pair64 + P * P);
-    for (int v = threadIdx.x; v < P; v += blockDim.x) pal[v] = g.pal[v];
+    for (int v = threadIdx.x; v < P; v += blockDim.x) {
+        pal[v] = g.pal[v];
+        palinv[v] = 1.0 / g.pal[v];
+    }
     for (int v = threadIdx.x; v < P * P; v += blockDim.x) {
         pair64[v] = g.pair64[v];
         pair32[v] = g.pair32[v];
     }
     centre_offsets<N>(tco);
-    const EpsPalette E{mat, pal, pair64, pair32, P};
+    const EpsPalette E{mat, pal, palinv, pair64, pair32, P};
     double* ys = scratch_y + (size_t)blockIdx.x * D::NNN;
     float* ss = scratch_s + (size_t)blockIdx.x * D::NNN;
     __syncthreads();
@@ -684,6 +688,10 @@ static int prepare(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params
     P->stop = p->stop_dist;
     P->seed = p->seed;
     P->prm = make_params(&p->fdm, p->N);
+    if (p->fdm.warm_start) {
+        rc = warm_tables(ctx, p->N, P->prm.warm);
+        if (rc) return rc;
+    }
     return DRWC_OK;
 }
 

@@ -109,7 +109,8 @@ class GgftSolver:
 
 
 def fdm_solve_batch(eps_list_or_batch, code=None, tol: float = 1e-10, inner_tol: float = 1e-5,
-                    ctx: Context | None = None, max_outer: int = 8, max_inner: int = 0):
+                    ctx: Context | None = None, max_outer: int = 8, max_inner: int = 0,
+                    warm_start: bool = True):
     """Solve many cubes (host arrays). Accepts a list of [N,N,N] arrays or a
     ``workloads.MixedBatch``. Returns (list of 6N^2 arrays, iters, relres,
     status)."""
@@ -131,7 +132,7 @@ def fdm_solve_batch(eps_list_or_batch, code=None, tol: float = 1e-10, inner_tol:
     codes = None
     if code is not None:
         codes = np.ascontiguousarray(np.broadcast_to(np.asarray(code, dtype=np.int32), (n,)))
-    opts = abi.FdmOpts(tol, inner_tol, max_outer, max_inner)
+    opts = abi.FdmOpts(tol, inner_tol, max_outer, max_inner, 1 if warm_start else 0)
     iters = np.zeros(n, dtype=np.int32)
     relres = np.zeros(n)
     status = np.zeros(n, dtype=np.int32)

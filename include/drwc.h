@@ -89,10 +89,13 @@ DRWC_API int drwc_ctx_launch_count(drwc_ctx* ctx, int64_t* count_out);
  * refinement loop stops at; inner_tol is the relative reduction each FP32 PCG
  * sweep aims for. */
 typedef struct drwc_fdm_opts {
-    double tol;        /* default 1e-10 */
-    double inner_tol;  /* default 1e-5 */
-    int32_t max_outer; /* FP64 refinement sweeps, default 8 */
-    int32_t max_inner; /* FP32 PCG iterations per sweep, default 4 * N * N */
+    double tol;         /* default 1e-10 */
+    double inner_tol;   /* default 1e-5 */
+    int32_t max_outer;  /* FP64 refinement sweeps, default 8 */
+    int32_t max_inner;  /* FP32 PCG iterations per sweep, default 4 * N * N */
+    int32_t warm_start; /* start from the uniform-permittivity solution, as ggft's
+                           solveWithGuess (ggft_solver.cpp:554-560); default 1 */
+    int32_t reserved_;
 } drwc_fdm_opts;
 DRWC_API void drwc_fdm_opts_default(drwc_fdm_opts* opts);
 
