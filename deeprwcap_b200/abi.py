@@ -40,7 +40,7 @@ EXPORTS = [
     "drwc_fdm_solve_batch", "drwc_structure_construction", "drwc_transition_batch",
     "drwc_first_hop_batch", "drwc_job_params_default", "drwc_frw_run", "drwc_frw_walks",
     "drwc_job_create", "drwc_job_destroy", "drwc_job_walks_device", "drwc_job_h2d_bytes",
-    "drwc_fdm_solve_noalloc",
+    "drwc_fdm_solve_noalloc", "drwc_gemm_bf16",
 ]
 
 
@@ -137,6 +137,8 @@ def load():
     L.drwc_job_h2d_bytes.argtypes = [vp, C.POINTER(i64)]
     L.drwc_fdm_solve_noalloc.argtypes = [vp, C.c_int, C.c_int, vp, vp, C.POINTER(FdmOpts), vp,
                                          vp, vp]
+    L.drwc_gemm_bf16.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, i64, vp, i64, vp, i64, vp,
+                                 C.c_int, vp]
     _lib = L
     return L
 

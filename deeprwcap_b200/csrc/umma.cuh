@@ -1,0 +1,224 @@
+// Blackwell (sm_100a) tensor-core GEMM building block: C = A * B^T with A
+// [M, K] and B [N, K] in BF16, FP32 accumulation in tensor memory (TMEM).
+//
+// One CTA of 128 threads owns a 128 x BN tile of C. Operand tiles are
+// produced by the threads through loader functors (plain matrices or the
+// implicit-GEMM gathers of the 3-D convolutions) and written to shared memory
+// in the canonical K-major, no-swizzle UMMA layout: 8-row x 16-byte core
+// matrices, the two 8-element K halves of a 16-wide K step 128 B apart (LBO)
+// and consecutive 8-row groups 256 B apart (SBO). One thread issues
+// tcgen05.mma.cta_group::1.kind::f16 (M = 128, N = BN, K = 16 per
+// instruction) for each K step and commits to an mbarrier; two shared-memory
+// stages let the threads fill one while the tensor cores read the other. The
+// epilogue reads the accumulator with tcgen05.ld (32 lanes x 32 columns per
+// warp access) and hands rows to an epilogue functor.
+//
+// Bit layouts of the shared-memory and instruction descriptors follow the
+// public CUTLASS definitions (cute/arch/mma_sm100_desc.hpp: SmemDescriptor,
+// InstrDescriptor). Every wait is bounded: on timeout the kernel raises an
+// error flag, still waits (bounded) for its own MMAs and frees its TMEM.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace drwc {
+
+constexpr int kUmmaM = 128;
+constexpr int kUmmaBK = 64;                      // K per shared-memory stage (4 MMAs)
+constexpr uint32_t kWaitTicks = 1000000;         // try_wait suspend hint (ns)
+constexpr int kWaitRounds = 20000;               // => bounded wait of about 20 s
+
+DRWC_DEV uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, no swizzle, K-major canonical layout.
+DRWC_DEV uint64_t umma_smem_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);              // [0,14)  start address >> 4
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;    // [16,30) leading byte offset >> 4
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;    // [32,46) stride byte offset >> 4
+    d |= (uint64_t)1u << 46;                               // [46,48) descriptor version 1
+    return d;                                              // base offset 0, no swizzle
+}
+
+// Instruction descriptor: kind::f16, A = B = BF16, D = F32, both K-major.
+template <int BN>
+DRWC_DEV constexpr uint32_t umma_idesc_bf16() {
+    static_assert(BN % 16 == 0 && BN >= 16 && BN <= 256, "UMMA N for M=128");
+    return (1u << 4)                          // D format F32
+           | (1u << 7)                        // A format BF16
+           | (1u << 10)                       // B format BF16
+           | ((uint32_t)(BN >> 3) << 17)      // N >> 3
+           | ((uint32_t)(kUmmaM >> 4) << 24); // M >> 4
+}
+
+DRWC_DEV void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+// Bounded wait on phase `parity`; returns false on timeout.
+DRWC_DEV bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t a = smem_u32(bar);
+    for (int round = 0; round < kWaitRounds; ++round) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(a), "r"(parity), "r"(kWaitTicks)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+DRWC_DEV void umma_fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+DRWC_DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+DRWC_DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+DRWC_DEV void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+DRWC_DEV void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar)) : "memory");
+}
+
+DRWC_DEV void tmem_ld32(uint32_t taddr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Offset (bytes) of element (row, k) of a [rows x 64] stage tile in the
+// canonical layout: K step s = k/16 holds rows*32 bytes; inside it, row group
+// g = row/8 at g*256, K half h = (k%16)/8 at h*128, row-in-group at 16 B.
+DRWC_DEV uint32_t umma_tile_off(int row, int k, int rows) {
+    return (uint32_t)((k >> 4) * rows * 32 + (row >> 3) * 256 + ((k >> 3) & 1) * 128 +
+                      (row & 7) * 16 + (k & 7) * 2);
+}
+
+// Shared memory a CTA of umma_gemm<BN> needs.
+template <int BN>
+constexpr size_t umma_smem_bytes() {
+    return 2 * (size_t)(kUmmaM + BN) * kUmmaBK * 2 + 64;
+}
+
+// C tile = A[m0:m0+128, :] * B[n0:n0+BN, :]^T.
+//   la(row, k8, out) / lb(row, k8, out): write the 8 BF16 values of columns
+//   k8..k8+7 of operand row `row` (zeros outside the matrix) as a uint4.
+//   epi(row, col0, v[32]): consume 32 FP32 accumulator values of one row.
+// err: device flag set on a wait timeout.
+template <int BN, class LA, class LB, class EPI>
+DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, const LB& lb,
+                             const EPI& epi, int* err, unsigned char* smem) {
+    constexpr int STAGE_A = kUmmaM * kUmmaBK * 2, STAGE_B = BN * kUmmaBK * 2;
+    unsigned char* sa[2] = {smem, smem + STAGE_A + STAGE_B};
+    unsigned char* sb[2] = {smem + STAGE_A, smem + 2 * STAGE_A + STAGE_B};
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * (STAGE_A + STAGE_B));
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+    constexpr uint32_t TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+    const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+
+    if (t == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tslot)), "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tslot;
+
+    const int ktiles = (K + kUmmaBK - 1) / kUmmaBK;
+    uint32_t uses[2] = {0, 0};
+    bool ok = true;
+    for (int kt = 0; kt < ktiles; ++kt) {
+        const int s = kt & 1;
+        // the MMAs that last read this stage must be done before refilling it
+        if (kt >= 2) {
+            ok &= mbar_wait(&bar[s], (uses[s] - 1) & 1);
+        }
+        const int k0 = kt * kUmmaBK;
+        // A: 128 rows x 8 chunks of 8 BF16; B: BN rows x 8 chunks
+        for (int v = t; v < kUmmaM * 8; v += blockDim.x) {
+            const int row = v >> 3, ch = v & 7;
+            uint4 val;
+            la(m0 + row, k0 + ch * 8, &val);
+            *reinterpret_cast<uint4*>(sa[s] + umma_tile_off(row, ch * 8, kUmmaM)) = val;
+        }
+        for (int v = t; v < BN * 8; v += blockDim.x) {
+            const int row = v >> 3, ch = v & 7;
+            uint4 val;
+            lb(n0 + row, k0 + ch * 8, &val);
+            *reinterpret_cast<uint4*>(sb[s] + umma_tile_off(row, ch * 8, BN)) = val;
+        }
+        umma_fence_proxy_async();
+        __syncthreads();
+        if (t == 0) {
+            tc_fence_after();
+            const int ksteps = min(kUmmaBK, K - k0 + 15) / 16;  // K steps with data
+            for (int ks = 0; ks < ksteps && ks < kUmmaBK / 16; ++ks) {
+                const uint64_t da = umma_smem_desc(smem_u32(sa[s] + ks * kUmmaM * 32), 128, 256);
+                const uint64_t db = umma_smem_desc(smem_u32(sb[s] + ks * BN * 32), 128, 256);
+                umma_bf16(tmem, da, db, umma_idesc_bf16<BN>(), (kt > 0 || ks > 0) ? 1u : 0u);
+            }
+            umma_commit(&bar[s]);
+        }
+        uses[s] += 1;
+    }
+    // all MMAs done: the last commit covers every earlier MMA of this thread
+    {
+        const int s_last = (ktiles - 1) & 1;
+        ok &= mbar_wait(&bar[s_last], (uses[s_last] - 1) & 1);
+        if (ktiles >= 2) {
+            const int s_prev = ktiles & 1;
+            ok &= mbar_wait(&bar[s_prev], (uses[s_prev] - 1) & 1);
+        }
+    }
+    tc_fence_after();
+    if (!ok && err) atomicExch(err, 1);
+    // epilogue: warp w reads accumulator lanes (rows) 32w .. 32w+31
+    const int row = m0 + warp * 32 + lane;
+    for (int c = 0; c < BN; c += 32) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+        if (ok && row < M && n0 + c < N) epi(row, n0 + c, v);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TCOLS));
+    }
+}
+
+}  // namespace drwc

@@ -182,6 +182,16 @@ DRWC_API int drwc_first_hop_batch(drwc_ctx* ctx, int n, int N, const float* laye
                                   const float* cuboids, const int32_t* axis, uint64_t seed,
                                   uint64_t stream, float* out);
 
+/* ---- tensor-core GEMM (the learned transition kernels' building block) ----- */
+/* C[M,N] (FP32, row-major, ldc) = act(A[M,K] * B[N,K]^T + bias[N]) with A, B
+ * BF16 row-major (lda, ldb >= K), FP32 accumulation in tensor memory
+ * (tcgen05.mma, sm_100a). act: 0 none, 1 ReLU. bias and err_flag (an int the
+ * kernel sets to 1 if a bounded wait ran out) are nullable. Device pointers;
+ * async on the context stream. */
+DRWC_API int drwc_gemm_bf16(drwc_ctx* ctx, int M, int N, int K, const void* A, int64_t lda,
+                            const void* B, int64_t ldb, float* C, int64_t ldc, const float* bias,
+                            int act, int* err_flag);
+
 /* ---- structures and the FRW walk (the closed walker's role) --------------- */
 typedef struct drwc_box {
     double lo[3];
