@@ -41,6 +41,8 @@ EXPORTS = [
     "drwc_first_hop_batch", "drwc_job_params_default", "drwc_frw_run", "drwc_frw_walks",
     "drwc_job_create", "drwc_job_destroy", "drwc_job_walks_device", "drwc_job_h2d_bytes",
     "drwc_fdm_solve_noalloc", "drwc_gemm_bf16",
+    "drwc_net_create", "drwc_net_destroy", "drwc_net_param_count", "drwc_net_get_params",
+    "drwc_net_set_params", "drwc_net_gradients", "drwc_net_forward", "drwc_net_train_step",
 ]
 
 
@@ -139,6 +141,15 @@ def load():
                                          vp, vp]
     L.drwc_gemm_bf16.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, i64, vp, i64, vp, i64, vp,
                                  C.c_int, vp]
+    L.drwc_net_create.argtypes = [vp, C.c_int, C.c_uint64, C.POINTER(vp)]
+    L.drwc_net_destroy.argtypes = [vp]
+    L.drwc_net_param_count.argtypes = [vp, C.POINTER(i64)]
+    L.drwc_net_get_params.argtypes = [vp, vp]
+    L.drwc_net_set_params.argtypes = [vp, vp]
+    L.drwc_net_gradients.argtypes = [vp, vp]
+    L.drwc_net_forward.argtypes = [vp, C.c_int, vp, vp, vp]
+    L.drwc_net_train_step.argtypes = [vp, C.c_int, vp, vp, vp, C.c_float, C.c_float, C.c_float,
+                                      C.c_float, C.c_float, C.c_int, vp]
     _lib = L
     return L
 

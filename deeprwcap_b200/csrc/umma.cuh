@@ -222,3 +222,54 @@ DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, 
 }
 
 }  // namespace drwc
+
+namespace drwc {
+
+// Generic launchable GEMM kernel: one CTA per 128 x BN tile of C.
+template <int BN, class LA, class LB, class EPI>
+__global__ void __launch_bounds__(128) umma_kernel(int M, int N, int K, LA la, LB lb, EPI epi,
+                                                   int* err) {
+    extern __shared__ __align__(1024) unsigned char umma_smem[];
+    umma_gemm_tile<BN>(M, N, K, blockIdx.x * kUmmaM, blockIdx.y * BN, la, lb, epi, err,
+                       umma_smem);
+}
+
+// Loader of a row-major BF16 matrix [rows, cols] with leading dimension ld;
+// optional row map (operand row r reads matrix row map[r]).
+struct RowsBf16 {
+    const __nv_bfloat16* __restrict__ p;
+    int rows, cols;
+    int64_t ld;
+    const int* __restrict__ map;
+    DRWC_DEV void operator()(int r, int k8, uint4* out) const {
+        if (r >= rows || k8 >= cols) { *out = make_uint4(0, 0, 0, 0); return; }
+        const int64_t rr = map ? map[r] : r;
+        const __nv_bfloat16* src = p + rr * ld + k8;
+        if (k8 + 8 <= cols && ((reinterpret_cast<uintptr_t>(src) & 15) == 0)) {
+            *out = *reinterpret_cast<const uint4*>(src);
+            return;
+        }
+        __align__(16) __nv_bfloat16 tmp[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) tmp[i] = (k8 + i < cols) ? src[i] : __float2bfloat16(0.f);
+        *out = *reinterpret_cast<const uint4*>(tmp);
+    }
+};
+
+// Loader of the transpose of a row-major BF16 matrix S [K_rows, R_cols]:
+// operand row r, columns k8..k8+7 are S[k8..k8+7][r] (strided gather).
+struct ColsBf16 {
+    const __nv_bfloat16* __restrict__ p;
+    int rows, cols;      // operand shape (rows = S columns, cols = S rows)
+    int64_t ld;          // S leading dimension
+    DRWC_DEV void operator()(int r, int k8, uint4* out) const {
+        __align__(16) __nv_bfloat16 tmp[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            tmp[i] = (r < rows && k8 + i < cols) ? p[(int64_t)(k8 + i) * ld + r]
+                                                 : __float2bfloat16(0.f);
+        *out = *reinterpret_cast<const uint4*>(tmp);
+    }
+};
+
+}  // namespace drwc

@@ -375,3 +375,72 @@ class Job:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ learned
+NET_OUT = 1552
+NET_PANELS = 1536
+
+
+def _param_layout():
+    """Offsets of the flat FP32 parameter vector (mirrors ParamLayout in nn.cu)."""
+    names = [("w1", 16 * 27), ("b1", 16), ("w2", 32 * 432), ("b2", 32), ("w3", 64 * 864),
+             ("b3", 64), ("wd", NET_OUT * 512), ("bd", NET_OUT), ("wg", NET_PANELS * 512),
+             ("bg", NET_PANELS)]
+    off, lay = 0, {}
+    for name, n in names:
+        lay[name] = (off, n)
+        off += (n + 63) // 64 * 64
+    return lay, off
+
+
+class Net:
+    """The learned transition network (device-resident; see include/drwc.h)."""
+
+    def __init__(self, seed: int = 0, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(self.ctx.lib.drwc_net_create(self.ctx.h, 16, seed, C.byref(h)), "drwc_net_create")
+        self.h = h
+        n = C.c_int64()
+        check(self.ctx.lib.drwc_net_param_count(h, C.byref(n)), "drwc_net_param_count")
+        self.nparams = n.value
+
+    def get_params(self) -> np.ndarray:
+        out = np.zeros(self.nparams, dtype=np.float32)
+        check(self.ctx.lib.drwc_net_get_params(self.h, out.ctypes.data), "drwc_net_get_params")
+        return out
+
+    def set_params(self, p: np.ndarray) -> None:
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.nparams
+        check(self.ctx.lib.drwc_net_set_params(self.h, p.ctypes.data), "drwc_net_set_params")
+
+    def gradients(self) -> np.ndarray:
+        out = np.zeros(self.nparams, dtype=np.float32)
+        check(self.ctx.lib.drwc_net_gradients(self.h, out.ctypes.data), "drwc_net_gradients")
+        return out
+
+    def forward(self, X, O, G=None) -> None:
+        """X: [B, 4096] bfloat16 device tensor; O: [B, 1552] float32; G: [B, 1536]."""
+        check(self.ctx.lib.drwc_net_forward(self.h, int(X.shape[0]), ptr(X), ptr(O), ptr(G)),
+              "drwc_net_forward")
+
+    def train_step(self, X, T, TG=None, lr=1e-3, weight_decay=1e-10, clip=1.0, w_conf=0.1,
+                   w_grad=1.0, apply=True):
+        loss = (C.c_float * 3)()
+        check(self.ctx.lib.drwc_net_train_step(self.h, int(X.shape[0]), ptr(X), ptr(T), ptr(TG),
+                                               lr, weight_decay, clip, w_conf, w_grad,
+                                               1 if apply else 0, loss), "drwc_net_train_step")
+        return list(loss)
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.drwc_net_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

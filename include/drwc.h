@@ -192,6 +192,36 @@ DRWC_API int drwc_gemm_bf16(drwc_ctx* ctx, int M, int N, int K, const void* A, i
                             const void* B, int64_t ldb, float* C, int64_t ldc, const float* bias,
                             int act, int* err_flag);
 
+/* ---- learned transition kernels (N = 16) ----------------------------------- */
+/* A 3-D convolutional network on the cube's normalised permittivity (eps /
+ * max eps, BF16 [B, 16^3], cell order as above): encoder 1 -> 16 -> 32 -> 64
+ * channels (3^3 kernels, stride 2, pad 1, ReLU), Poisson head (1536 logits,
+ * softmax over the 6N^2 panels, plus a confidence output = predicted log10 KL
+ * divergence to the FDM Green's function) and gradient head (1536 WVTZ
+ * values, scaled). BF16 operands, FP32 accumulation on tcgen05 tensor cores,
+ * FP32 master weights. Architecture family of training_pytorch/src/
+ * architecture.py; trained here on FDM data the engine generates. */
+typedef struct drwc_net drwc_net;
+#define DRWC_NET_N 16
+#define DRWC_NET_OUT 1552      /* Poisson logits (1536) + confidence + padding */
+#define DRWC_NET_PANELS 1536
+DRWC_API int drwc_net_create(drwc_ctx* ctx, int N, uint64_t seed, drwc_net** out);
+DRWC_API int drwc_net_destroy(drwc_net* net);
+DRWC_API int drwc_net_param_count(drwc_net* net, int64_t* count);
+DRWC_API int drwc_net_get_params(drwc_net* net, float* host);
+DRWC_API int drwc_net_set_params(drwc_net* net, const float* host);
+DRWC_API int drwc_net_gradients(drwc_net* net, float* host);
+/* Device buffers: X [B, 4096] BF16 -> O [B, 1552] FP32, G [B, 1536] FP32
+ * (nullable). Async on the context stream. */
+DRWC_API int drwc_net_forward(drwc_net* net, int B, const void* X, float* O, float* G);
+/* One optimisation step (device buffers X, T = target Green's functions
+ * [B, 1536] rows summing to 1, TG = scaled gradient targets [B, 1536] or
+ * NULL); apply = 0 computes losses and gradients without updating.
+ * loss_out (host, 3): cross entropy, confidence MSE, gradient MSE. */
+DRWC_API int drwc_net_train_step(drwc_net* net, int B, const void* X, const float* T,
+                                 const float* TG, float lr, float weight_decay, float clip,
+                                 float w_conf, float w_grad, int apply, float* loss_out);
+
 /* ---- structures and the FRW walk (the closed walker's role) --------------- */
 typedef struct drwc_box {
     double lo[3];
