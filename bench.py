@@ -173,6 +173,68 @@ def traffic_from_profile():
     return None
 
 
+def learned_section(ctx, args):
+    """Train the network on engine-generated FDM data (untimed), then run the
+    same walks with the learned transition kernels and with the FDM per hop,
+    on the dense structure (3 orthogonal layers x 8 wires, 5 stratified
+    dielectric layers, 10 dielectric blocks), and time the network alone."""
+    import torch
+    from deeprwcap_b200 import engine, train
+    from deeprwcap_b200 import workloads as W
+    t0 = time.perf_counter()
+    X, T, TG = train.build_dataset(ctx, args.train_samples, seed=0, log=lambda *a: None)
+    Xt, Tt, TGt, Xv, Tv, TGv = train.split(X, T, TG)
+    net = engine.Net(seed=1, ctx=ctx)
+    tsec = train.train(net, Xt, Tt, TGt, epochs=args.train_epochs, batch=512, lr=1e-3,
+                       log=lambda *a: None)
+    ev = train.evaluate(net, Xv, Tv, TGv)
+    t_train = time.perf_counter() - t0
+    s = W.dense_stack(seed=3)
+    p = W.job_params_plain(N=16, seed=4242, tol=FDM_TOL)
+    nw = args.learned_walks
+    o = engine.learned_opts(slots=65536, conf_threshold=-1.5, audit_frac=0.01)
+    engine.frw_walks_learned(s, p, net, 50_000_000, 20000, o)  # warm-up
+    l0 = ctx.launches
+    e1, h1, w1, st = engine.frw_walks_learned(s, p, net, 0, nw, o)
+    l_launch = ctx.launches - l0
+    t1 = time.perf_counter()
+    e0, h0, w0 = engine.frw_walks(s, p, 0, nw, ctx=ctx)
+    t_fdm = time.perf_counter() - t1
+    cap = lambda e, w: [float(w[e == j].sum() / len(w)) for j in range(s.n_nets + 1)]
+    c1, c0 = cap(e1, w1), cap(e0, w0)
+    # the network alone on a fixed batch (tensor-core fraction)
+    B = 65536
+    dev = torch.device("cuda", ctx.device)
+    Xb = X[:B].contiguous()
+    O = torch.empty(B, engine.NET_OUT, device=dev)
+    torch.cuda.synchronize()
+    net.forward(Xb, O)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    reps = 5
+    ev0.record(stream)
+    for _ in range(reps):
+        ctx.lib.drwc_net_forward(net.h, B, Xb.data_ptr(), O.data_ptr(), None)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_nn = ev0.elapsed_time(ev1) / 1e3 / reps
+    flop = B * 2.0 * (512 * 16 * 27 + 64 * 32 * 432 + 8 * 64 * 864 + 512 * engine.NET_OUT)
+    _, bf16, src = peaks()
+    hl, hf = h1.sum() / st["seconds"], h0.sum() / t_fdm
+    return {"structure": "dense_stack (24 conductors, 5 layers, 10 blocks)", "walks": nw,
+            "train": {"samples": int(X.shape[0]), "epochs": args.train_epochs,
+                      "seconds": t_train, "train_step_seconds": tsec, **ev},
+            "learned_hops_per_s": hl, "fdm_hops_per_s": hf, "gain": hl / hf,
+            "net_hops": st["net_hops"], "fdm_hops": st["fdm_hops"],
+            "fallbacks": st["fallbacks"], "audits": st["audits"],
+            "audit_kl_mean": st["audit_kl"], "learned_launches": int(l_launch),
+            "cap_learned_fF": c1, "cap_fdm_fF": c0,
+            "self_rel_diff": abs(c1[0] - c0[0]) / abs(c0[0]),
+            "nn_forward": {"cubes": B, "seconds": t_nn, "tflops": flop / t_nn / 1e12,
+                           "peak_tflops": bf16, "frac": flop / t_nn / 1e12 / bf16,
+                           "peak_source": src}}
+
+
 def run_b200(args, world, rank, local):
     import torch
     from deeprwcap_b200 import engine
@@ -273,6 +335,12 @@ def run_b200(args, world, rank, local):
                     "cap_fF": [float(x) for x in r.cap],
                     "stderr_fF": [float(x) for x in r.stderr]}
 
+    # ---- learned transition kernels (network trained here on engine-generated
+    #      FDM data) vs the FDM walk on the dense 24-conductor structure
+    learned = None
+    if rank == 0 and not args.no_learned:
+        learned = learned_section(ctx, args)
+
     # ---- roofline of the dominant kernel (the per-hop FDM solve inside the walk kernel)
     hbm, bf16, src = peaks()
     NNN = N_CUBE ** 3
@@ -313,6 +381,7 @@ def run_b200(args, world, rank, local):
             "clocks": clk.summary(),
             "wall_s_timed": t_wall,
             "job": job_info,
+            "learned": learned,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -440,6 +509,10 @@ def main():
     ap.add_argument("--no-job", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="frw", choices=["frw", "fdm_batch"])
+    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--train-samples", type=int, default=1 << 20)
+    ap.add_argument("--train-epochs", type=int, default=4)
+    ap.add_argument("--learned-walks", type=int, default=1 << 20)
     ap.add_argument("--cubes", type=int, default=8192)
     args = ap.parse_args()
     world, rank, local = dist_init()

@@ -43,6 +43,8 @@ EXPORTS = [
     "drwc_fdm_solve_noalloc", "drwc_gemm_bf16",
     "drwc_net_create", "drwc_net_destroy", "drwc_net_param_count", "drwc_net_get_params",
     "drwc_net_set_params", "drwc_net_gradients", "drwc_net_forward", "drwc_net_train_step",
+    "drwc_frw_harvest", "drwc_records_voxelise", "drwc_cubes_random", "drwc_learned_opts_default",
+    "drwc_frw_walks_learned",
 ]
 
 
@@ -84,6 +86,11 @@ class JobParams(C.Structure):
                 ("c_ratio", C.c_double), ("min_walks", C.c_int64), ("max_walks", C.c_int64),
                 ("batch_walks", C.c_int64), ("max_hops", C.c_int32), ("pad_", C.c_int32),
                 ("seed", C.c_uint64), ("fdm", FdmOpts)]
+
+
+class LearnedOpts(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("conf_threshold", C.c_float), ("audit_frac", C.c_float),
+                ("use_graph", C.c_int32), ("max_steps", C.c_int32)]
 
 
 class JobResult(C.Structure):
@@ -150,6 +157,14 @@ def load():
     L.drwc_net_forward.argtypes = [vp, C.c_int, vp, vp, vp]
     L.drwc_net_train_step.argtypes = [vp, C.c_int, vp, vp, vp, C.c_float, C.c_float, C.c_float,
                                       C.c_float, C.c_float, C.c_int, vp]
+    L.drwc_frw_harvest.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams), i64, i64,
+                                   i32, vp, vp, C.POINTER(i32)]
+    L.drwc_records_voxelise.argtypes = [vp, C.POINTER(Structure), C.c_int, vp, vp, vp, vp]
+    L.drwc_cubes_random.argtypes = [vp, C.c_int, C.c_uint64, C.c_float, vp, vp]
+    L.drwc_learned_opts_default.argtypes = [C.POINTER(LearnedOpts)]
+    L.drwc_learned_opts_default.restype = None
+    L.drwc_frw_walks_learned.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams), vp,
+                                         C.POINTER(LearnedOpts), i64, i64, vp, vp, vp, vp]
     _lib = L
     return L
 

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "host.cuh"
+#include "nn.cuh"
 #include "umma_launch.cuh"
 
 namespace drwc {
@@ -490,10 +491,29 @@ static int net_heads(drwc_net* n, int rows, const int* rowmap, float* O, float* 
         rc = launch_umma<128>(ctx, rows_g, kNP, kFeat,
                               RowsBf16{n->a3, rows_g, kFeat, kFeat, rowmap_g},
                               RowsBf16{n->pb + n->L.wg, kNP, kFeat, kFeat, nullptr},
-                              EpiF32{G, n->p + n->L.bg, kNP, kNP, rowmap_g}, n->err);
+                              EpiF32{G, n->p + n->L.bg, kNP, kNP, nullptr}, n->err);
     }
     return rc;
 }
+
+int net_forward_locked(drwc_net* n, int B, const bf16* X, float* O, float* G) {
+    int rc = net_reserve(n, B);
+    if (rc) return rc;
+    rc = net_encode(n, B, X);
+    if (rc) return rc;
+    return net_heads(n, B, nullptr, O, G, nullptr, B);
+}
+
+int net_forward_mapped(drwc_net* n, int B, const bf16* X, float* O, float* G, const int* gmap,
+                       int rows_g) {
+    int rc = net_reserve(n, B);
+    if (rc) return rc;
+    rc = net_encode(n, B, X);
+    if (rc) return rc;
+    return net_heads(n, B, nullptr, O, G, gmap, rows_g);
+}
+
+drwc_ctx* net_context(drwc_net* n) { return n->ctx; }
 
 }  // namespace drwc
 
@@ -589,11 +609,7 @@ DRWC_API int drwc_net_forward(drwc_net* n, int B, const void* X, float* O, float
     if (B == 0) return DRWC_OK;
     std::lock_guard<std::mutex> lock(n->ctx->mu);
     DRWC_CUDA_TRY(cudaSetDevice(n->ctx->device));
-    int rc = net_reserve(n, B);
-    if (rc) return rc;
-    rc = net_encode(n, B, (const bf16*)X);
-    if (rc) return rc;
-    return net_heads(n, B, nullptr, O, G, nullptr, B);
+    return net_forward_locked(n, B, (const bf16*)X, O, G);
 }
 
 // One training step on a batch: X [B, 4096] BF16, T [B, 1536] FP32 target

@@ -1,0 +1,26 @@
+// Internal host API of the learned transition network (nn.cu) for the
+// learned walker (walker.cu). Not part of the C ABI.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "host.cuh"
+
+struct drwc_net;
+
+namespace drwc {
+
+// Scale of the gradient head: outputs are WVTZ surface values times this.
+constexpr float kGradScale = 64.0f;
+
+// Encoder + heads on B rows of X (BF16 [B, 4096], device): O [B, 1552] and G
+// [B, 1536] (either nullable). Launches on the net's context stream; the
+// caller holds the context lock.
+int net_forward_locked(drwc_net* n, int B, const __nv_bfloat16* X, float* O, float* G);
+// Same, with the gradient head only on rows_g feature rows (gmap[r] is the
+// encoder row of gradient output row r).
+int net_forward_mapped(drwc_net* n, int B, const __nv_bfloat16* X, float* O, float* G,
+                       const int* gmap, int rows_g);
+drwc_ctx* net_context(drwc_net* n);
+
+}  // namespace drwc

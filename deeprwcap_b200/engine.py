@@ -28,6 +28,17 @@ from . import abi
 from .abi import GFT, WVTX, WVTY, WVTZ, check, load, ptr
 
 
+def torch_ready() -> None:
+    """Order the library after the torch work queued so far: the library runs
+    on its context's own (non-blocking) stream, torch plumbing on torch's
+    current stream. Call before handing torch-produced device buffers to the
+    library; library outputs are ordered back by Context.synchronize()."""
+    import sys
+    torch = sys.modules.get("torch")
+    if torch is not None and torch.cuda.is_available() and torch.cuda.is_initialized():
+        torch.cuda.current_stream().synchronize()
+
+
 class Context:
     """One device context (stream + workspaces), as DNNSolver's constructor
     (dnn_solver.cpp:13-38)."""
@@ -355,6 +366,8 @@ class Job:
         self.h = h
 
     def walks_device(self, walk0: int, nwalks: int, end, hops, weight, stats=None) -> None:
+        """Async on the context stream; order torch work before it with
+        torch_ready() and read the outputs after Context.synchronize()."""
         check(self.ctx.lib.drwc_job_walks_device(self.h, int(walk0), int(nwalks), ptr(end),
                                                  ptr(hops), ptr(weight), ptr(stats)),
               "drwc_job_walks_device")
@@ -423,12 +436,15 @@ class Net:
 
     def forward(self, X, O, G=None) -> None:
         """X: [B, 4096] bfloat16 device tensor; O: [B, 1552] float32; G: [B, 1536]."""
+        torch_ready()
         check(self.ctx.lib.drwc_net_forward(self.h, int(X.shape[0]), ptr(X), ptr(O), ptr(G)),
               "drwc_net_forward")
+        self.ctx.synchronize()
 
     def train_step(self, X, T, TG=None, lr=1e-3, weight_decay=1e-10, clip=1.0, w_conf=0.1,
                    w_grad=1.0, apply=True):
         loss = (C.c_float * 3)()
+        torch_ready()
         check(self.ctx.lib.drwc_net_train_step(self.h, int(X.shape[0]), ptr(X), ptr(T), ptr(TG),
                                                lr, weight_decay, clip, w_conf, w_grad,
                                                1 if apply else 0, loss), "drwc_net_train_step")
@@ -444,3 +460,82 @@ class Net:
             self.close()
         except Exception:
             pass
+
+
+def learned_opts(**kw) -> "abi.LearnedOpts":
+    o = abi.LearnedOpts()
+    load().drwc_learned_opts_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def frw_walks_learned(structure, params, net: Net, walk0: int, nwalks: int, opts=None,
+                      ctx: Context | None = None):
+    """Walks with the learned transition kernels. Returns (end, hops, weight,
+    stats dict)."""
+    ctx = ctx or net.ctx
+    s = structure.to_c() if hasattr(structure, "to_c") else structure
+    end = np.zeros(nwalks, dtype=np.int32)
+    hops = np.zeros(nwalks, dtype=np.int32)
+    w = np.zeros(nwalks)
+    st = np.zeros(8)
+    o = opts or learned_opts()
+    rc = ctx.lib.drwc_frw_walks_learned(ctx.h, C.byref(s), C.byref(params), net.h, C.byref(o),
+                                        int(walk0), int(nwalks), end.ctypes.data,
+                                        hops.ctypes.data, w.ctypes.data, st.ctypes.data)
+    check(rc, "drwc_frw_walks_learned")
+    keys = ["net_hops", "fdm_hops", "fallbacks", "audits", "audit_kl", "steps", "seconds",
+            "walks"]
+    return end, hops, w, dict(zip(keys, st.tolist()))
+
+
+def harvest(structure, params, walk0: int, nwalks: int, cap: int, ctx: Context | None = None):
+    """Log the transition cubes of real walks: device tensors rec [n, 4] (centre,
+    half-width) and code [n] (solver code), n <= cap."""
+    import torch
+    ctx = ctx or default_context()
+    s = structure.to_c() if hasattr(structure, "to_c") else structure
+    dev = torch.device("cuda", ctx.device)
+    rec = torch.empty(cap, 4, dtype=torch.float64, device=dev)
+    code = torch.empty(cap, dtype=torch.int32, device=dev)
+    cnt = C.c_int32(0)
+    torch_ready()
+    check(ctx.lib.drwc_frw_harvest(ctx.h, C.byref(s), C.byref(params), int(walk0), int(nwalks),
+                                   int(cap), ptr(rec), ptr(code), C.byref(cnt)),
+          "drwc_frw_harvest")
+    return rec[:cnt.value], code[:cnt.value]
+
+
+def records_voxelise(structure, rec, code, X, eps64=None, ctx: Context | None = None):
+    ctx = ctx or default_context()
+    s = structure.to_c() if hasattr(structure, "to_c") else structure
+    torch_ready()
+    check(ctx.lib.drwc_records_voxelise(ctx.h, C.byref(s), int(rec.shape[0]), ptr(rec), ptr(code),
+                                        ptr(X), ptr(eps64)), "drwc_records_voxelise")
+
+
+def cubes_random(n: int, seed: int, X, eps64, noise_frac: float = 0.1,
+                 ctx: Context | None = None):
+    ctx = ctx or default_context()
+    torch_ready()
+    check(ctx.lib.drwc_cubes_random(ctx.h, int(n), seed, noise_frac, ptr(X), ptr(eps64)),
+          "drwc_cubes_random")
+    ctx.synchronize()
+
+
+def fdm_solve_device(ctx: Context, eps64, N: int, code, out, tol: float = 1e-8):
+    """Packed same-N device batch through the regular batched entry point:
+    eps64 [n, N^3] float64, code int or [n] int32 host array, out [n, 6N^2]."""
+    n = int(eps64.shape[0])
+    Ns = np.full(n, N, dtype=np.int32)
+    eoff = np.arange(n, dtype=np.int64) * N ** 3
+    ooff = np.arange(n, dtype=np.int64) * 6 * N * N
+    codes = np.ascontiguousarray(np.broadcast_to(np.asarray(code, dtype=np.int32), (n,)))
+    opts = abi.FdmOpts(tol, 1e-5, 8, 0, 1)
+    torch_ready()
+    check(ctx.lib.drwc_fdm_solve_batch_device(ctx.h, n, Ns.ctypes.data, eoff.ctypes.data,
+                                              ptr(eps64), codes.ctypes.data, C.byref(opts),
+                                              ooff.ctypes.data, ptr(out), None, None, None, None),
+          "drwc_fdm_solve_batch_device")
+    ctx.synchronize()

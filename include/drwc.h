@@ -297,6 +297,43 @@ DRWC_API int drwc_job_walks_device(drwc_job* job, int64_t walk0, int64_t nwalks,
 /* Bytes of structure data the job uploaded to the device. */
 DRWC_API int drwc_job_h2d_bytes(drwc_job* job, int64_t* bytes);
 
+/* Training data from the walks themselves: run walks [walk0, walk0+nwalks)
+ * of a job and log every hop's transition cube (centre xyz, half-width: 4
+ * doubles) and solver code into DEVICE arrays rec / code (up to cap hops);
+ * *count (host) receives the number logged. */
+DRWC_API int drwc_frw_harvest(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
+                              int64_t walk0, int64_t nwalks, int32_t cap, double* rec,
+                              int32_t* code, int32_t* count);
+/* Logged cubes -> network inputs X (BF16 [n, 4096], eps / max eps) and FP64
+ * permittivity (nullable), N = 16. First-hop cubes are voxelised in the frame
+ * where their gradient axis is z, so their gradient target is WVTZ. */
+DRWC_API int drwc_records_voxelise(drwc_ctx* ctx, const drwc_structure* s, int n,
+                                   const double* rec, const int32_t* code, void* X,
+                                   double* eps64);
+/* Random transition cubes (1-4 layers along a random axis, 0-2 boxes, eps in
+ * [2, 8], noise_frac of them with voxel noise), N = 16: X BF16 and FP64. */
+DRWC_API int drwc_cubes_random(drwc_ctx* ctx, int n, uint64_t seed, float noise_frac, void* X,
+                               double* eps64);
+
+typedef struct drwc_learned_opts {
+    int32_t slots;          /* walks in flight (default 65536) */
+    float conf_threshold;   /* route a hop to FDM when the predicted log10 KL exceeds it */
+    float audit_frac;       /* fraction of hops also solved by FDM (default 0.01) */
+    int32_t use_graph;      /* reserved (steps size their launches to the active slots) */
+    int32_t max_steps;
+} drwc_learned_opts;
+DRWC_API void drwc_learned_opts_default(drwc_learned_opts* o);
+/* Walks with the learned transition kernels (N = 16): per step, every slot's
+ * cube goes through the network on the tensor cores; low-confidence hops and
+ * audits go through the FDM solve. Records as drwc_frw_walks (host arrays).
+ * stats (host, 8 doubles, nullable): network hops, FDM hops, fallbacks,
+ * audits, mean audited KL(FDM || network), steps, seconds, walks finished. */
+DRWC_API int drwc_frw_walks_learned(drwc_ctx* ctx, const drwc_structure* s,
+                                    const drwc_job_params* p, drwc_net* net,
+                                    const drwc_learned_opts* opts, int64_t walk0, int64_t nwalks,
+                                    int32_t* end_net, int32_t* hops, double* weight,
+                                    double* stats);
+
 /* Run one extraction job (master row of the capacitance matrix) to
  * convergence on the device. Host structure in, host result out. */
 DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,

@@ -68,10 +68,10 @@ def test_forward_matches_reference(ctx):
         assert (got - ref).abs().max().item() <= 2e-2 * scale
 
 
-def test_backward_matches_autograd(ctx):
+@pytest.mark.parametrize("B", [64, 512])
+def test_backward_matches_autograd(ctx, B):
     import torch
     net = engine.Net(seed=5, ctx=ctx)
-    B = 64
     X = _inputs(B, 2)
     g = torch.Generator().manual_seed(0)
     T = torch.rand(B, 1536, generator=g) ** 4

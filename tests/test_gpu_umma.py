@@ -26,6 +26,7 @@ def test_gemm_bf16_matches_fp32_reference(ctx, M, N, K, act):
     Ad, Bd, bd = A.to(dev), B.to(dev), bias.to(dev)
     C = torch.full((M, N), float("nan"), device=dev)
     err = torch.zeros(1, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()  # buffers ready before the library's stream runs
     rc = ctx.lib.drwc_gemm_bf16(ctx.h, M, N, K, Ad.data_ptr(), K, Bd.data_ptr(), K, C.data_ptr(),
                                 N, bd.data_ptr(), act, err.data_ptr())
     assert rc == 0

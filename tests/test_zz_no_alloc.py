@@ -39,6 +39,7 @@ def test_noalloc_matches_regular_entry_point(N):
     eps_dev = torch.from_numpy(eps.reshape(-1).copy()).to(dev)
     code_dev = torch.from_numpy(codes).to(dev)
     ref = torch.zeros(n * 6 * N * N, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
     _regular(ctx, eps_dev, N, n, codes, ref, torch)
     ref = ref.cpu().numpy().reshape(n, -1)
     opts = abi.FdmOpts(1e-10, 1e-5, 8, 0)
@@ -46,6 +47,7 @@ def test_noalloc_matches_regular_entry_point(N):
         out = torch.full((n * 6 * N * N,), float("nan"), dtype=torch.float64, device=dev)
         iters = torch.full((n,), -1, dtype=torch.int32, device=dev)
         status = torch.full((n,), -1, dtype=torch.int32, device=dev)
+        torch.cuda.synchronize()  # buffers filled before the library's stream uses them
         rc = ctx.lib.drwc_fdm_solve_noalloc(ctx.h, N, n, eps_dev.data_ptr(), code_dev.data_ptr(),
                                             C.byref(opts), out.data_ptr(), iters.data_ptr(),
                                             status.data_ptr())
