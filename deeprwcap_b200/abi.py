@@ -45,6 +45,8 @@ EXPORTS = [
     "drwc_net_set_params", "drwc_net_gradients", "drwc_net_forward", "drwc_net_train_step",
     "drwc_frw_harvest", "drwc_records_voxelise", "drwc_cubes_random", "drwc_learned_opts_default",
     "drwc_frw_walks_learned",
+    "drwc_server_opts_default", "drwc_server_create", "drwc_server_destroy", "drwc_server_submit",
+    "drwc_server_poll", "drwc_server_wait", "drwc_server_job_times", "drwc_server_stats_get",
 ]
 
 
@@ -91,6 +93,31 @@ class JobParams(C.Structure):
 class LearnedOpts(C.Structure):
     _fields_ = [("slots", C.c_int32), ("conf_threshold", C.c_float), ("audit_frac", C.c_float),
                 ("use_graph", C.c_int32), ("max_steps", C.c_int32)]
+
+
+SERVER_MAX_SIZES = 4
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED = 0, 1, 2, 3
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("slots", C.c_int32), ("max_jobs", C.c_int32), ("hbm_budget", C.c_int64),
+                ("n_sizes", C.c_int32), ("sizes", C.c_int32 * SERVER_MAX_SIZES),
+                ("steps_per_graph", C.c_int32), ("max_materials", C.c_int32),
+                ("max_nets", C.c_int32), ("conf_threshold", C.c_float), ("audit_frac", C.c_float),
+                ("timing", C.c_int32), ("reserved_", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in (
+        "submitted", "admitted", "completed", "failed", "queued", "running", "max_running",
+        "hops", "net_hops", "fdm_hops", "fallbacks", "audits", "walks_finished", "walks_dropped",
+        "graph_launches", "kernels_launched", "arena_bytes", "arena_used", "arena_peak")] + \
+        [(n, C.c_double) for n in ("busy_seconds", "fdm_seconds", "net_seconds", "net_rows",
+                                   "audit_kl_mean")] + \
+        [("fdm_iters", C.c_int64), ("fdm_sweeps", C.c_int64), ("fdm_bytes", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
 
 
 class JobResult(C.Structure):
@@ -165,6 +192,16 @@ def load():
     L.drwc_learned_opts_default.restype = None
     L.drwc_frw_walks_learned.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams), vp,
                                          C.POINTER(LearnedOpts), i64, i64, vp, vp, vp, vp]
+    L.drwc_server_opts_default.argtypes = [C.POINTER(ServerOpts)]
+    L.drwc_server_opts_default.restype = None
+    L.drwc_server_create.argtypes = [vp, C.POINTER(ServerOpts), vp, C.POINTER(vp)]
+    L.drwc_server_destroy.argtypes = [vp]
+    L.drwc_server_submit.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams),
+                                     C.POINTER(i64)]
+    L.drwc_server_poll.argtypes = [vp, i64, C.POINTER(i32), C.POINTER(JobResult)]
+    L.drwc_server_wait.argtypes = [vp, i64, dbl, C.POINTER(JobResult)]
+    L.drwc_server_job_times.argtypes = [vp, i64, C.POINTER(dbl), C.POINTER(dbl)]
+    L.drwc_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
     _lib = L
     return L
 

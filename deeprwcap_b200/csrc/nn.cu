@@ -436,12 +436,14 @@ struct drwc_net {
     float* O = nullptr;
     float* G = nullptr;
     int* err = nullptr;
+    int holders = 0;  // servers whose captured graphs point at the activations
 };
 
 namespace drwc {
 
 static int net_reserve(drwc_net* n, int B) {
     if (B <= n->cap) return DRWC_OK;
+    if (n->holders > 0) return DRWC_ERR_INVALID;  // a server's graph uses the buffers
     auto fr = [](void* q) { if (q) cudaFree(q); };
     fr(n->a1); fr(n->a2); fr(n->a3); fr(n->dO); fr(n->dG); fr(n->dF); fr(n->dz2); fr(n->dz1);
     fr(n->tmpf); fr(n->O); fr(n->G);
@@ -513,6 +515,39 @@ int net_forward_mapped(drwc_net* n, int B, const bf16* X, float* O, float* G, co
     return net_heads(n, B, nullptr, O, G, gmap, rows_g);
 }
 
+int net_forward_dyn(drwc_net* n, int Bmax, const unsigned* nrows, const bf16* X, float* O,
+                    float* G, const int* gmap, const unsigned* nrows_g) {
+    if (Bmax > n->cap) return DRWC_ERR_INVALID;  // reserve first (not during capture)
+    drwc_ctx* ctx = n->ctx;
+    const bf16* pb = n->pb;
+    int rc = launch_umma_dyn<16>(ctx, Bmax * 512, nrows, 512, 16, 27,
+                                 ConvGather<16, 1>{X, Bmax * 512},
+                                 RowsBf16{pb + n->L.w1, 16, 27, 27, nullptr},
+                                 EpiReluBf16{n->a1, n->p + n->L.b1, 16}, n->err);
+    if (rc) return rc;
+    rc = launch_umma_dyn<32>(ctx, Bmax * 64, nrows, 64, 32, 27 * 16, ConvGather<8, 16>{n->a1, Bmax * 64},
+                             RowsBf16{pb + n->L.w2, 32, 27 * 16, 27 * 16, nullptr},
+                             EpiReluBf16{n->a2, n->p + n->L.b2, 32}, n->err);
+    if (rc) return rc;
+    rc = launch_umma_dyn<64>(ctx, Bmax * 8, nrows, 8, 64, 27 * 32, ConvGather<4, 32>{n->a2, Bmax * 8},
+                             RowsBf16{pb + n->L.w3, 64, 27 * 32, 27 * 32, nullptr},
+                             EpiReluBf16{n->a3, n->p + n->L.b3, 64}, n->err);
+    if (rc) return rc;
+    rc = launch_umma_dyn<128>(ctx, Bmax, nrows, 1, kDecRows, kFeat,
+                              RowsBf16{n->a3, Bmax, kFeat, kFeat, nullptr},
+                              RowsBf16{n->pb + n->L.wd, kDecRows, kFeat, kFeat, nullptr},
+                              EpiF32{O, n->p + n->L.bd, kDecRows, kDecRows, nullptr}, n->err);
+    if (rc) return rc;
+    return launch_umma_dyn<128>(ctx, Bmax, nrows_g, 1, kNP, kFeat,
+                                RowsBf16{n->a3, Bmax, kFeat, kFeat, gmap},
+                                RowsBf16{n->pb + n->L.wg, kNP, kFeat, kFeat, nullptr},
+                                EpiF32{G, n->p + n->L.bg, kNP, kNP, nullptr}, n->err);
+}
+
+int net_reserve_rows(drwc_net* n, int B) { return net_reserve(n, B); }
+
+void net_hold(drwc_net* n, int delta) { n->holders += delta; }
+
 drwc_ctx* net_context(drwc_net* n) { return n->ctx; }
 
 }  // namespace drwc
@@ -556,7 +591,7 @@ DRWC_API int drwc_net_create(drwc_ctx* ctx, int N, uint64_t seed, drwc_net** out
 }
 
 DRWC_API int drwc_net_destroy(drwc_net* n) {
-    if (!n) return DRWC_ERR_INVALID;
+    if (!n || n->holders > 0) return DRWC_ERR_INVALID;  // destroy its servers first
     cudaSetDevice(n->ctx->device);
     cudaStreamSynchronize(n->ctx->stream);
     void* ps[] = {n->p, n->pb, n->g, n->m, n->v, n->err, n->a1, n->a2, n->a3, n->dO, n->dG,

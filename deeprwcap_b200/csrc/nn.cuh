@@ -21,6 +21,16 @@ int net_forward_locked(drwc_net* n, int B, const __nv_bfloat16* X, float* O, flo
 // encoder row of gradient output row r).
 int net_forward_mapped(drwc_net* n, int B, const __nv_bfloat16* X, float* O, float* G,
                        const int* gmap, int rows_g);
+// Same on row counts read on the device (*nrows rows of X, *nrows_g rows
+// of the gradient head), for CUDA-graph replay: every launch covers Bmax
+// rows and tiles past the count exit at once. Call net_reserve_rows(Bmax)
+// beforehand (it allocates).
+int net_forward_dyn(drwc_net* n, int Bmax, const unsigned* nrows, const __nv_bfloat16* X,
+                    float* O, float* G, const int* gmap, const unsigned* nrows_g);
+int net_reserve_rows(drwc_net* n, int B);
+// A held network keeps its activation buffers: calls that would need larger
+// ones fail with DRWC_ERR_INVALID until every holder lets go.
+void net_hold(drwc_net* n, int delta);
 drwc_ctx* net_context(drwc_net* n);
 
 }  // namespace drwc

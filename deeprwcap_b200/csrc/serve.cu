@@ -1,0 +1,1342 @@
+// Multi-job FRW server: a persistent request loop that runs many extraction
+// jobs at once on one device.
+//
+// Device state
+//   * a job table (host-written between graph replays): each running job's
+//     structure (DevGeom, in the server's HBM arena), Gaussian surface, walk
+//     parameters, claim limit and the two batches of walk ids whose records
+//     it is collecting;
+//   * per-job counters (device-written): next walk id, finished walks per
+//     batch parity, walks in flight, reduced flags;
+//   * a pool of S walker slots (position, weight, hop count, job, walk id);
+//   * per-step work lists: network rows (N = 16 jobs when a network is
+//     loaded) and FDM rows bucketed by cube resolution.
+//
+// One step (all slots advance one hop)
+//   reset lists -> prepare (warp per slot: drop walks of finished jobs,
+//   claim a walk from the running jobs, nearest conductor, absorption,
+//   record the finished walk, append the hop to a list) -> [voxelise ->
+//   network (tensor cores) -> sample / route] -> FDM solve per bucket.
+// Buckets that do not wait for the network fork right after prepare, so
+// their solves overlap the network on parallel graph branches. A replay of
+// the captured graph runs steps_per_graph steps and then reduces every batch
+// whose walks have all finished (fixed-order sums per capacitance entry).
+//
+// Host loop (one thread): admit queued jobs first-in first-out while their
+// footprint fits the arena and a table entry is free, replay the graph,
+// read the counters and the reduced batches, fold them into each job's
+// compensated sums in batch order, test convergence exactly as
+// drwc_frw_run does, retire converged jobs (their walks still in flight are
+// dropped on the next step, then their arena block is freed), and widen each
+// job's claim window by one batch when the oldest batch has been reduced.
+// Walk w of a job draws from Philox counters (w, hop, draw) of the job's
+// seed, so its record does not depend on which slot or step carried it, and
+// the per-batch reduction order depends only on walk ids.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <thread>
+
+#include "geom.cuh"
+#include "nn.cuh"
+
+namespace drwc {
+
+constexpr int kSvMaxJobs = 64;
+constexpr int kSvNetN = DRWC_NET_N;
+constexpr int kSvDecRows = DRWC_NET_OUT;
+constexpr int kSvMaxSteps = 8;
+constexpr size_t kSvBsumStride = 3 * (DRWC_MAX_NETS + 2) + 8;  // doubles per (job, parity)
+
+struct SvJob {
+    DevGeom g;
+    Gauss G;
+    WalkParams W;
+    int state;         // 0 free, 1 running, 2 draining
+    int use_net;       // hops go through the network
+    int bucket;        // index of the job's cube resolution among the served sizes
+    int n_entries;     // nets + ground
+    long long total;   // walk ids [0, total)
+    long long batch;   // walks per batch
+    long long limit;   // ids below this may be claimed
+    long long bfirst[2];
+    long long bcount[2];
+    double* rec_w;     // 2 x batch records, parity p at p * batch
+    int32_t* rec_end;
+    int32_t* rec_hops;
+};
+
+struct SvCtr {
+    unsigned long long next;
+    unsigned long long done[2];
+    unsigned long long inflight;  // two's complement
+    unsigned long long reduced[2];
+    unsigned long long pad[2];
+};
+
+struct SvHdr {
+    int n_act;
+    int act[kSvMaxJobs];
+};
+
+struct SvSlots {
+    double *px, *py, *pz, *omega, *sgn, *a, *epsw;
+    long long* walk;
+    int *hops, *mode, *code, *job, *grow;
+};
+
+enum SvStat {
+    SV_HOPS = 0, SV_NET_HOPS, SV_FDM_HOPS, SV_FALLBACKS, SV_AUDITS, SV_WALKS_DONE,
+    SV_WALKS_DROPPED, SV_NET_ROWS, SV_FDM_ITERS, SV_FDM_SWEEPS, SV_FDM_BYTES, SV_NSTATS
+};
+
+struct SvArgs {
+    int S;
+    int n_buckets;
+    const SvJob* jobs;
+    SvCtr* ctr;
+    const SvHdr* hdr;
+    SvSlots st;
+    int* blist[DRWC_SERVER_MAX_SIZES];
+    int* bkind[DRWC_SERVER_MAX_SIZES];  // bit 0 audit, bits 1.. network row
+    unsigned* cnt;                      // [0] network rows, [1] first-hop rows, [2 + b] bucket b
+    float conf_thresh, audit_frac;
+    __nv_bfloat16* X;
+    float* O;
+    float* Gh;
+    int* alist;
+    int* frow;
+    unsigned long long* stats;
+    double* audit_kl;                   // [0] sum, [1] count
+    double* bsum;
+};
+
+// ------------------------------------------------------------------ device
+DRWC_DEV long long sv_claim(const SvArgs& A, int slot, int* job_out) {
+    const int n = A.hdr->n_act;
+    for (int q = 0; q < n; ++q) {
+        const int j = A.hdr->act[(slot + q) % n];
+        const SvJob& J = A.jobs[j];
+        if (J.state != 1) continue;
+        // keep the counter from running far past the limit; the host clamps it
+        if (*(volatile unsigned long long*)&A.ctr[j].next >= (unsigned long long)J.limit) continue;
+        const unsigned long long w = atomicAdd(&A.ctr[j].next, 1ull);
+        if ((long long)w < J.limit) {
+            *job_out = j;
+            return (long long)w;
+        }
+    }
+    return -1;
+}
+
+DRWC_DEV void sv_start(const SvArgs& A, int slot, int j, long long w) {
+    const SvJob& J = A.jobs[j];
+    double r[3], sgn;
+    int code;
+    walk_start_point(J.G, J.W.seed, (uint64_t)w, r, &sgn, &code);
+    A.st.px[slot] = r[0]; A.st.py[slot] = r[1]; A.st.pz[slot] = r[2];
+    A.st.sgn[slot] = sgn;
+    A.st.code[slot] = code;
+    A.st.hops[slot] = 0;
+    A.st.omega[slot] = 0.0;
+    A.st.walk[slot] = w;
+    A.st.job[slot] = j;
+    A.st.mode[slot] = 1;
+    atomicAdd(&A.ctr[j].inflight, 1ull);
+}
+
+// Record the walk on `net` (-1: lost) and free the slot.
+DRWC_DEV void sv_finish(const SvArgs& A, int slot, int net) {
+    const int j = A.st.job[slot];
+    const SvJob& J = A.jobs[j];
+    const long long w = A.st.walk[slot];
+    const int p = (int)((w / J.batch) & 1);
+    const long long i = w - J.bfirst[p];
+    if (i >= 0 && i < J.bcount[p]) {  // always, as claims stop at the window's end
+        const long long r = (long long)p * J.batch + i;
+        J.rec_end[r] = net;
+        J.rec_hops[r] = A.st.hops[slot];
+        J.rec_w[r] = A.st.omega[slot];
+        atomicAdd(&A.ctr[j].done[p], 1ull);
+    }
+    atomicAdd(&A.ctr[j].inflight, ~0ull);
+    atomicAdd(A.stats + SV_WALKS_DONE, 1ull);
+    A.st.mode[slot] = 0;
+}
+
+__global__ void sv_reset_kernel(SvArgs A) {
+    if (threadIdx.x < 2 + DRWC_SERVER_MAX_SIZES) A.cnt[threadIdx.x] = 0;
+}
+
+// One warp per slot.
+__global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
+    const int slot = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (slot >= A.S) return;
+    int act = 0;
+    for (int tries = 0; tries < 4; ++tries) {
+        int mode = A.st.mode[slot];
+        if (mode == 1 && A.jobs[A.st.job[slot]].state != 1) {
+            // the job has finished (or was cancelled): drop its walk
+            if (lane == 0) {
+                atomicAdd(&A.ctr[A.st.job[slot]].inflight, ~0ull);
+                atomicAdd(A.stats + SV_WALKS_DROPPED, 1ull);
+                A.st.mode[slot] = 0;
+            }
+            mode = 0;
+        }
+        if (mode == 0) {
+            long long w = -1;
+            if (lane == 0) {
+                int j = -1;
+                w = sv_claim(A, slot, &j);
+                if (w >= 0) sv_start(A, slot, j, w);
+            }
+            w = __shfl_sync(0xffffffffu, w, 0);
+            if (w < 0) break;  // nothing to claim: the slot idles this step
+        }
+        __syncwarp();
+        const SvJob& J = A.jobs[A.st.job[slot]];
+        const double r[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
+        double d;
+        int net;
+        nearest(J.g, r, &d, &net);
+        if (lane == 0) {
+            if (d < J.W.stop) sv_finish(A, slot, net);
+            else if (A.st.hops[slot] >= J.W.max_hops) sv_finish(A, slot, -1);
+            else { A.st.a[slot] = d; act = 1; }
+        }
+        act = __shfl_sync(0xffffffffu, act, 0);
+        __syncwarp();
+        if (act) break;
+    }
+    if (lane == 0 && act) {
+        const SvJob& J = A.jobs[A.st.job[slot]];
+        if (J.use_net) {
+            const unsigned idx = atomicAdd(&A.cnt[0], 1u);
+            A.alist[idx] = slot;
+            if (A.st.hops[slot] == 0) {
+                const unsigned f = atomicAdd(&A.cnt[1], 1u);
+                A.frow[f] = (int)idx;
+                A.st.grow[slot] = (int)f;
+            }
+        } else {
+            const int b = J.bucket;
+            const unsigned idx = atomicAdd(&A.cnt[2 + b], 1u);
+            A.blist[b][idx] = slot;
+            A.bkind[b][idx] = 0;
+        }
+    }
+}
+
+// One CTA (256 threads) per network row: the cube as network input.
+__global__ void __launch_bounds__(256) sv_voxelise_kernel(SvArgs A) {
+    constexpr int N = kSvNetN;
+    __shared__ double tco[N];
+    __shared__ double pal[kMaxMaterials];
+    __shared__ uint8_t mat[N * N * N];
+    __shared__ float red[32];
+    centre_offsets<N>(tco);
+    const int na = (int)A.cnt[0];
+    int loaded = -1;
+    for (int row = blockIdx.x; row < na; row += gridDim.x) {
+        const int slot = A.alist[row];
+        const int j = A.st.job[slot];
+        const SvJob& J = A.jobs[j];
+        if (j != loaded) {
+            __syncthreads();
+            for (int v = threadIdx.x; v < J.g.n_mat; v += blockDim.x) pal[v] = J.g.pal[v];
+            loaded = j;
+        }
+        __syncthreads();
+        const bool first = A.st.hops[slot] == 0;
+        const int rot = first ? rot_of_code(A.st.code[slot]) : 0;
+        const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
+        voxelise_net<N>(J.g, c, A.st.a[slot], rot, tco, pal, mat, A.X + (size_t)row * N * N * N,
+                        nullptr, red);
+        if (first && threadIdx.x == 0) {
+            const EpsPalette E{mat, pal, nullptr, nullptr, nullptr, 0};
+            A.st.epsw[slot] = center_diel<N>(E, DRWC_WVTZ);
+        }
+        __syncthreads();
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.stats + SV_NET_ROWS, (unsigned long long)na);
+}
+
+// One CTA (256 threads) per network row: draw from the prediction, or route
+// the hop to the FDM bucket of its job.
+__global__ void __launch_bounds__(256) sv_sample_kernel(SvArgs A) {
+    constexpr int N = kSvNetN, M = 6 * N * N, NT = 256;
+    __shared__ double wv[M];
+    __shared__ double red[2 * (NT / 32) + 16];
+    __shared__ int route;
+    const int na = (int)A.cnt[0];
+    unsigned long long my_net = 0;
+    for (int row = blockIdx.x; row < na; row += gridDim.x) {
+        const int slot = A.alist[row];
+        const SvJob& J = A.jobs[A.st.job[slot]];
+        const long long w = A.st.walk[slot];
+        const int h = A.st.hops[slot];
+        const bool first = h == 0;
+        if (threadIdx.x == 0) {
+            const float conf = A.O[(size_t)row * kSvDecRows + M];
+            const bool audit =
+                philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 2).x < (double)A.audit_frac;
+            const bool fallback = conf > A.conf_thresh;
+            route = 0;
+            if (audit || fallback) {
+                const int b = J.bucket;
+                const unsigned idx = atomicAdd(&A.cnt[2 + b], 1u);
+                A.blist[b][idx] = slot;
+                A.bkind[b][idx] = (audit ? 1 : 0) | (row << 1);
+                route = 1;
+                atomicAdd(A.stats + (audit ? SV_AUDITS : SV_FALLBACKS), 1ull);
+            }
+        }
+        __syncthreads();
+        if (route) { __syncthreads(); continue; }
+        double tot = 0.0;
+        int b;
+        if (first) {
+            const float* g = A.Gh + (size_t)A.st.grow[slot] * M;
+            for (int q = threadIdx.x; q < M; q += NT) wv[q] = (double)g[q] / (double)kGradScale;
+            __syncthreads();
+            const double u = philox_uniform2(J.W.seed, (uint64_t)w, 0, 1).y;
+            b = cta_sample<NT>(wv, M, true, u, red, &tot);
+        } else {
+            const float* o = A.O + (size_t)row * kSvDecRows;
+            float mx = -1e30f;
+            for (int q = threadIdx.x; q < M; q += NT) mx = fmaxf(mx, o[q]);
+            for (int s = 16; s > 0; s >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, s));
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+            __syncthreads();
+            float m = (float)red[0];
+            for (int q = 1; q < NT / 32; ++q) m = fmaxf(m, (float)red[q]);
+            __syncthreads();
+            for (int q = threadIdx.x; q < M; q += NT) wv[q] = (double)__expf(o[q] - m);
+            __syncthreads();
+            const double u = philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 0).x;
+            b = cta_sample<NT>(wv, M, false, u, red, &tot);
+        }
+        if (threadIdx.x == 0) {
+            if (b < 0) {
+                sv_finish(A, slot, -1);  // no transition possible: the walk is lost
+            } else {
+                const double a = A.st.a[slot];
+                double loc[3], mv[3];
+                locate_f64(N, b, loc);
+                if (first) {
+                    unrotate(rot_of_code(A.st.code[slot]), loc, mv);
+                    A.st.omega[slot] =
+                        first_hop_weight(J.G, A.st.sgn[slot], A.st.epsw[slot], tot, wv[b], a);
+                } else {
+                    mv[0] = loc[0]; mv[1] = loc[1]; mv[2] = loc[2];
+                }
+                A.st.px[slot] = dadd(A.st.px[slot], dmul(a, mv[0]));
+                A.st.py[slot] = dadd(A.st.py[slot], dmul(a, mv[1]));
+                A.st.pz[slot] = dadd(A.st.pz[slot], dmul(a, mv[2]));
+                A.st.hops[slot] = h + 1;
+            }
+            my_net += 1;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && my_net) {
+        atomicAdd(A.stats + SV_NET_HOPS, my_net);
+        atomicAdd(A.stats + SV_HOPS, my_net);
+    }
+}
+
+// FDM hops of one resolution bucket: persistent CTAs over the bucket list;
+// the palette tables are reloaded when the job changes between rows. The
+// arithmetic of a hop is walk_kernel's.
+template <int N>
+__global__ void __launch_bounds__(Cube<N>::NT, CubeTraits<N>::kMinBlocks)
+sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
+              float* __restrict__ scratch_s) {
+    extern __shared__ __align__(128) unsigned char drwc_dyn_smem[];
+    unsigned char* smem = drwc_dyn_smem;
+    using D = Cube<N>;
+    constexpr int M = 6 * D::NN;
+    const CubeSmem<N> sm = CubeSmem<N>::carve(smem);
+    unsigned char* xs = smem + D::kSmemBytes;
+    uint8_t* mat = xs;
+    double* tco = reinterpret_cast<double*>(xs + ((size_t)D::NNN + 15) / 16 * 16);
+    double* pal = tco + N;
+    double* palinv = pal + maxP;
+    double* pair64 = palinv + maxP;
+    float* pair32 = reinterpret_cast<float*>(pair64 + maxP * maxP);
+    centre_offsets<N>(tco);
+    double* ys = scratch_y + (size_t)blockIdx.x * D::NNN;
+    float* ss = scratch_s + (size_t)blockIdx.x * D::NNN;
+    const unsigned count = A.cnt[2 + bucket];
+    int loaded = -1, P = 0;
+    unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0;
+    for (unsigned idx = blockIdx.x; idx < count; idx += gridDim.x) {
+        const int slot = A.blist[bucket][idx];
+        const int kind = A.bkind[bucket][idx];
+        const int j = A.st.job[slot];
+        const SvJob& J = A.jobs[j];
+        if (j != loaded) {
+            __syncthreads();
+            P = J.g.n_mat;
+            for (int v = threadIdx.x; v < P; v += blockDim.x) {
+                pal[v] = J.g.pal[v];
+                palinv[v] = 1.0 / J.g.pal[v];
+            }
+            for (int v = threadIdx.x; v < P * P; v += blockDim.x) {
+                pair64[v] = J.g.pair64[v];
+                pair32[v] = J.g.pair32[v];
+            }
+            loaded = j;
+        }
+        __syncthreads();
+        const EpsPalette E{mat, pal, palinv, pair64, pair32, P};
+        const long long w = A.st.walk[slot];
+        const int h = A.st.hops[slot];
+        const bool first = h == 0;
+        const int code = first ? A.st.code[slot] : DRWC_GFT;
+        const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
+        const double a = A.st.a[slot];
+        voxelise<N>(J.g, c, a, tco, mat);
+        __syncthreads();
+        FdmStats st;
+        cube_solve<N>(E, ys, ss, code, J.W.prm, &st);
+        double* wv = reinterpret_cast<double*>(sm.stage());
+        for_each_panel<N>(E, ys, [&](int b, double v) { wv[b] = v; });
+        __syncthreads();
+        if ((kind & 1) && !first) {
+            // audit: KL(FDM || network) over the panels
+            const float* o = A.O + (size_t)(kind >> 1) * kSvDecRows;
+            const double ls = block_lse<D::NW>(o, M, sm.red);
+            __syncthreads();
+            double kl = 0.0;
+            for (int q = threadIdx.x; q < M; q += blockDim.x) {
+                const double gq = fmax(wv[q], 0.0);
+                if (gq > 0.0) kl += gq * (log(gq) - ((double)o[q] - ls));
+            }
+            kl = block_sum_d<D::NW>(kl, sm.red, 1);
+            if (threadIdx.x == 0) {
+                atomicAdd(A.audit_kl + 0, kl);
+                atomicAdd(A.audit_kl + 1, 1.0);
+            }
+            __syncthreads();
+        }
+        const double2 u2 = first ? philox_uniform2(J.W.seed, (uint64_t)w, 0, 1)
+                                 : philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 0);
+        const double ud = first ? u2.y : u2.x;
+        double tot = 0.0;
+        const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
+        if (threadIdx.x == 0) {
+            if (b < 0 || st.status == 2) {
+                sv_finish(A, slot, -1);  // no transition possible: the walk is lost
+            } else {
+                if (first)
+                    A.st.omega[slot] =
+                        first_hop_weight(J.G, A.st.sgn[slot], center_diel<N>(E, code), tot, wv[b], a);
+                double loc[3];
+                locate_f64(N, b, loc);
+                A.st.px[slot] = dadd(A.st.px[slot], dmul(a, loc[0]));
+                A.st.py[slot] = dadd(A.st.py[slot], dmul(a, loc[1]));
+                A.st.pz[slot] = dadd(A.st.pz[slot], dmul(a, loc[2]));
+                A.st.hops[slot] = h + 1;
+            }
+            my_hops += 1;
+            my_iters += (unsigned long long)st.iters;
+            my_sweeps += (unsigned long long)st.sweeps;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && my_hops) {
+        atomicAdd(A.stats + SV_FDM_HOPS, my_hops);
+        atomicAdd(A.stats + SV_HOPS, my_hops);
+        atomicAdd(A.stats + SV_FDM_ITERS, my_iters);
+        atomicAdd(A.stats + SV_FDM_SWEEPS, my_sweeps);
+        // streamed-PCG algorithmic bytes: 48 B/cell per FP32 iteration, 40 B/cell per
+        // FP64 sweep, the permittivity in (8 B/cell) and the 6N^2 panel values out
+        atomicAdd(A.stats + SV_FDM_BYTES,
+                  (48ull * my_iters + 40ull * my_sweeps + 8ull * my_hops) * D::NNN +
+                      48ull * D::NN * my_hops);
+    }
+}
+
+// Fixed-order sums of every batch whose walks have all finished: block
+// (job, parity) x entry; entry n_entries + 1 sums the hop counts.
+__global__ void __launch_bounds__(256) sv_reduce_kernel(SvArgs A) {
+    const int j = blockIdx.x >> 1, p = blockIdx.x & 1, e = blockIdx.y;
+    const SvJob& J = A.jobs[j];
+    if (J.state != 1 || e > J.n_entries + 1) return;
+    const SvCtr& C = A.ctr[j];
+    const long long n = J.bcount[p];
+    if (n <= 0 || C.reduced[p] || (long long)C.done[p] < n) return;
+    double* out = A.bsum + ((size_t)j * 2 + p) * kSvBsumStride;
+    const long long base = (long long)p * J.batch;
+    if (e <= J.n_entries) {
+        reduce_entry(e, J.n_entries, n, J.rec_end + base, J.rec_w + base, out);
+        return;
+    }
+    unsigned long long s = 0;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) s += (unsigned long long)J.rec_hops[base + i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ unsigned long long ws[8];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += ws[q];
+        out[3 * (J.n_entries + 1)] = (double)t;
+    }
+}
+
+__global__ void sv_mark_kernel(SvArgs A) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * kSvMaxJobs) return;
+    const int j = t >> 1, p = t & 1;
+    const SvJob& J = A.jobs[j];
+    if (J.state != 1) return;
+    SvCtr& C = A.ctr[j];
+    if (J.bcount[p] > 0 && !C.reduced[p] && (long long)C.done[p] >= J.bcount[p]) C.reduced[p] = 1;
+}
+
+// ------------------------------------------------------------------- host
+// First-fit allocator over the job arena (offsets, 256-byte granules).
+struct Arena {
+    size_t size = 0, used = 0, peak = 0;
+    std::map<size_t, size_t> free_;  // offset -> bytes
+    void init(size_t bytes) { size = bytes; free_.clear(); free_[0] = bytes; used = peak = 0; }
+    bool alloc(size_t bytes, size_t* off) {
+        bytes = (bytes + 255) / 256 * 256;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            *off = it->first;
+            const size_t rest = it->second - bytes;
+            const size_t roff = it->first + bytes;
+            free_.erase(it);
+            if (rest) free_[roff] = rest;
+            used += bytes;
+            peak = std::max(peak, used);
+            return true;
+        }
+        return false;
+    }
+    void release(size_t off, size_t bytes) {
+        bytes = (bytes + 255) / 256 * 256;
+        used -= bytes;
+        auto it = free_.emplace(off, bytes).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
+
+struct SvHostJob {
+    int64_t id = 0;
+    std::vector<drwc_box> boxes;
+    std::vector<double> zlo, leps;
+    std::vector<drwc_diel_box> diel;
+    drwc_structure s{};
+    drwc_job_params p{};
+    HostGeom hg;
+    Gauss G{};
+    WalkParams W{};
+    int state = DRWC_JOB_QUEUED;
+    int error = DRWC_OK;
+    int table = -1;
+    size_t arena_off = 0, arena_bytes = 0, blob_bytes = 0;
+    bool draining = false;
+    std::vector<double> S, Sc, S2, S2c;
+    long long walks = 0, lost = 0, next_batch = 0;
+    unsigned long long hops = 0;
+    drwc_job_result result{};
+    std::chrono::steady_clock::time_point t_submit, t_admit, t_done;
+};
+
+}  // namespace drwc
+
+using namespace drwc;
+
+struct drwc_server {
+    drwc_ctx* ctx = nullptr;
+    drwc_net* net = nullptr;
+    drwc_server_opts o{};
+    int bucket_of_N[DRWC_N_MAX + 1];
+    int net_bucket = -1;
+    // device
+    void* dblock = nullptr;
+    void* arena_dev = nullptr;
+    SvJob* d_jobs = nullptr;
+    SvCtr* d_ctr = nullptr;
+    SvHdr* d_hdr = nullptr;
+    double* d_bsum = nullptr;
+    unsigned long long* d_stats = nullptr;
+    double* d_akl = nullptr;
+    SvArgs A{};
+    int fdm_grid[DRWC_SERVER_MAX_SIZES] = {};
+    size_t fdm_smem[DRWC_SERVER_MAX_SIZES] = {};
+    double* fdm_sy[DRWC_SERVER_MAX_SIZES] = {};
+    float* fdm_ss[DRWC_SERVER_MAX_SIZES] = {};
+    // pinned mirrors
+    void* hblock = nullptr;
+    SvJob* h_jobs = nullptr;
+    SvCtr* h_ctr = nullptr;
+    SvHdr* h_hdr = nullptr;
+    double* h_bsum = nullptr;
+    unsigned long long* h_stats = nullptr;
+    double* h_akl = nullptr;
+    // graph
+    cudaStream_t side[DRWC_SERVER_MAX_SIZES] = {};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[DRWC_SERVER_MAX_SIZES] = {};
+    cudaEvent_t ev_round0 = nullptr, ev_round1 = nullptr;
+    cudaEvent_t ev_t[kSvMaxSteps][2 + 2 * DRWC_SERVER_MAX_SIZES] = {};
+    bool timing = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels_per_graph = 0;
+    // host state
+    std::mutex mu;
+    std::condition_variable cv;
+    std::thread thr;
+    bool stop = false;
+    int thread_error = DRWC_OK;
+    std::deque<SvHostJob*> queue;
+    std::map<int64_t, std::unique_ptr<SvHostJob>> jobs;
+    SvHostJob* table[kSvMaxJobs] = {};
+    int64_t next_id = 1;
+    Arena arena;
+    drwc_server_stats st{};
+};
+
+namespace drwc {
+
+template <int N>
+static int sv_fdm_setup(drwc_server* v, int b) {
+    using D = Cube<N>;
+    const size_t smem = WalkSmem<N>::bytes(v->o.max_materials);
+    DRWC_CUDA_TRY(cudaFuncSetAttribute(sv_fdm_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+    int per_sm = 0;
+    DRWC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sv_fdm_kernel<N>, D::NT, smem));
+    if (per_sm < 1) return DRWC_ERR_INVALID;
+    v->fdm_grid[b] = per_sm * v->ctx->sm_count;
+    v->fdm_smem[b] = smem;
+    return DRWC_OK;
+}
+
+static int sv_fdm_launch(drwc_server* v, int b, cudaStream_t s) {
+    const int N = v->o.sizes[b];
+    return dispatch_N(N, [&](auto nc) -> int {
+        constexpr int NC = decltype(nc)::value;
+        sv_fdm_kernel<NC><<<v->fdm_grid[b], Cube<NC>::NT, v->fdm_smem[b], s>>>(
+            v->A, b, v->o.max_materials, v->fdm_sy[b], v->fdm_ss[b]);
+        return launch_check(v->ctx);
+    });
+}
+
+// Event nodes when captured (plain records otherwise): stage timing.
+static int sv_mark(drwc_server* v, cudaEvent_t e, cudaStream_t s) {
+    if (!v->timing) return DRWC_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    DRWC_CUDA_TRY(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusActive)
+        DRWC_CUDA_TRY(cudaEventRecordWithFlags(e, s, cudaEventRecordExternal));
+    else
+        DRWC_CUDA_TRY(cudaEventRecord(e, s));
+    return DRWC_OK;
+}
+
+// One step on the context stream (captured into the graph).
+static int sv_step(drwc_server* v, int k) {
+    drwc_ctx* ctx = v->ctx;
+    cudaStream_t s = ctx->stream;
+    const SvArgs& A = v->A;
+    int rc;
+    sv_reset_kernel<<<1, 32, 0, s>>>(A);
+    if ((rc = launch_check(ctx))) return rc;
+    sv_prepare_kernel<<<(A.S * 32 + 255) / 256, 256, 0, s>>>(A);
+    if ((rc = launch_check(ctx))) return rc;
+    DRWC_CUDA_TRY(cudaEventRecord(v->ev_fork, s));
+    // buckets that do not wait for the network fork now
+    for (int b = 0; b < v->o.n_sizes; ++b) {
+        if (b == v->net_bucket) continue;
+        DRWC_CUDA_TRY(cudaStreamWaitEvent(v->side[b], v->ev_fork, 0));
+        if ((rc = sv_mark(v, v->ev_t[k][2 + 2 * b], v->side[b]))) return rc;
+        if ((rc = sv_fdm_launch(v, b, v->side[b]))) return rc;
+        if ((rc = sv_mark(v, v->ev_t[k][3 + 2 * b], v->side[b]))) return rc;
+        DRWC_CUDA_TRY(cudaEventRecord(v->ev_join[b], v->side[b]));
+    }
+    if (v->net) {
+        const int g2 = std::min(A.S, ctx->sm_count * 16);
+        if ((rc = sv_mark(v, v->ev_t[k][0], s))) return rc;
+        sv_voxelise_kernel<<<g2, 256, 0, s>>>(A);
+        if ((rc = launch_check(ctx))) return rc;
+        rc = net_forward_dyn(v->net, A.S, A.cnt, A.X, A.O, A.Gh, A.frow, A.cnt + 1);
+        if (rc) return rc;
+        if ((rc = sv_mark(v, v->ev_t[k][1], s))) return rc;
+        sv_sample_kernel<<<g2, 256, 0, s>>>(A);
+        if ((rc = launch_check(ctx))) return rc;
+        const int b = v->net_bucket;
+        if ((rc = sv_mark(v, v->ev_t[k][2 + 2 * b], s))) return rc;
+        if ((rc = sv_fdm_launch(v, b, s))) return rc;
+        if ((rc = sv_mark(v, v->ev_t[k][3 + 2 * b], s))) return rc;
+    }
+    for (int b = 0; b < v->o.n_sizes; ++b) {
+        if (b == v->net_bucket) continue;
+        DRWC_CUDA_TRY(cudaStreamWaitEvent(s, v->ev_join[b], 0));
+    }
+    return DRWC_OK;
+}
+
+static int sv_round_body(drwc_server* v) {
+    for (int k = 0; k < v->o.steps_per_graph; ++k) {
+        const int rc = sv_step(v, k);
+        if (rc) return rc;
+    }
+    cudaStream_t s = v->ctx->stream;
+    sv_reduce_kernel<<<dim3(2 * kSvMaxJobs, v->o.max_nets + 3), 256, 0, s>>>(v->A);
+    int rc = launch_check(v->ctx);
+    if (rc) return rc;
+    sv_mark_kernel<<<1, 2 * kSvMaxJobs, 0, s>>>(v->A);
+    return launch_check(v->ctx);
+}
+
+static int sv_capture(drwc_server* v) {
+    drwc_ctx* ctx = v->ctx;
+    // one uncaptured pass with no job running sets every kernel attribute
+    int rc = sv_round_body(v);
+    if (rc) return rc;
+    DRWC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+    const int64_t before = ctx->launches.load();
+    DRWC_CUDA_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    rc = sv_round_body(v);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (rc || e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        if (e != cudaSuccess)
+            std::fprintf(stderr, "drwc: server graph capture failed: %s\n", cudaGetErrorString(e));
+        return rc ? rc : DRWC_ERR_CUDA;
+    }
+    v->kernels_per_graph = ctx->launches.load() - before;
+    ctx->launches.fetch_sub(v->kernels_per_graph);
+    v->graph = g;
+    DRWC_CUDA_TRY(cudaGraphInstantiate(&v->exec, g, 0));
+    return DRWC_OK;
+}
+
+static double sv_secs(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+    return std::chrono::duration<double>(b - a).count();
+}
+
+// Footprint of a job in the arena: its structure blob and two batches of records.
+static size_t sv_footprint(const SvHostJob* J, size_t* blob_bytes) {
+    const size_t blob = (J->hg.blob.size() + 255) / 256 * 256;
+    *blob_bytes = blob;
+    const size_t b = (size_t)J->p.batch_walks;
+    return blob + 2 * b * 8 + 2 * b * 4 + 2 * b * 4 + 256;
+}
+
+// Admit queued jobs in arrival order (caller holds v->mu and the context lock).
+static int sv_admit(drwc_server* v) {
+    while (!v->queue.empty()) {
+        SvHostJob* J = v->queue.front();
+        int t = -1;
+        for (int q = 0; q < v->o.max_jobs; ++q)
+            if (!v->table[q]) { t = q; break; }
+        if (t < 0) break;
+        size_t blob = 0;
+        const size_t need = sv_footprint(J, &blob);
+        size_t off = 0;
+        if (!v->arena.alloc(need, &off)) {
+            if (need > v->arena.size) {  // can never fit
+                v->queue.pop_front();
+                J->state = DRWC_JOB_FAILED;
+                J->error = DRWC_ERR_NOMEM;
+                v->st.failed += 1;
+                v->cv.notify_all();
+                continue;
+            }
+            break;  // wait for memory to free up
+        }
+        v->queue.pop_front();
+        unsigned char* base = (unsigned char*)v->arena_dev + off;
+        // a copy from pageable memory has read the source when it returns
+        DRWC_CUDA_TRY(cudaMemcpyAsync(base, J->hg.blob.data(), J->hg.blob.size(),
+                                      cudaMemcpyHostToDevice, v->ctx->stream));
+        bind_geom(&J->hg, base);
+        const long long batch = J->p.batch_walks, total = J->p.max_walks;
+        SvJob& T = v->h_jobs[t];
+        std::memset(&T, 0, sizeof T);
+        T.g = J->hg.dev;
+        T.G = J->G;
+        T.W = J->W;
+        T.state = 1;
+        T.use_net = v->net && J->p.N == kSvNetN;
+        T.bucket = v->bucket_of_N[J->p.N];
+        T.n_entries = J->s.n_nets + 1;
+        T.total = total;
+        T.batch = batch;
+        T.limit = std::min(2 * batch, total);
+        T.bfirst[0] = 0;
+        T.bcount[0] = std::min(batch, total);
+        T.bfirst[1] = batch < total ? batch : -1;
+        T.bcount[1] = batch < total ? std::min(batch, total - batch) : 0;
+        T.rec_w = (double*)(base + blob);
+        T.rec_end = (int32_t*)(base + blob + 2 * batch * 8);
+        T.rec_hops = T.rec_end + 2 * batch;
+        std::memset(&v->h_ctr[t], 0, sizeof(SvCtr));
+        J->table = t;
+        J->arena_off = off;
+        J->arena_bytes = need;
+        J->blob_bytes = blob;
+        J->state = DRWC_JOB_RUNNING;
+        J->t_admit = std::chrono::steady_clock::now();
+        const int ne = J->s.n_nets + 1;
+        J->S.assign(ne + 1, 0.0); J->Sc.assign(ne + 1, 0.0);
+        J->S2.assign(ne + 1, 0.0); J->S2c.assign(ne + 1, 0.0);
+        v->table[t] = J;
+        v->st.admitted += 1;
+    }
+    // active list
+    SvHdr& H = *v->h_hdr;
+    H.n_act = 0;
+    for (int q = 0; q < kSvMaxJobs; ++q)
+        if (v->table[q] && !v->table[q]->draining) H.act[H.n_act++] = q;
+    v->st.max_running = std::max<int64_t>(v->st.max_running, H.n_act);
+    return DRWC_OK;
+}
+
+// Fold the reduced batches of a running job in batch order; retire it when
+// it converges or runs out of walks (same test, same order as drwc_frw_run).
+static void sv_fold(drwc_server* v, int t) {
+    SvHostJob* J = v->table[t];
+    SvJob& T = v->h_jobs[t];
+    SvCtr& C = v->h_ctr[t];
+    // ids past the limit were never handed out
+    if ((long long)C.next > T.limit) C.next = (unsigned long long)T.limit;
+    const drwc_job_params& p = J->p;
+    const int ne = J->s.n_nets + 1;
+    auto kadd = [](double& s, double& c, double x) {
+        const double u = s + x;
+        if (std::fabs(s) >= std::fabs(x)) c += (s - u) + x;
+        else c += (x - u) + s;
+        s = u;
+    };
+    for (;;) {
+        const long long k = J->next_batch;
+        const int par = (int)(k & 1);
+        if (T.bcount[par] <= 0 || T.bfirst[par] != k * T.batch || !C.reduced[par]) break;
+        const double* sums = v->h_bsum + ((size_t)t * 2 + par) * kSvBsumStride;
+        for (int e = 0; e <= ne; ++e) {
+            kadd(J->S[e], J->Sc[e], sums[3 * e]);
+            kadd(J->S2[e], J->S2c[e], sums[3 * e + 1]);
+        }
+        J->lost += (long long)sums[3 * ne + 2];
+        J->hops += (unsigned long long)sums[3 * (ne + 1)];
+        J->walks += T.bcount[par];
+        J->next_batch = k + 1;
+        bool finished = J->walks >= p.max_walks;
+        int converged = 0;
+        if (J->walks >= p.min_walks) {
+            const double n = (double)J->walks;
+            auto mean = [&](int e) { return (J->S[e] + J->Sc[e]) / n; };
+            auto sem = [&](int e) {
+                const double m = mean(e);
+                const double var = std::max(0.0, (J->S2[e] + J->S2c[e]) / n - m * m);
+                return std::sqrt(var / n);
+            };
+            const double cs = mean(p.master);
+            bool ok = cs != 0.0 && sem(p.master) <= p.p_tol * std::fabs(cs);
+            std::vector<std::pair<double, int>> cpl;
+            double ctot = 0.0;
+            for (int e = 0; e < ne; ++e) {
+                if (e == p.master) continue;
+                cpl.push_back({std::fabs(mean(e)), e});
+                ctot += std::fabs(mean(e));
+            }
+            std::sort(cpl.begin(), cpl.end(), [](auto& a, auto& b) { return a.first > b.first; });
+            double acc = 0.0;
+            for (auto& ce : cpl) {
+                if (acc >= p.c_ratio * ctot) break;
+                acc += ce.first;
+                if (!(ce.first > 0.0) || sem(ce.second) > p.c_tol * ce.first) { ok = false; break; }
+            }
+            if (ok) { converged = 1; finished = true; }
+        }
+        if (finished) {
+            const double n = (double)std::max(1LL, J->walks);
+            drwc_job_result& R = J->result;
+            std::memset(&R, 0, sizeof R);
+            R.n_entries = ne;
+            R.converged = converged;
+            R.walks = J->walks;
+            R.hops = (int64_t)J->hops;
+            R.lost = J->lost;
+            for (int e = 0; e < ne; ++e) {
+                const double m = (J->S[e] + J->Sc[e]) / n;
+                R.cap[e] = m;
+                const double var = std::max(0.0, (J->S2[e] + J->S2c[e]) / n - m * m);
+                R.stderr_[e] = std::sqrt(var / n);
+            }
+            J->t_done = std::chrono::steady_clock::now();
+            R.seconds = sv_secs(J->t_submit, J->t_done);
+            J->state = DRWC_JOB_DONE;
+            J->draining = true;
+            T.state = 2;
+            v->st.completed += 1;
+            v->cv.notify_all();
+            return;
+        }
+        // parity par now holds batch k + 2; the window grows by one batch
+        const long long k2 = k + 2;
+        if (k2 * T.batch < T.total) {
+            T.bfirst[par] = k2 * T.batch;
+            T.bcount[par] = std::min(T.batch, T.total - k2 * T.batch);
+        } else {
+            T.bfirst[par] = -1;
+            T.bcount[par] = 0;
+        }
+        C.done[par] = 0;
+        C.reduced[par] = 0;
+        T.limit = std::min((k + 3) * T.batch, T.total);
+    }
+}
+
+static void sv_release(drwc_server* v, int t) {
+    SvHostJob* J = v->table[t];
+    v->arena.release(J->arena_off, J->arena_bytes);
+    std::memset(&v->h_jobs[t], 0, sizeof(SvJob));
+    std::memset(&v->h_ctr[t], 0, sizeof(SvCtr));
+    J->table = -1;
+    J->hg.blob.clear();
+    J->hg.blob.shrink_to_fit();
+    v->table[t] = nullptr;
+}
+
+// One graph replay and the reads after it (context lock held).
+static int sv_round(drwc_server* v) {
+    drwc_ctx* ctx = v->ctx;
+    cudaStream_t s = ctx->stream;
+    DRWC_CUDA_TRY(cudaMemcpyAsync(v->d_jobs, v->h_jobs, sizeof(SvJob) * kSvMaxJobs,
+                                  cudaMemcpyHostToDevice, s));
+    DRWC_CUDA_TRY(cudaMemcpyAsync(v->d_ctr, v->h_ctr, sizeof(SvCtr) * kSvMaxJobs,
+                                  cudaMemcpyHostToDevice, s));
+    DRWC_CUDA_TRY(cudaMemcpyAsync(v->d_hdr, v->h_hdr, sizeof(SvHdr), cudaMemcpyHostToDevice, s));
+    DRWC_CUDA_TRY(cudaEventRecord(v->ev_round0, s));
+    DRWC_CUDA_TRY(cudaGraphLaunch(v->exec, s));
+    DRWC_CUDA_TRY(cudaEventRecord(v->ev_round1, s));
+    ctx->launches.fetch_add(v->kernels_per_graph);
+    DRWC_CUDA_TRY(cudaMemcpyAsync(v->h_ctr, v->d_ctr, sizeof(SvCtr) * kSvMaxJobs,
+                                  cudaMemcpyDeviceToHost, s));
+    DRWC_CUDA_TRY(cudaMemcpyAsync(v->h_bsum, v->d_bsum, sizeof(double) * kSvBsumStride * 2 * kSvMaxJobs,
+                                  cudaMemcpyDeviceToHost, s));
+    DRWC_CUDA_TRY(cudaMemcpyAsync(v->h_stats, v->d_stats, sizeof(unsigned long long) * SV_NSTATS,
+                                  cudaMemcpyDeviceToHost, s));
+    DRWC_CUDA_TRY(cudaMemcpyAsync(v->h_akl, v->d_akl, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DRWC_CUDA_TRY(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, v->ev_round0, v->ev_round1) == cudaSuccess)
+        v->st.busy_seconds += ms * 1e-3;
+    if (v->timing) {
+        for (int k = 0; k < v->o.steps_per_graph; ++k) {
+            if (v->net && cudaEventElapsedTime(&ms, v->ev_t[k][0], v->ev_t[k][1]) == cudaSuccess)
+                v->st.net_seconds += ms * 1e-3;
+            for (int b = 0; b < v->o.n_sizes; ++b)
+                if (cudaEventElapsedTime(&ms, v->ev_t[k][2 + 2 * b], v->ev_t[k][3 + 2 * b]) ==
+                    cudaSuccess)
+                    v->st.fdm_seconds += ms * 1e-3;
+        }
+        cudaGetLastError();
+    }
+    v->st.graph_launches += 1;
+    v->st.kernels_launched += v->kernels_per_graph;
+    return DRWC_OK;
+}
+
+static void sv_thread(drwc_server* v) {
+    std::unique_lock<std::mutex> lk(v->mu);
+    for (;;) {
+        if (v->stop) break;
+        bool any = false;
+        for (int q = 0; q < kSvMaxJobs; ++q) any |= v->table[q] != nullptr;
+        if (!any && v->queue.empty()) {
+            v->cv.wait_for(lk, std::chrono::milliseconds(20));
+            continue;
+        }
+        int rc;
+        {
+            std::lock_guard<std::mutex> clk(v->ctx->mu);
+            cudaSetDevice(v->ctx->device);
+            rc = sv_admit(v);
+            bool running = false;
+            for (int q = 0; q < kSvMaxJobs; ++q) running |= v->table[q] != nullptr;
+            if (!rc && running) {
+                lk.unlock();  // submissions and polls proceed during the replay
+                rc = sv_round(v);
+                lk.lock();
+            }
+        }
+        if (rc) {
+            v->thread_error = rc;
+            break;
+        }
+        std::this_thread::yield();  // let other users of the context in between replays
+        for (int q = 0; q < kSvMaxJobs; ++q) {
+            if (!v->table[q]) continue;
+            if (!v->table[q]->draining) sv_fold(v, q);
+            else if ((long long)v->h_ctr[q].inflight == 0) sv_release(v, q);
+        }
+        const unsigned long long* h = v->h_stats;
+        v->st.hops = (int64_t)h[SV_HOPS];
+        v->st.net_hops = (int64_t)h[SV_NET_HOPS];
+        v->st.fdm_hops = (int64_t)h[SV_FDM_HOPS];
+        v->st.fallbacks = (int64_t)h[SV_FALLBACKS];
+        v->st.audits = (int64_t)h[SV_AUDITS];
+        v->st.walks_finished = (int64_t)h[SV_WALKS_DONE];
+        v->st.walks_dropped = (int64_t)h[SV_WALKS_DROPPED];
+        v->st.net_rows = (double)h[SV_NET_ROWS];
+        v->st.fdm_iters = (int64_t)h[SV_FDM_ITERS];
+        v->st.fdm_sweeps = (int64_t)h[SV_FDM_SWEEPS];
+        v->st.fdm_bytes = (double)h[SV_FDM_BYTES];
+        v->st.audit_kl_mean = v->h_akl[1] > 0 ? v->h_akl[0] / v->h_akl[1] : 0.0;
+    }
+    // stopped (destroy or an error): every job not done ends as failed
+    const int why = v->thread_error ? v->thread_error : DRWC_ERR_SHUTDOWN;
+    for (auto& kv : v->jobs) {
+        SvHostJob* J = kv.second.get();
+        if (J->state == DRWC_JOB_QUEUED || J->state == DRWC_JOB_RUNNING) {
+            J->state = DRWC_JOB_FAILED;
+            J->error = why;
+            v->st.failed += 1;
+        }
+    }
+    v->queue.clear();
+    v->stop = true;
+    v->cv.notify_all();
+}
+
+static int sv_alloc(drwc_server* v) {
+    const int S = v->o.slots;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t r = off; off += (bytes + 255) / 256 * 256; return r; };
+    const size_t o_jobs = take(sizeof(SvJob) * kSvMaxJobs), o_ctr = take(sizeof(SvCtr) * kSvMaxJobs),
+                 o_hdr = take(sizeof(SvHdr)), o_bsum = take(8 * kSvBsumStride * 2 * kSvMaxJobs),
+                 o_stats = take(8 * SV_NSTATS), o_akl = take(16), o_cnt = take(64),
+                 o_dbl = take(8 * (size_t)S * 7), o_walk = take(8 * (size_t)S),
+                 o_int = take(4 * (size_t)S * 5), o_lists = take(4 * (size_t)S * 2),
+                 o_b = take(4 * (size_t)S * 2 * DRWC_SERVER_MAX_SIZES);
+    size_t o_X = 0, o_O = 0, o_G = 0;
+    if (v->net) {
+        o_X = take(2 * (size_t)S * kSvNetN * kSvNetN * kSvNetN);
+        o_O = take(4 * (size_t)S * kSvDecRows);
+        o_G = take(4 * (size_t)S * DRWC_NET_PANELS);
+    }
+    size_t o_sy[DRWC_SERVER_MAX_SIZES], o_ss[DRWC_SERVER_MAX_SIZES];
+    for (int b = 0; b < v->o.n_sizes; ++b) {
+        const size_t nnn = (size_t)v->o.sizes[b] * v->o.sizes[b] * v->o.sizes[b];
+        o_sy[b] = take(8 * (size_t)v->fdm_grid[b] * nnn);
+        o_ss[b] = take(4 * (size_t)v->fdm_grid[b] * nnn);
+    }
+    if (cudaMalloc(&v->dblock, off) != cudaSuccess) { cudaGetLastError(); return DRWC_ERR_NOMEM; }
+    DRWC_CUDA_TRY(cudaMemset(v->dblock, 0, off));
+    if (cudaMalloc(&v->arena_dev, (size_t)v->o.hbm_budget) != cudaSuccess) {
+        cudaGetLastError();
+        return DRWC_ERR_NOMEM;
+    }
+    v->arena.init((size_t)v->o.hbm_budget);
+    unsigned char* B = (unsigned char*)v->dblock;
+    v->d_jobs = (SvJob*)(B + o_jobs);
+    v->d_ctr = (SvCtr*)(B + o_ctr);
+    v->d_hdr = (SvHdr*)(B + o_hdr);
+    v->d_bsum = (double*)(B + o_bsum);
+    v->d_stats = (unsigned long long*)(B + o_stats);
+    v->d_akl = (double*)(B + o_akl);
+    SvArgs& A = v->A;
+    A.S = S;
+    A.n_buckets = v->o.n_sizes;
+    A.jobs = v->d_jobs;
+    A.ctr = v->d_ctr;
+    A.hdr = v->d_hdr;
+    A.bsum = v->d_bsum;
+    A.stats = v->d_stats;
+    A.audit_kl = v->d_akl;
+    A.cnt = (unsigned*)(B + o_cnt);
+    double* dd = (double*)(B + o_dbl);
+    A.st.px = dd; A.st.py = dd + S; A.st.pz = dd + 2 * S; A.st.omega = dd + 3 * S;
+    A.st.sgn = dd + 4 * S; A.st.a = dd + 5 * S; A.st.epsw = dd + 6 * S;
+    A.st.walk = (long long*)(B + o_walk);
+    int* ii = (int*)(B + o_int);
+    A.st.hops = ii; A.st.mode = ii + S; A.st.code = ii + 2 * S; A.st.job = ii + 3 * S;
+    A.st.grow = ii + 4 * S;
+    A.alist = (int*)(B + o_lists);
+    A.frow = A.alist + S;
+    int* bl = (int*)(B + o_b);
+    for (int b = 0; b < DRWC_SERVER_MAX_SIZES; ++b) {
+        A.blist[b] = bl + (size_t)2 * b * S;
+        A.bkind[b] = bl + (size_t)(2 * b + 1) * S;
+    }
+    A.conf_thresh = v->o.conf_threshold;
+    A.audit_frac = v->o.audit_frac;
+    if (v->net) {
+        A.X = (__nv_bfloat16*)(B + o_X);
+        A.O = (float*)(B + o_O);
+        A.Gh = (float*)(B + o_G);
+    }
+    for (int b = 0; b < v->o.n_sizes; ++b) {
+        v->fdm_sy[b] = (double*)(B + o_sy[b]);
+        v->fdm_ss[b] = (float*)(B + o_ss[b]);
+    }
+    // pinned mirrors
+    size_t hoff = 0;
+    auto htake = [&](size_t bytes) { size_t r = hoff; hoff += (bytes + 255) / 256 * 256; return r; };
+    const size_t h_jobs = htake(sizeof(SvJob) * kSvMaxJobs), h_ctr = htake(sizeof(SvCtr) * kSvMaxJobs),
+                 h_hdr = htake(sizeof(SvHdr)), h_bsum = htake(8 * kSvBsumStride * 2 * kSvMaxJobs),
+                 h_stats = htake(8 * SV_NSTATS), h_akl = htake(16);
+    if (cudaMallocHost(&v->hblock, hoff) != cudaSuccess) { cudaGetLastError(); return DRWC_ERR_NOMEM; }
+    std::memset(v->hblock, 0, hoff);
+    unsigned char* H = (unsigned char*)v->hblock;
+    v->h_jobs = (SvJob*)(H + h_jobs);
+    v->h_ctr = (SvCtr*)(H + h_ctr);
+    v->h_hdr = (SvHdr*)(H + h_hdr);
+    v->h_bsum = (double*)(H + h_bsum);
+    v->h_stats = (unsigned long long*)(H + h_stats);
+    v->h_akl = (double*)(H + h_akl);
+    return DRWC_OK;
+}
+
+static void sv_free(drwc_server* v) {
+    if (v->exec) cudaGraphExecDestroy(v->exec);
+    if (v->graph) cudaGraphDestroy(v->graph);
+    for (int b = 0; b < DRWC_SERVER_MAX_SIZES; ++b) {
+        if (v->side[b]) cudaStreamDestroy(v->side[b]);
+        if (v->ev_join[b]) cudaEventDestroy(v->ev_join[b]);
+    }
+    for (cudaEvent_t e : {v->ev_fork, v->ev_round0, v->ev_round1})
+        if (e) cudaEventDestroy(e);
+    for (int k = 0; k < kSvMaxSteps; ++k)
+        for (int q = 0; q < 2 + 2 * DRWC_SERVER_MAX_SIZES; ++q)
+            if (v->ev_t[k][q]) cudaEventDestroy(v->ev_t[k][q]);
+    if (v->dblock) cudaFree(v->dblock);
+    if (v->arena_dev) cudaFree(v->arena_dev);
+    if (v->hblock) cudaFreeHost(v->hblock);
+}
+
+}  // namespace drwc
+
+extern "C" {
+
+DRWC_API void drwc_server_opts_default(drwc_server_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->slots = 65536;
+    o->max_jobs = 32;
+    o->hbm_budget = 1LL << 30;
+    o->n_sizes = 3;
+    o->sizes[0] = 16;
+    o->sizes[1] = 21;
+    o->sizes[2] = 23;
+    o->steps_per_graph = 2;
+    o->max_materials = 16;
+    o->max_nets = 64;
+    o->conf_threshold = -1.5f;
+    o->audit_frac = 0.01f;
+    o->timing = 0;
+}
+
+DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drwc_net* net,
+                                drwc_server** out) {
+    if (!ctx || !out) return DRWC_ERR_INVALID;
+    *out = nullptr;
+    drwc_server_opts o;
+    drwc_server_opts_default(&o);
+    if (opts) o = *opts;
+    if (o.slots < 1 || o.slots > (1 << 22) || o.max_jobs < 1 || o.max_jobs > kSvMaxJobs ||
+        o.hbm_budget < 4096 || o.n_sizes < 1 || o.n_sizes > DRWC_SERVER_MAX_SIZES ||
+        o.steps_per_graph < 1 || o.steps_per_graph > kSvMaxSteps || o.max_materials < 1 ||
+        o.max_materials > kMaxMaterials || o.max_nets < 1 || o.max_nets > DRWC_MAX_NETS ||
+        !(o.audit_frac >= 0.f && o.audit_frac <= 1.f))
+        return DRWC_ERR_INVALID;
+    if (net && net_context(net) != ctx) return DRWC_ERR_INVALID;
+    std::unique_ptr<drwc_server> v(new drwc_server());
+    v->ctx = ctx;
+    v->net = net;
+    v->o = o;
+    v->timing = o.timing != 0;
+    for (int n = 0; n <= DRWC_N_MAX; ++n) v->bucket_of_N[n] = -1;
+    for (int b = 0; b < o.n_sizes; ++b) {
+        const int N = o.sizes[b];
+        if (!n_supported(N) || v->bucket_of_N[N] >= 0) return DRWC_ERR_INVALID;
+        v->bucket_of_N[N] = b;
+        if (net && N == kSvNetN) v->net_bucket = b;
+    }
+    if (net && v->net_bucket < 0) return DRWC_ERR_INVALID;  // the network serves N = 16 jobs
+    {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        DRWC_CUDA_TRY(cudaSetDevice(ctx->device));
+        int rc = DRWC_OK;
+        for (int b = 0; !rc && b < o.n_sizes; ++b) {
+            rc = dispatch_N(o.sizes[b], [&](auto nc) -> int {
+                return sv_fdm_setup<decltype(nc)::value>(v.get(), b);
+            });
+            const double* w[4];
+            if (!rc) rc = warm_tables(ctx, o.sizes[b], w);
+        }
+        if (!rc) rc = sv_alloc(v.get());
+        if (!rc && net) rc = net_reserve_rows(net, o.slots);
+        for (int b = 0; !rc && b < o.n_sizes; ++b) {
+            if (cudaStreamCreateWithFlags(&v->side[b], cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&v->ev_join[b], cudaEventDisableTiming) != cudaSuccess)
+                rc = DRWC_ERR_CUDA;
+        }
+        if (!rc && (cudaEventCreateWithFlags(&v->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                    cudaEventCreate(&v->ev_round0) != cudaSuccess ||
+                    cudaEventCreate(&v->ev_round1) != cudaSuccess))
+            rc = DRWC_ERR_CUDA;
+        for (int k = 0; !rc && v->timing && k < o.steps_per_graph; ++k)
+            for (int q = 0; q < 2 + 2 * o.n_sizes; ++q)
+                if (cudaEventCreate(&v->ev_t[k][q]) != cudaSuccess) rc = DRWC_ERR_CUDA;
+        if (!rc) rc = sv_capture(v.get());
+        if (!rc && net) net_hold(net, 1);
+        if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = DRWC_ERR_CUDA;
+        if (rc) {
+            cudaGetLastError();
+            cudaStreamSynchronize(ctx->stream);
+            sv_free(v.get());
+            return rc;
+        }
+    }
+    v->st.arena_bytes = o.hbm_budget;
+    drwc_server* raw = v.release();
+    raw->thr = std::thread(sv_thread, raw);
+    *out = raw;
+    return DRWC_OK;
+}
+
+DRWC_API int drwc_server_destroy(drwc_server* v) {
+    if (!v) return DRWC_ERR_INVALID;
+    {
+        std::lock_guard<std::mutex> lk(v->mu);
+        v->stop = true;
+        v->cv.notify_all();
+    }
+    if (v->thr.joinable()) v->thr.join();
+    {
+        std::lock_guard<std::mutex> lock(v->ctx->mu);
+        cudaSetDevice(v->ctx->device);
+        cudaStreamSynchronize(v->ctx->stream);
+        if (v->net) net_hold(v->net, -1);
+        sv_free(v);
+    }
+    delete v;
+    return DRWC_OK;
+}
+
+DRWC_API int drwc_server_submit(drwc_server* v, const drwc_structure* s, const drwc_job_params* p,
+                                int64_t* job_id) {
+    if (!v || !s || !p || !job_id) return DRWC_ERR_INVALID;
+    *job_id = 0;
+    if (!n_supported(p->N) || v->bucket_of_N[p->N] < 0 || p->batch_walks < 1 ||
+        p->max_walks < 1 || p->min_walks < 0 || s->n_nets > v->o.max_nets || s->n_boxes < 0 ||
+        (s->n_boxes > 0 && !s->boxes))
+        return DRWC_ERR_INVALID;
+    std::unique_ptr<SvHostJob> J(new SvHostJob());
+    J->boxes.assign(s->boxes, s->boxes + s->n_boxes);
+    if (s->n_layers > 0 && s->layer_zlo && s->layer_eps) {
+        J->zlo.assign(s->layer_zlo, s->layer_zlo + s->n_layers);
+        J->leps.assign(s->layer_eps, s->layer_eps + s->n_layers);
+    }
+    if (s->n_diel > 0 && s->diel) J->diel.assign(s->diel, s->diel + s->n_diel);
+    J->s = *s;
+    J->s.boxes = J->boxes.data();
+    J->s.layer_zlo = J->zlo.empty() ? nullptr : J->zlo.data();
+    J->s.layer_eps = J->leps.empty() ? nullptr : J->leps.data();
+    J->s.diel = J->diel.empty() ? nullptr : J->diel.data();
+    J->p = *p;
+    // validation, Gaussian surface and packing run on the host; the
+    // warm-start tables of the served sizes were made at creation, so this
+    // needs neither the device nor the context lock
+    const int rc = prepare(v->ctx, &J->s, &J->p, &J->hg, &J->G, &J->W);
+    if (rc) return rc;
+    if (J->hg.dev.n_mat > v->o.max_materials) return DRWC_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(v->mu);
+    if (v->stop) return DRWC_ERR_SHUTDOWN;
+    J->id = v->next_id++;
+    J->t_submit = std::chrono::steady_clock::now();
+    *job_id = J->id;
+    v->queue.push_back(J.get());
+    v->jobs[J->id] = std::move(J);
+    v->st.submitted += 1;
+    v->cv.notify_all();
+    return DRWC_OK;
+}
+
+DRWC_API int drwc_server_poll(drwc_server* v, int64_t id, int32_t* state, drwc_job_result* out) {
+    if (!v || !state) return DRWC_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(v->mu);
+    auto it = v->jobs.find(id);
+    if (it == v->jobs.end()) return DRWC_ERR_INVALID;
+    const SvHostJob* J = it->second.get();
+    *state = J->state;
+    if (out && J->state == DRWC_JOB_DONE) *out = J->result;
+    return J->state == DRWC_JOB_FAILED ? J->error : DRWC_OK;
+}
+
+DRWC_API int drwc_server_wait(drwc_server* v, int64_t id, double timeout_s, drwc_job_result* out) {
+    if (!v) return DRWC_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(v->mu);
+    auto it = v->jobs.find(id);
+    if (it == v->jobs.end()) return DRWC_ERR_INVALID;
+    const SvHostJob* J = it->second.get();
+    const auto deadline = std::chrono::steady_clock::now() +
+                          std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+                              std::chrono::duration<double>(std::max(0.0, timeout_s)));
+    while (J->state != DRWC_JOB_DONE && J->state != DRWC_JOB_FAILED) {
+        if (v->cv.wait_until(lk, deadline) == std::cv_status::timeout &&
+            J->state != DRWC_JOB_DONE && J->state != DRWC_JOB_FAILED)
+            return DRWC_ERR_TIMEOUT;
+    }
+    if (J->state == DRWC_JOB_FAILED) return J->error ? J->error : DRWC_ERR_SHUTDOWN;
+    if (out) *out = J->result;
+    return DRWC_OK;
+}
+
+DRWC_API int drwc_server_job_times(drwc_server* v, int64_t id, double* queued_s, double* latency_s) {
+    if (!v) return DRWC_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(v->mu);
+    auto it = v->jobs.find(id);
+    if (it == v->jobs.end()) return DRWC_ERR_INVALID;
+    const SvHostJob* J = it->second.get();
+    if (J->state != DRWC_JOB_DONE) return DRWC_ERR_INVALID;
+    if (queued_s) *queued_s = sv_secs(J->t_submit, J->t_admit);
+    if (latency_s) *latency_s = sv_secs(J->t_submit, J->t_done);
+    return DRWC_OK;
+}
+
+DRWC_API int drwc_server_stats_get(drwc_server* v, drwc_server_stats* out) {
+    if (!v || !out) return DRWC_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(v->mu);
+    drwc_server_stats s = v->st;
+    s.queued = (int64_t)v->queue.size();
+    s.running = 0;
+    for (int q = 0; q < kSvMaxJobs; ++q) s.running += v->table[q] && !v->table[q]->draining;
+    s.arena_bytes = (int64_t)v->arena.size;
+    s.arena_used = (int64_t)v->arena.used;
+    s.arena_peak = (int64_t)v->arena.peak;
+    *out = s;
+    return v->thread_error;
+}
+
+}  // extern "C"

@@ -29,187 +29,9 @@
 #include <type_traits>
 #include <vector>
 
-#include "fdm_cube.cuh"
-#include "host.cuh"
-#include "sample.cuh"
+#include "geom.cuh"
 
 namespace drwc {
-
-FdmParams make_params(const drwc_fdm_opts* o, int N);
-
-constexpr double kEps0FfPerUm = 8.8541878128e-3;  // vacuum permittivity, fF/um
-constexpr int kBruteBoxes = 16;                  // <= this many boxes: scan all
-
-constexpr int kMaxMaterials = 32;              // distinct permittivities per structure
-
-struct DevGeom {
-    int n_boxes, n_nets, n_layers, n_diel;
-    const double* box;      // n_boxes x 6 (lo xyz, hi xyz)
-    const int* net;         // n_boxes
-    const double* zlo;      // n_layers
-    const int* lmat;        // n_layers material ids
-    const double* diel;     // n_diel x 7 (eps slot unused on the device)
-    const int* dmat;        // n_diel material ids
-    const double* pal;      // n_mat distinct permittivities
-    const double* pair64;   // n_mat x n_mat conductances e e' / (e + e')
-    const float* pair32;
-    int n_mat;
-    double encl_lo[3], encl_hi[3];
-    // uniform grid over the enclosure (CSR cell -> boxes)
-    int gdim[3];
-    double gcell[3];
-    double gmin_cell;
-    const int* gstart;      // ncells + 1
-    const int* gitems;
-};
-
-struct Gauss {
-    double lo[3], hi[3], area[6], total;
-};
-
-struct WalkParams {
-    int N, max_hops, master;
-    double stop;
-    uint64_t seed;
-    FdmParams prm;
-    // optional hop log: centre + half-width (4 doubles) and solver code per hop
-    double* log;
-    int* log_code;
-    unsigned int* log_count;
-    unsigned int log_cap;
-};
-
-// ------------------------------------------------------------------ geometry
-DRWC_DEV double box_dist(const double* b, const double r[3]) {
-    double d = 0.0;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const double lo = dsub(b[a], r[a]);
-        const double hi = dsub(r[a], b[3 + a]);
-        const double m = lo > hi ? lo : hi;
-        if (m > d) d = m;
-    }
-    return d;
-}
-
-DRWC_DEV double encl_dist(const DevGeom& g, const double r[3]) {
-    double best = CUDART_INF;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const double d1 = dsub(r[a], g.encl_lo[a]);
-        const double d2 = dsub(g.encl_hi[a], r[a]);
-        if (d1 < best) best = d1;
-        if (d2 < best) best = d2;
-    }
-    return best;
-}
-
-// Nearest conductor (L-infinity) for warp 0: the enclosure wins ties, then
-// the lowest box index. Result in lane 0 (and broadcast to the warp).
-DRWC_DEV void nearest(const DevGeom& g, const double r[3], double* d_out, int* net_out) {
-    const int lane = threadIdx.x & 31;
-    double best = CUDART_INF;
-    int bidx = 0x7fffffff;
-    if (g.n_boxes <= kBruteBoxes || g.gstart == nullptr) {
-        for (int b = lane; b < g.n_boxes; b += 32) {
-            const double d = box_dist(g.box + 6 * b, r);
-            if (d < best || (d == best && b < bidx)) { best = d; bidx = b; }
-        }
-    } else if (lane == 0) {
-        int ci[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            int v = (int)floor((r[a] - g.encl_lo[a]) / g.gcell[a]);
-            ci[a] = v < 0 ? 0 : (v >= g.gdim[a] ? g.gdim[a] - 1 : v);
-        }
-        const double dwall = encl_dist(g, r);
-        const int rmax = max(g.gdim[0], max(g.gdim[1], g.gdim[2]));
-        for (int ring = 0; ring <= rmax; ++ring) {
-            // boxes not met in rings < ring lie at least (ring-1) cells away
-            const double reach = (double)(ring - 1) * g.gmin_cell * (1.0 - 1e-12);
-            if (ring > 1 && (best < reach || dwall < reach)) break;
-            for (int z = ci[2] - ring; z <= ci[2] + ring; ++z) {
-                if (z < 0 || z >= g.gdim[2]) continue;
-                for (int y = ci[1] - ring; y <= ci[1] + ring; ++y) {
-                    if (y < 0 || y >= g.gdim[1]) continue;
-                    for (int x = ci[0] - ring; x <= ci[0] + ring; ++x) {
-                        if (x < 0 || x >= g.gdim[0]) continue;
-                        const int cheb = max(abs(x - ci[0]), max(abs(y - ci[1]), abs(z - ci[2])));
-                        if (cheb != ring) continue;
-                        const int cell = x + g.gdim[0] * (y + g.gdim[1] * z);
-                        for (int it = g.gstart[cell]; it < g.gstart[cell + 1]; ++it) {
-                            const int b = g.gitems[it];
-                            const double d = box_dist(g.box + 6 * b, r);
-                            if (d < best || (d == best && b < bidx)) { best = d; bidx = b; }
-                        }
-                    }
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
-        if (ob < best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
-    }
-    const double dw = encl_dist(g, r);
-    if (dw <= best) {
-        *d_out = dw;
-        *net_out = g.n_nets;
-    } else {
-        *d_out = best;
-        *net_out = g.net[bidx];
-    }
-}
-
-// Material id at a point: first containing dielectric block, else the last
-// stratified layer with zlo <= z (layer 0 below all of them).
-DRWC_DEV int mat_at(const DevGeom& g, const double p[3]) {
-    for (int b = 0; b < g.n_diel; ++b) {
-        const double* D = g.diel + 7 * b;
-        if (p[0] >= D[0] && p[0] <= D[3] && p[1] >= D[1] && p[1] <= D[4] && p[2] >= D[2] &&
-            p[2] <= D[5])
-            return g.dmat[b];
-    }
-    if (g.n_layers <= 0) return 0;
-    int li = 0;
-    for (int l = 0; l < g.n_layers; ++l) {
-        if (p[2] >= g.zlo[l]) li = l;
-        else break;
-    }
-    return g.lmat[li];
-}
-
-// Cell-centre offsets (2i+1)/N - 1, rounded exactly as the CPU walk computes them.
-template <int N>
-DRWC_DEV void centre_offsets(double* tco) {
-    for (int i = threadIdx.x; i < N; i += blockDim.x)
-        tco[i] = dsub(ddiv(dadd(dmul(2.0, (double)i), 1.0), (double)N), 1.0);
-}
-
-template <int N>
-DRWC_DEV void voxelise(const DevGeom& g, const double c[3], double a, const double* tco,
-                       uint8_t* mat) {
-    for (int v = threadIdx.x; v < N * N * N; v += blockDim.x) {
-        const int i = v % N, j = (v / N) % N, k = v / (N * N);
-        double p[3];
-        p[0] = dadd(c[0], dmul(a, tco[i]));
-        p[1] = dadd(c[1], dmul(a, tco[j]));
-        p[2] = dadd(c[2], dmul(a, tco[k]));
-        mat[v] = (uint8_t)mat_at(g, p);
-    }
-}
-
-// Shared memory beyond the solver's: material ids, cell-centre offsets, the
-// palette and its pair-conductance tables.
-template <int N>
-struct WalkSmem {
-    static size_t bytes(int P) {
-        return Cube<N>::kSmemBytes + ((size_t)N * N * N + 15) / 16 * 16 + 8 * N + 16 * P +
-               8 * (size_t)P * P + 4 * (size_t)P * P + 16;
-    }
-};
 
 struct WalkState {
     double r[3];
@@ -267,22 +89,7 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
         const uint64_t w = (uint64_t)(walk0 + idx);
         // ---- start point on the Gaussian surface
         if (t == 0) {
-            const double2 u = philox_uniform2(W.seed, w, 0, 0);
-            const double2 v = philox_uniform2(W.seed, w, 0, 1);
-            const double target = dmul(u.x, G.total);
-            double run = 0.0;
-            int f = 5;
-            for (int q = 0; q < 6; ++q) {
-                run = dadd(run, G.area[q]);
-                if (run > target) { f = q; break; }
-            }
-            const int axis = f < 2 ? 2 : f < 4 ? 1 : 0;
-            const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
-            S.r[t0] = dadd(G.lo[t0], dmul(u.y, dsub(G.hi[t0], G.lo[t0])));
-            S.r[t1] = dadd(G.lo[t1], dmul(v.x, dsub(G.hi[t1], G.lo[t1])));
-            S.r[axis] = (f & 1) ? G.hi[axis] : G.lo[axis];
-            S.sgn_out = (f & 1) ? 1.0 : -1.0;
-            S.code = axis == 0 ? DRWC_WVTX : axis == 1 ? DRWC_WVTY : DRWC_WVTZ;
+            walk_start_point(G, W.seed, w, S.r, &S.sgn_out, &S.code);
             S.hops = 0;
             S.done = 0;
             S.omega = 0.0;
@@ -338,16 +145,9 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
                     S.net = -1;  // no transition possible: count as lost
                     S.done = 2;
                 } else {
-                    if (first) {
-                        const double sg = wv[b] < 0.0 ? -1.0 : 1.0;
-                        const double eps_w = center_diel<N>(E, code);
-                        double om = dmul(-S.sgn_out, G.total);
-                        om = dmul(om, eps_w);
-                        om = dmul(om, tot);
-                        om = dmul(om, sg);
-                        om = ddiv(om, a);
-                        S.omega = dmul(om, kEps0FfPerUm);
-                    }
+                    if (first)
+                        S.omega = first_hop_weight(G, S.sgn_out, center_diel<N>(E, code), tot,
+                                                   wv[b], a);
                     double loc[3];
                     locate_f64(N, b, loc);
                     for (int d = 0; d < 3; ++d) S.r[d] = dadd(S.r[d], dmul(a, loc[d]));
@@ -371,37 +171,12 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
     }
 }
 
-// Per-entry sums of one batch of walk records, fixed order: block e sums
-// entry e (0..n_nets = ground) over all walks; lost walks (net -1) go to the
-// last slot. out[e] = {sum w, sum w^2, count}.
-__global__ void reduce_kernel(int n_entries, long long nw, const int32_t* __restrict__ end,
-                              const double* __restrict__ w,
-                              double* __restrict__ out) {
-    const int e = blockIdx.x;  // 0..n_entries (n_entries = lost + hops slot)
-    double s = 0, s2 = 0, cnt = 0;
-    for (long long i = threadIdx.x; i < nw; i += blockDim.x) {
-        const int ne = end[i] < 0 ? n_entries : end[i];
-        if (ne == e) {
-            const double v = w[i];
-            s += v; s2 += v * v; cnt += 1.0;
-        }
-    }
-    __shared__ double r0[256], r1[256], r2[256];
-    r0[threadIdx.x] = s; r1[threadIdx.x] = s2; r2[threadIdx.x] = cnt;
-    __syncthreads();
-    for (int o = 128; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) {
-            r0[threadIdx.x] += r0[threadIdx.x + o];
-            r1[threadIdx.x] += r1[threadIdx.x + o];
-            r2[threadIdx.x] += r2[threadIdx.x + o];
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        out[3 * e + 0] = r0[0];
-        out[3 * e + 1] = r1[0];
-        out[3 * e + 2] = r2[0];
-    }
+// Per-entry sums of one batch of walk records: block e sums entry e.
+__global__ void __launch_bounds__(256) reduce_kernel(int n_entries, long long nw,
+                                                     const int32_t* __restrict__ end,
+                                                     const double* __restrict__ w,
+                                                     double* __restrict__ out) {
+    reduce_entry(blockIdx.x, n_entries, nw, end, w, out);
 }
 
 __global__ void hop_sum_kernel(long long nw, const int32_t* __restrict__ hops,
@@ -416,223 +191,6 @@ __global__ void hop_sum_kernel(long long nw, const int32_t* __restrict__ hops,
 }
 
 // ------------------------------------------------------------------ host side
-struct HostGeom {
-    std::vector<double> box, zlo, diel, pal, pair64;
-    std::vector<float> pair32;
-    std::vector<int> net, gstart, gitems, lmat, dmat;
-    DevGeom dev{};
-    void* dbuf = nullptr;
-};
-
-static int validate(const drwc_structure* s) {
-    if (!s || s->n_boxes < 1 || s->n_nets < 1 || s->n_nets > DRWC_MAX_NETS || !s->boxes)
-        return DRWC_ERR_INVALID;
-    if (s->n_layers < 0 || s->n_diel < 0) return DRWC_ERR_INVALID;
-    if (s->n_layers > 0 && (!s->layer_zlo || !s->layer_eps)) return DRWC_ERR_INVALID;
-    if (s->n_diel > 0 && !s->diel) return DRWC_ERR_INVALID;
-    for (int a = 0; a < 3; ++a)
-        if (!(s->encl_hi[a] > s->encl_lo[a])) return DRWC_ERR_GEOMETRY;
-    for (int b = 0; b < s->n_boxes; ++b) {
-        const drwc_box& B = s->boxes[b];
-        if (B.net < 0 || B.net >= s->n_nets) return DRWC_ERR_INVALID;
-        for (int a = 0; a < 3; ++a)
-            if (!(B.hi[a] > B.lo[a]) || B.lo[a] < s->encl_lo[a] || B.hi[a] > s->encl_hi[a])
-                return DRWC_ERR_GEOMETRY;
-    }
-    for (int l = 0; l < s->n_layers; ++l) {
-        if (!(s->layer_eps[l] > 0)) return DRWC_ERR_INVALID;
-        if (l > 0 && !(s->layer_zlo[l] >= s->layer_zlo[l - 1])) return DRWC_ERR_INVALID;
-    }
-    for (int d = 0; d < s->n_diel; ++d)
-        if (!(s->diel[d].eps > 0)) return DRWC_ERR_INVALID;
-    return DRWC_OK;
-}
-
-static int upload_geom(drwc_ctx* ctx, const drwc_structure* s, HostGeom* h) {
-    const int nb = s->n_boxes;
-    h->box.resize(6 * nb);
-    h->net.resize(nb);
-    for (int b = 0; b < nb; ++b) {
-        for (int a = 0; a < 3; ++a) {
-            h->box[6 * b + a] = s->boxes[b].lo[a];
-            h->box[6 * b + 3 + a] = s->boxes[b].hi[a];
-        }
-        h->net[b] = s->boxes[b].net;
-    }
-    h->zlo.assign(s->layer_zlo, s->layer_zlo + s->n_layers);
-    // material palette: distinct permittivities of layers and blocks
-    h->pal.clear();
-    auto mat_of = [&](double e) {
-        for (size_t m = 0; m < h->pal.size(); ++m)
-            if (h->pal[m] == e) return (int)m;
-        h->pal.push_back(e);
-        return (int)h->pal.size() - 1;
-    };
-    h->lmat.resize(s->n_layers);
-    for (int l = 0; l < s->n_layers; ++l) h->lmat[l] = mat_of(s->layer_eps[l]);
-    if (s->n_layers == 0) mat_of(1.0);  // vacuum when no layer is given
-    h->dmat.resize(s->n_diel);
-    for (int d = 0; d < s->n_diel; ++d) h->dmat[d] = mat_of(s->diel[d].eps);
-    const int P = (int)h->pal.size();
-    if (P > kMaxMaterials) return DRWC_ERR_GEOMETRY;
-    h->pair64.resize((size_t)P * P);
-    h->pair32.resize((size_t)P * P);
-    for (int a = 0; a < P; ++a)
-        for (int b = 0; b < P; ++b) {
-            const double e1 = h->pal[a], e2 = h->pal[b];
-            h->pair64[a * P + b] = e1 * e2 / (e1 + e2);
-            const float f1 = (float)e1, f2 = (float)e2;
-            h->pair32[a * P + b] = f1 * f2 / (f1 + f2);
-        }
-    h->diel.resize(7 * s->n_diel);
-    for (int d = 0; d < s->n_diel; ++d) {
-        for (int a = 0; a < 3; ++a) {
-            h->diel[7 * d + a] = s->diel[d].lo[a];
-            h->diel[7 * d + 3 + a] = s->diel[d].hi[a];
-        }
-        h->diel[7 * d + 6] = s->diel[d].eps;
-    }
-    // uniform grid: about 4 cells per box, at most 128 per axis
-    double ext[3], vol = 1.0;
-    for (int a = 0; a < 3; ++a) {
-        ext[a] = s->encl_hi[a] - s->encl_lo[a];
-        vol *= ext[a];
-    }
-    const double hcell = std::cbrt(vol / (4.0 * nb));
-    int dim[3];
-    double cell[3], minc = 1e300;
-    for (int a = 0; a < 3; ++a) {
-        dim[a] = (int)std::min(128.0, std::max(1.0, std::ceil(ext[a] / hcell)));
-        cell[a] = ext[a] / dim[a];
-        minc = std::min(minc, cell[a]);
-    }
-    const int ncell = dim[0] * dim[1] * dim[2];
-    std::vector<std::vector<int>> lists(ncell);
-    for (int b = 0; b < nb; ++b) {
-        int lo[3], hi[3];
-        for (int a = 0; a < 3; ++a) {
-            lo[a] = (int)std::floor((s->boxes[b].lo[a] - s->encl_lo[a]) / cell[a]) - 1;
-            hi[a] = (int)std::floor((s->boxes[b].hi[a] - s->encl_lo[a]) / cell[a]) + 1;
-            lo[a] = std::max(0, lo[a]);
-            hi[a] = std::min(dim[a] - 1, hi[a]);
-        }
-        for (int z = lo[2]; z <= hi[2]; ++z)
-            for (int y = lo[1]; y <= hi[1]; ++y)
-                for (int x = lo[0]; x <= hi[0]; ++x) {
-                    // keep the box in every cell its (slightly grown) extent touches
-                    const double cx0 = s->encl_lo[0] + x * cell[0], cx1 = cx0 + cell[0];
-                    const double cy0 = s->encl_lo[1] + y * cell[1], cy1 = cy0 + cell[1];
-                    const double cz0 = s->encl_lo[2] + z * cell[2], cz1 = cz0 + cell[2];
-                    const double tol = 1e-9 * minc;
-                    if (s->boxes[b].lo[0] <= cx1 + tol && s->boxes[b].hi[0] >= cx0 - tol &&
-                        s->boxes[b].lo[1] <= cy1 + tol && s->boxes[b].hi[1] >= cy0 - tol &&
-                        s->boxes[b].lo[2] <= cz1 + tol && s->boxes[b].hi[2] >= cz0 - tol)
-                        lists[x + dim[0] * (y + dim[1] * z)].push_back(b);
-                }
-    }
-    h->gstart.assign(ncell + 1, 0);
-    for (int c = 0; c < ncell; ++c) h->gstart[c + 1] = h->gstart[c] + (int)lists[c].size();
-    h->gitems.clear();
-    for (int c = 0; c < ncell; ++c) h->gitems.insert(h->gitems.end(), lists[c].begin(), lists[c].end());
-    if (h->gitems.empty()) h->gitems.push_back(0);
-
-    size_t off = 0;
-    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
-    const size_t o_box = take(h->box.size() * 8), o_net = take(h->net.size() * 4),
-                 o_zlo = take(std::max<size_t>(1, h->zlo.size()) * 8),
-                 o_lmat = take(std::max<size_t>(1, h->lmat.size()) * 4),
-                 o_dmat = take(std::max<size_t>(1, h->dmat.size()) * 4),
-                 o_pal = take(h->pal.size() * 8), o_p64 = take(h->pair64.size() * 8),
-                 o_p32 = take(h->pair32.size() * 4),
-                 o_diel = take(std::max<size_t>(1, h->diel.size()) * 8),
-                 o_gs = take(h->gstart.size() * 4), o_gi = take(h->gitems.size() * 4);
-    void* d = nullptr;
-    int rc = ws_get(ctx, WS_AUX2, off, &d);
-    if (rc) return rc;
-    std::vector<unsigned char> hb(off, 0);
-    std::memcpy(hb.data() + o_box, h->box.data(), h->box.size() * 8);
-    std::memcpy(hb.data() + o_net, h->net.data(), h->net.size() * 4);
-    if (!h->zlo.empty()) std::memcpy(hb.data() + o_zlo, h->zlo.data(), h->zlo.size() * 8);
-    if (!h->lmat.empty()) std::memcpy(hb.data() + o_lmat, h->lmat.data(), h->lmat.size() * 4);
-    if (!h->dmat.empty()) std::memcpy(hb.data() + o_dmat, h->dmat.data(), h->dmat.size() * 4);
-    std::memcpy(hb.data() + o_pal, h->pal.data(), h->pal.size() * 8);
-    std::memcpy(hb.data() + o_p64, h->pair64.data(), h->pair64.size() * 8);
-    std::memcpy(hb.data() + o_p32, h->pair32.data(), h->pair32.size() * 4);
-    if (!h->diel.empty()) std::memcpy(hb.data() + o_diel, h->diel.data(), h->diel.size() * 8);
-    std::memcpy(hb.data() + o_gs, h->gstart.data(), h->gstart.size() * 4);
-    std::memcpy(hb.data() + o_gi, h->gitems.data(), h->gitems.size() * 4);
-    DRWC_CUDA_TRY(cudaMemcpyAsync(d, hb.data(), off, cudaMemcpyHostToDevice, ctx->stream));
-    unsigned char* base = (unsigned char*)d;
-    DevGeom& g = h->dev;
-    g.n_boxes = nb;
-    g.n_nets = s->n_nets;
-    g.n_layers = s->n_layers;
-    g.n_diel = s->n_diel;
-    g.box = (const double*)(base + o_box);
-    g.net = (const int*)(base + o_net);
-    g.zlo = (const double*)(base + o_zlo);
-    g.lmat = (const int*)(base + o_lmat);
-    g.dmat = (const int*)(base + o_dmat);
-    g.pal = (const double*)(base + o_pal);
-    g.pair64 = (const double*)(base + o_p64);
-    g.pair32 = (const float*)(base + o_p32);
-    g.n_mat = (int)h->pal.size();
-    g.diel = (const double*)(base + o_diel);
-    for (int a = 0; a < 3; ++a) {
-        g.encl_lo[a] = s->encl_lo[a];
-        g.encl_hi[a] = s->encl_hi[a];
-        g.gdim[a] = dim[a];
-        g.gcell[a] = cell[a];
-    }
-    g.gmin_cell = minc;
-    g.gstart = (const int*)(base + o_gs);
-    g.gitems = (const int*)(base + o_gi);
-    h->dbuf = d;
-    return DRWC_OK;
-}
-
-// Same arithmetic (order, no contraction) as the CPU restatement.
-static int gauss_build(const drwc_structure* s, const drwc_job_params* p, Gauss* G) {
-    for (int a = 0; a < 3; ++a) {
-        G->lo[a] = INFINITY;
-        G->hi[a] = -INFINITY;
-    }
-    bool any = false;
-    for (int b = 0; b < s->n_boxes; ++b) {
-        if (s->boxes[b].net != p->master) continue;
-        any = true;
-        for (int a = 0; a < 3; ++a) {
-            if (s->boxes[b].lo[a] < G->lo[a]) G->lo[a] = s->boxes[b].lo[a];
-            if (s->boxes[b].hi[a] > G->hi[a]) G->hi[a] = s->boxes[b].hi[a];
-        }
-    }
-    if (!any) return DRWC_ERR_INVALID;
-    for (int a = 0; a < 3; ++a) {
-        volatile double lo = G->lo[a] - p->gauss_offset;
-        volatile double hi = G->hi[a] + p->gauss_offset;
-        G->lo[a] = lo;
-        G->hi[a] = hi;
-        if (lo < s->encl_lo[a] || hi > s->encl_hi[a]) return DRWC_ERR_GEOMETRY;
-    }
-    // the Gaussian surface must not cut another net's box
-    for (int b = 0; b < s->n_boxes; ++b) {
-        if (s->boxes[b].net == p->master) continue;
-        bool overlap = true;
-        for (int a = 0; a < 3; ++a)
-            overlap &= s->boxes[b].lo[a] < G->hi[a] && s->boxes[b].hi[a] > G->lo[a];
-        if (overlap) return DRWC_ERR_GEOMETRY;
-    }
-    volatile double dx = G->hi[0] - G->lo[0], dy = G->hi[1] - G->lo[1], dz = G->hi[2] - G->lo[2];
-    volatile double az = dx * dy, ay = dx * dz, ax = dy * dz;
-    G->area[0] = az; G->area[1] = az;
-    G->area[2] = ay; G->area[3] = ay;
-    G->area[4] = ax; G->area[5] = ax;
-    volatile double tot = 0;
-    for (int f = 0; f < 6; ++f) tot = tot + G->area[f];
-    G->total = tot;
-    return DRWC_OK;
-}
-
 // Resident CTAs per SM for a given palette size (the shared-memory request
 // grows with it); the attribute is set once for the largest palette.
 template <int N>
@@ -684,34 +242,6 @@ static int launch_walks(drwc_ctx* ctx, const HostGeom& hg, const Gauss& G, const
             hg.dev, G, P, walk0, nw, wb.counter, wb.counter + 2, wb.end, wb.hops, wb.w, sy, sf);
         return launch_check(ctx);
     });
-}
-
-static int prepare(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
-                   HostGeom* hg, Gauss* G, WalkParams* P) {
-    int rc = validate(s);
-    if (rc) return rc;
-    if (!p || !n_supported(p->N) || p->master < 0 || p->master >= s->n_nets ||
-        !(p->gauss_offset > 0) || !(p->stop_dist > 0) || p->max_hops < 1)
-        return DRWC_ERR_INVALID;
-    rc = gauss_build(s, p, G);
-    if (rc) return rc;
-    rc = upload_geom(ctx, s, hg);
-    if (rc) return rc;
-    P->N = p->N;
-    P->max_hops = p->max_hops;
-    P->master = p->master;
-    P->stop = p->stop_dist;
-    P->seed = p->seed;
-    P->prm = make_params(&p->fdm, p->N);
-    P->log = nullptr;
-    P->log_code = nullptr;
-    P->log_count = nullptr;
-    P->log_cap = 0;
-    if (p->fdm.warm_start) {
-        rc = warm_tables(ctx, p->N, P->prm.warm);
-        if (rc) return rc;
-    }
-    return DRWC_OK;
 }
 
 static int walk_buffers(drwc_ctx* ctx, long long nw, int n_entries, WalkBuffers* wb) {
@@ -777,16 +307,15 @@ DRWC_API int drwc_job_create(drwc_ctx* ctx, const drwc_structure* s, const drwc_
     int rc = prepare(ctx, s, p, &j->hg, &j->G, &j->P);
     if (rc) { delete j; return rc; }
     // the job owns its geometry copy (the context workspace is shared)
-    const size_t bytes = ctx->ws_bytes[WS_AUX2];
     void* own = nullptr;
-    if (cudaMalloc(&own, bytes) != cudaSuccess) { cudaGetLastError(); delete j; return DRWC_ERR_NOMEM; }
-    DRWC_CUDA_TRY(cudaMemcpyAsync(own, j->hg.dbuf, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-    const ptrdiff_t shift = (unsigned char*)own - (unsigned char*)j->hg.dbuf;
-    DevGeom& g = j->hg.dev;
-    auto mv = [&](auto*& ptr) { ptr = (std::remove_reference_t<decltype(ptr)>)((const unsigned char*)ptr + shift); };
-    mv(g.box); mv(g.net); mv(g.zlo); mv(g.lmat); mv(g.dmat); mv(g.diel); mv(g.pal);
-    mv(g.pair64); mv(g.pair32); mv(g.gstart); mv(g.gitems);
-    j->hg.dbuf = own;
+    if (cudaMalloc(&own, j->hg.blob.size()) != cudaSuccess) {
+        cudaGetLastError();
+        delete j;
+        return DRWC_ERR_NOMEM;
+    }
+    DRWC_CUDA_TRY(cudaMemcpyAsync(own, j->hg.blob.data(), j->hg.blob.size(),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+    bind_geom(&j->hg, own);
     j->n_entries = s->n_nets + 1;
     j->h2d_bytes = (int64_t)(j->hg.box.size() * 8 + j->hg.net.size() * 4 + j->hg.zlo.size() * 8 +
                              j->hg.lmat.size() * 4 + j->hg.dmat.size() * 4 +
@@ -990,59 +519,6 @@ DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job
 
 namespace drwc {
 
-// Cell-centre points of a cube in the frame the gradient head works in: the
-// gradient axis becomes z'. rot = 0: identity; rot = 1 (x gradient):
-// (x, y, z) = (z', x', y'); rot = 2 (y gradient): (x, y, z) = (y', z', x').
-DRWC_DEV void rotated_point(const double c[3], double a, const double* tco, int i, int j, int k,
-                            int rot, double p[3]) {
-    int ax, ay, az;  // original-axis offsets taken from rotated indices
-    if (rot == 1) { ax = k; ay = i; az = j; }
-    else if (rot == 2) { ax = j; ay = k; az = i; }
-    else { ax = i; ay = j; az = k; }
-    p[0] = dadd(c[0], dmul(a, tco[ax]));
-    p[1] = dadd(c[1], dmul(a, tco[ay]));
-    p[2] = dadd(c[2], dmul(a, tco[az]));
-}
-
-DRWC_DEV void unrotate(int rot, const double v[3], double out[3]) {
-    if (rot == 1) { out[0] = v[2]; out[1] = v[0]; out[2] = v[1]; }
-    else if (rot == 2) { out[0] = v[1]; out[1] = v[2]; out[2] = v[0]; }
-    else { out[0] = v[0]; out[1] = v[1]; out[2] = v[2]; }
-}
-
-DRWC_DEV int rot_of_code(int code) { return code == DRWC_WVTX ? 1 : code == DRWC_WVTY ? 2 : 0; }
-
-// CTA-wide: voxelise one cube (rotated frame) into BF16 eps / max eps and,
-// optionally, FP64 eps; returns the centre permittivity of the gradient
-// convention (thread 0's value valid).
-template <int N>
-DRWC_DEV void voxelise_net(const DevGeom& g, const double c[3], double a, int rot,
-                           const double* tco, const double* palsm, uint8_t* matsm,
-                           __nv_bfloat16* X, double* eps64, float* red) {
-    constexpr int NNN = N * N * N;
-    float mx = 0.f;
-    for (int v = threadIdx.x; v < NNN; v += blockDim.x) {
-        const int i = v % N, j = (v / N) % N, k = v / (N * N);
-        double p[3];
-        rotated_point(c, a, tco, i, j, k, rot, p);
-        const int m = mat_at(g, p);
-        matsm[v] = (uint8_t)m;
-        mx = fmaxf(mx, (float)palsm[m]);
-    }
-    for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-    __syncthreads();
-    float m = red[0];
-    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmaxf(m, red[w]);
-    const float inv = 1.f / m;
-    for (int v = threadIdx.x; v < NNN; v += blockDim.x) {
-        const double e = palsm[matsm[v]];
-        X[v] = __float2bfloat16((float)e * inv);
-        if (eps64) eps64[v] = e;
-    }
-    __syncthreads();
-}
-
 // Hop-log records -> network inputs (and FP64 permittivity for the FDM
 // targets). Records of first hops are voxelised in the rotated frame of
 // their gradient axis, so their target is always WVTZ.
@@ -1234,23 +710,6 @@ namespace drwc {
 
 constexpr int kDecRowsLw = DRWC_NET_OUT;  // network output row (logits + confidence)
 
-// log-sum-exp of M FP32 values over the CTA (all threads get it).
-template <int NW>
-DRWC_DEV double block_lse(const float* o, int M, double* red) {
-    float mx = -1e30f;
-    for (int j = threadIdx.x; j < M; j += blockDim.x) mx = fmaxf(mx, o[j]);
-    for (int s = 16; s > 0; s >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, s));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = (double)mx;
-    __syncthreads();
-    double m = red[0];
-    for (int w = 1; w < NW; ++w) m = fmax(m, red[w]);
-    __syncthreads();
-    double se = 0.0;
-    for (int j = threadIdx.x; j < M; j += blockDim.x) se += exp((double)o[j] - m);
-    se = block_sum_d<NW>(se, red, 0);
-    return log(se) + m;
-}
-
 struct LwState {
     double *px, *py, *pz, *omega, *sgn, *a, *epsw;
     long long* walk;
@@ -1286,26 +745,12 @@ struct LwArgs {
 };
 
 DRWC_DEV void lw_start(const LwArgs& A, int slot, long long w) {
-    const Gauss& G = A.G;
-    const uint64_t wu = (uint64_t)w;
-    const double2 u = philox_uniform2(A.W.seed, wu, 0, 0);
-    const double2 v = philox_uniform2(A.W.seed, wu, 0, 1);
-    const double target = dmul(u.x, G.total);
-    double run = 0.0;
-    int f = 5;
-    for (int q = 0; q < 6; ++q) {
-        run = dadd(run, G.area[q]);
-        if (run > target) { f = q; break; }
-    }
-    const int axis = f < 2 ? 2 : f < 4 ? 1 : 0;
-    const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
-    double r[3];
-    r[t0] = dadd(G.lo[t0], dmul(u.y, dsub(G.hi[t0], G.lo[t0])));
-    r[t1] = dadd(G.lo[t1], dmul(v.x, dsub(G.hi[t1], G.lo[t1])));
-    r[axis] = (f & 1) ? G.hi[axis] : G.lo[axis];
+    double r[3], sgn;
+    int code;
+    walk_start_point(A.G, A.W.seed, (uint64_t)w, r, &sgn, &code);
     A.st.px[slot] = r[0]; A.st.py[slot] = r[1]; A.st.pz[slot] = r[2];
-    A.st.sgn[slot] = (f & 1) ? 1.0 : -1.0;
-    A.st.code[slot] = axis == 0 ? DRWC_WVTX : axis == 1 ? DRWC_WVTY : DRWC_WVTZ;
+    A.st.sgn[slot] = sgn;
+    A.st.code[slot] = code;
     A.st.hops[slot] = 0;
     A.st.omega[slot] = 0.0;
     A.st.walk[slot] = w;
@@ -1459,13 +904,8 @@ __global__ void __launch_bounds__(256) lw_sample_kernel(LwArgs A) {
             if (first) {
                 const int rot = rot_of_code(A.st.code[slot]);
                 unrotate(rot, loc, mv);
-                const double sg = wv[b] < 0.0 ? -1.0 : 1.0;
-                double om = dmul(-A.st.sgn[slot], A.G.total);
-                om = dmul(om, A.st.epsw[slot]);
-                om = dmul(om, tot);
-                om = dmul(om, sg);
-                om = ddiv(om, a);
-                A.st.omega[slot] = dmul(om, kEps0FfPerUm);
+                A.st.omega[slot] =
+                    first_hop_weight(A.G, A.st.sgn[slot], A.st.epsw[slot], tot, wv[b], a);
             } else {
                 mv[0] = loc[0]; mv[1] = loc[1]; mv[2] = loc[2];
             }
@@ -1475,6 +915,7 @@ __global__ void __launch_bounds__(256) lw_sample_kernel(LwArgs A) {
             A.st.hops[slot] = h + 1;
             atomicAdd(A.ctr + 2, 1ull);
         }
+        if (threadIdx.x == 0 && b < 0) lw_finish(A, slot, -1);  // no transition: lost
         __syncthreads();
     }
 }
@@ -1553,16 +994,9 @@ lw_fdm_kernel(LwArgs A, double* __restrict__ scratch_y, float* __restrict__ scra
         double tot = 0.0;
         const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
         if (threadIdx.x == 0 && b >= 0 && st.status != 2) {
-            if (first) {
-                const double sg = wv[b] < 0.0 ? -1.0 : 1.0;
-                const double eps_w = center_diel<N>(E, code);
-                double om = dmul(-A.st.sgn[slot], A.G.total);
-                om = dmul(om, eps_w);
-                om = dmul(om, tot);
-                om = dmul(om, sg);
-                om = ddiv(om, a);
-                A.st.omega[slot] = dmul(om, kEps0FfPerUm);
-            }
+            if (first)
+                A.st.omega[slot] = first_hop_weight(A.G, A.st.sgn[slot], center_diel<N>(E, code),
+                                                    tot, wv[b], a);
             double loc[3];
             locate_f64(N, b, loc);
             A.st.px[slot] = dadd(A.st.px[slot], dmul(a, loc[0]));
@@ -1571,6 +1005,7 @@ lw_fdm_kernel(LwArgs A, double* __restrict__ scratch_y, float* __restrict__ scra
             A.st.hops[slot] = h + 1;
             atomicAdd(A.ctr + 3, 1ull);
         }
+        if (threadIdx.x == 0 && (b < 0 || st.status == 2)) lw_finish(A, slot, -1);  // lost
         __syncthreads();
     }
 }

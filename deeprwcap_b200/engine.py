@@ -539,3 +539,85 @@ def fdm_solve_device(ctx: Context, eps64, N: int, code, out, tol: float = 1e-8):
                                               ooff.ctypes.data, ptr(out), None, None, None, None),
           "drwc_fdm_solve_batch_device")
     ctx.synchronize()
+
+
+# ------------------------------------------------------------------ serving
+def server_opts(**kw) -> "abi.ServerOpts":
+    o = abi.ServerOpts()
+    load().drwc_server_opts_default(C.byref(o))
+    for k, v in kw.items():
+        if k == "sizes":
+            o.n_sizes = len(v)
+            for i, n in enumerate(v):
+                o.sizes[i] = int(n)
+        else:
+            setattr(o, k, v)
+    return o
+
+
+class Server:
+    """The persistent multi-job extraction server (drwc_server_* in
+    include/drwc.h): jobs are submitted from the host, admitted by device
+    footprint and run concurrently on the device; results come back per job.
+    With ``net`` the hops of N = 16 jobs go through the learned network."""
+
+    def __init__(self, ctx: Context | None = None, net: "Net | None" = None, **opts):
+        self.ctx = ctx or (net.ctx if net is not None else default_context())
+        self.opts = server_opts(**opts)
+        h = C.c_void_p()
+        torch_ready()
+        check(self.ctx.lib.drwc_server_create(self.ctx.h, C.byref(self.opts),
+                                              net.h if net is not None else None, C.byref(h)),
+              "drwc_server_create")
+        self.h = h
+        self.net = net
+
+    def submit(self, structure, params) -> int:
+        s = structure.to_c() if hasattr(structure, "to_c") else structure
+        jid = C.c_int64()
+        check(self.ctx.lib.drwc_server_submit(self.h, C.byref(s), C.byref(params), C.byref(jid)),
+              "drwc_server_submit")
+        return jid.value
+
+    def poll(self, jid: int):
+        """(state, JobResult or None); state is one of abi.JOB_*."""
+        st = C.c_int32()
+        r = abi.JobResult()
+        check(self.ctx.lib.drwc_server_poll(self.h, int(jid), C.byref(st), C.byref(r)),
+              "drwc_server_poll")
+        return st.value, (JobResult(r) if st.value == abi.JOB_DONE else None)
+
+    def wait(self, jid: int, timeout: float = 600.0) -> JobResult:
+        r = abi.JobResult()
+        check(self.ctx.lib.drwc_server_wait(self.h, int(jid), float(timeout), C.byref(r)),
+              "drwc_server_wait")
+        return JobResult(r)
+
+    def times(self, jid: int):
+        """(seconds queued before admission, seconds from submission to result)."""
+        q, l = C.c_double(), C.c_double()
+        check(self.ctx.lib.drwc_server_job_times(self.h, int(jid), C.byref(q), C.byref(l)),
+              "drwc_server_job_times")
+        return q.value, l.value
+
+    def stats(self) -> dict:
+        st = abi.ServerStats()
+        check(self.ctx.lib.drwc_server_stats_get(self.h, C.byref(st)), "drwc_server_stats_get")
+        return st.as_dict()
+
+    def close(self):
+        if self.h:
+            self.ctx.lib.drwc_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

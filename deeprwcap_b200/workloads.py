@@ -303,3 +303,48 @@ def job_params_plain(N: int = 16, master: int = 0, seed: int = 1, **kw) -> JobPa
     p.fdm.max_inner = kw.get("max_inner", 0)
     p.fdm.warm_start = kw.get("warm_start", 1)
     return p
+
+
+# ---------------------------------------------------------------------- serving
+@dataclass
+class ServeJob:
+    """One request of a serving stream: arrival time (s after the stream
+    starts), structure, cube resolution, walk count and seed."""
+    arrival: float
+    structure: StructureSpec
+    N: int
+    walks: int
+    seed: int
+
+
+def serving_stream(n_jobs: int = 16, rate: float = 50.0, seed: int = 0,
+                   walks=(1e5, 1e7), Ns=(16, 21, 23)) -> list:
+    """Poisson arrivals (mean `rate` jobs/s) of extraction jobs: 2-4 metal
+    layers of 4-16 wires (8-64 conductors), the dielectric of the
+    two-layer crossing (3 stratified layers) or of the dense stack (5 layers,
+    eps ~ U[2.5, 4.5], 10 blocks), N drawn from Ns, walks log-uniform in
+    `walks`. Everything is seeded."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n_jobs):
+        t += float(rng.exponential(1.0 / rate))
+        nl = int(rng.integers(2, 5))
+        nw = int(rng.integers(4, 17))
+        if rng.random() < 0.5:
+            eps, blocks = [3.9, 2.7, 4.2], 0
+        else:
+            eps, blocks = list(rng.uniform(2.5, 4.5, 5)), 10
+        s = wire_stack(nl, nw, diel_eps=eps, n_diel_blocks=blocks, seed=seed * 1000 + i,
+                       name=f"stack{nl}x{nw}")
+        N = int(Ns[int(rng.integers(0, len(Ns)))])
+        lo, hi = np.log(walks[0]), np.log(walks[1])
+        nwalks = int(np.exp(rng.uniform(lo, hi)))
+        out.append(ServeJob(t, s, N, nwalks, seed * 1000 + i + 1))
+    return out
+
+
+def serve_params(job: ServeJob, batch: int = 1 << 16, **kw) -> JobParams:
+    """A fixed-size job: exactly job.walks walks (master = wire 0)."""
+    return job_params_plain(N=job.N, seed=job.seed, min_walks=job.walks, max_walks=job.walks,
+                            batch_walks=min(batch, job.walks), **kw)

@@ -334,6 +334,81 @@ DRWC_API int drwc_frw_walks_learned(drwc_ctx* ctx, const drwc_structure* s,
                                     int32_t* end_net, int32_t* hops, double* weight,
                                     double* stats);
 
+/* ---- serving: a persistent multi-job extraction engine -------------------
+ * No counterpart in the reference (its walker runs one job per process and
+ * batches single-walker network queries through ParallelSampler,
+ * inference_cpp/src/parallel_sampler.cpp:12-211). A server owns a pool of
+ * walker slots on the device and a request thread: submitted jobs queue,
+ * are admitted first-in first-out when their device footprint (structure +
+ * two batches of walk records) fits the HBM arena and a job-table entry is
+ * free, and their walks then share the slots with every other running job.
+ * Each replay of a captured CUDA graph advances every slot by
+ * steps_per_graph hops: the geometry step of all slots, then (with a
+ * network) one batched network pass over the N = 16 cubes of all jobs, and
+ * the FDM solves bucketed by cube resolution, buckets on parallel graph
+ * branches. A job's walks are reduced batch by batch in walk-id order, so its
+ * result is bit-identical to drwc_frw_run (plain form) whatever else runs. */
+typedef struct drwc_server drwc_server;
+#define DRWC_SERVER_MAX_SIZES 4
+typedef struct drwc_server_opts {
+    int32_t slots;            /* walks in flight over all jobs (default 65536) */
+    int32_t max_jobs;         /* job-table entries, <= 64 (default 32) */
+    int64_t hbm_budget;       /* bytes of the job arena (default 1 GiB) */
+    int32_t n_sizes;          /* cube resolutions served (default 3) */
+    int32_t sizes[DRWC_SERVER_MAX_SIZES];  /* default {16, 21, 23} */
+    int32_t steps_per_graph;  /* hops per slot per graph replay (default 2, <= 8) */
+    int32_t max_materials;    /* distinct permittivities per structure (default 16) */
+    int32_t max_nets;         /* conductor nets per structure (default 64) */
+    float conf_threshold;     /* network hops: route to FDM above this predicted log10 KL */
+    float audit_frac;         /* network hops: fraction also solved by FDM */
+    int32_t timing;           /* 1: time the FDM and network stages with graph event nodes */
+    int32_t reserved_;
+} drwc_server_opts;
+DRWC_API void drwc_server_opts_default(drwc_server_opts* o);
+/* net (nullable): with a network, hops of N = 16 jobs go through it
+ * (confidence routing + audits as drwc_frw_walks_learned); without one every
+ * hop is an FDM solve. The server uses the context's stream and lock. */
+DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drwc_net* net,
+                                drwc_server** out);
+/* Stops the request thread; queued and running jobs end as failed
+ * (DRWC_ERR_SHUTDOWN). */
+DRWC_API int drwc_server_destroy(drwc_server* srv);
+/* Queue a job (structure and parameters are copied). Rejected at once when
+ * invalid, when its N is not served or its structure exceeds max_nets /
+ * max_materials. */
+DRWC_API int drwc_server_submit(drwc_server* srv, const drwc_structure* s,
+                                const drwc_job_params* p, int64_t* job_id);
+enum { DRWC_JOB_QUEUED = 0, DRWC_JOB_RUNNING = 1, DRWC_JOB_DONE = 2, DRWC_JOB_FAILED = 3 };
+/* state (host): queued / running / done / failed; out (nullable) gets the
+ * result once done, with seconds = submission to completion. Returns the
+ * job's error code when it failed. */
+DRWC_API int drwc_server_poll(drwc_server* srv, int64_t job_id, int32_t* state,
+                              drwc_job_result* out);
+/* Block until the job is done or failed (DRWC_ERR_TIMEOUT after timeout_s). */
+DRWC_API int drwc_server_wait(drwc_server* srv, int64_t job_id, double timeout_s,
+                              drwc_job_result* out);
+/* Seconds from submission to admission and to completion of a finished job. */
+DRWC_API int drwc_server_job_times(drwc_server* srv, int64_t job_id, double* queued_s,
+                                   double* latency_s);
+typedef struct drwc_server_stats {
+    int64_t submitted, admitted, completed, failed;
+    int64_t queued, running;          /* now */
+    int64_t max_running;              /* most jobs resident at once */
+    int64_t hops;                     /* hops executed (all jobs, dropped walks included) */
+    int64_t net_hops, fdm_hops, fallbacks, audits;
+    int64_t walks_finished, walks_dropped;
+    int64_t graph_launches, kernels_launched;
+    int64_t arena_bytes, arena_used, arena_peak;
+    double busy_seconds;              /* device time of the graph replays */
+    double fdm_seconds, net_seconds;  /* summed stage times (timing = 1), else 0 */
+    double net_rows;                  /* network rows evaluated */
+    double audit_kl_mean;             /* mean KL(FDM || network) over audited hops */
+    int64_t fdm_iters, fdm_sweeps;    /* FP32 CG iterations and FP64 sweeps of the FDM hops */
+    double fdm_bytes;                 /* streamed-PCG algorithmic bytes of the FDM hops */
+} drwc_server_stats;
+/* Returns the request thread's error code, if it stopped on one. */
+DRWC_API int drwc_server_stats_get(drwc_server* srv, drwc_server_stats* out);
+
 /* Run one extraction job (master row of the capacitance matrix) to
  * convergence on the device. Host structure in, host result out. */
 DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,

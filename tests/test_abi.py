@@ -57,3 +57,23 @@ def test_product_does_not_import_oracle():
         if f.suffix in (".py", ".cu", ".cuh", ".cpp", ".h"):
             txt = f.read_text()
             assert "oracle" not in re.sub(r"#.*|//.*", "", txt).replace("oracle/_ref", ""), f
+
+
+def test_server_defaults_and_argument_checks_without_device():
+    """The server's option defaults (struct layout shared with the header)
+    and the checks that reject a request before any CUDA call."""
+    from deeprwcap_b200 import abi, engine
+    L = abi.load()
+    o = engine.server_opts()
+    assert (o.slots, o.max_jobs, o.hbm_budget, o.n_sizes) == (65536, 32, 1 << 30, 3)
+    assert list(o.sizes[:3]) == [16, 21, 23] and o.steps_per_graph == 2
+    assert o.max_materials == 16 and o.max_nets == 64 and abs(o.audit_frac - 0.01) < 1e-7
+    o2 = engine.server_opts(sizes=(16, 23), slots=1024)
+    assert o2.n_sizes == 2 and list(o2.sizes[:2]) == [16, 23] and o2.slots == 1024
+    h = C.c_void_p()
+    assert L.drwc_server_create(None, C.byref(o), None, C.byref(h)) == 1
+    assert L.drwc_server_destroy(None) == 1
+    st = abi.ServerStats()
+    assert L.drwc_server_stats_get(None, C.byref(st)) == 1
+    jid = C.c_int64()
+    assert L.drwc_server_submit(None, None, None, C.byref(jid)) == 1

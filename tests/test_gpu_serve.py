@@ -1,0 +1,116 @@
+"""The multi-job server (drwc_server_*): continuous batching of extraction jobs
+on one device.
+
+Checks: (1) a job served alone gives exactly drwc_frw_run's result (same
+walks, same fixed-order batch sums, same compensated accumulation); (2) jobs
+of different structures and cube resolutions submitted one after another,
+with an arena that holds only two at a time, overlap on the device, wait for
+memory when it is full, and each still gives exactly its stand-alone result;
+(3) with the learned network, each job's result in the mix equals its result
+served alone; (4) requests the server cannot take fail cleanly."""
+import time
+
+import numpy as np
+import pytest
+
+from deeprwcap_b200 import abi, engine, train
+from deeprwcap_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _params(N, seed, walks, batch):
+    return W.job_params_plain(N=N, seed=seed, min_walks=walks, max_walks=walks,
+                              batch_walks=batch)
+
+
+def _same(a, b):
+    assert (a.walks, a.hops, a.lost, a.converged) == (b.walks, b.hops, b.lost, b.converged)
+    np.testing.assert_array_equal(a.cap, b.cap)
+    np.testing.assert_array_equal(a.stderr, b.stderr)
+
+
+def _jobs():
+    return [
+        (W.two_layer_crossing(), _params(16, 11, 40000, 8192)),
+        (W.wire_stack(3, 6, diel_eps=[3.0, 4.0, 2.5, 3.6, 4.4], n_diel_blocks=6, seed=2),
+         _params(21, 12, 30000, 8192)),
+        (W.wire_stack(2, 8, seed=3), _params(23, 13, 20000, 8192)),
+        (W.wire_stack(4, 4, diel_eps=[3.9, 2.7, 4.2], seed=4), _params(16, 14, 35000, 8192)),
+        (W.dense_stack(seed=5), _params(21, 15, 25000, 8192)),
+    ]
+
+
+def test_served_job_equals_frw_run(ctx):
+    s = W.two_layer_crossing()
+    p = _params(16, 7, 3 * 16384 + 1000, 16384)
+    ref = engine.extract(s, p, ctx)
+    with engine.Server(ctx, slots=8192, hbm_budget=64 << 20) as srv:
+        r = srv.wait(srv.submit(s, p), timeout=300)
+        st = srv.stats()
+    _same(r, ref)
+    assert st["completed"] == 1 and st["fdm_hops"] >= r.hops
+
+
+def test_mix_equals_alone_with_admission_by_footprint(ctx):
+    jobs = _jobs()
+    alone = [engine.extract(s, p, ctx) for s, p in jobs]
+    # each job needs its structure + two batches of records (8192 walks x 16 B x 2)
+    budget = 2 * (2 * 8192 * 16 + 64 * 1024)
+    with engine.Server(ctx, slots=16384, max_jobs=8, hbm_budget=budget) as srv:
+        ids = []
+        for s, p in jobs:
+            ids.append(srv.submit(s, p))
+            time.sleep(0.005)
+        res = [srv.wait(i, timeout=600) for i in ids]
+        st = srv.stats()
+        queued = [srv.times(i)[0] for i in ids]
+    for r, a in zip(res, alone):
+        _same(r, a)
+    assert st["completed"] == len(jobs) and st["failed"] == 0
+    assert st["max_running"] == 2           # the arena held two jobs at a time
+    assert st["arena_peak"] <= budget
+    assert max(queued) > 0.0                # later jobs waited for memory
+    assert st["walks_dropped"] >= 0 and st["hops"] >= sum(r.hops for r in res)
+
+
+@pytest.fixture(scope="module")
+def small_net(ctx):
+    X, T, TG = train.build_dataset(ctx, 1 << 16, seed=8, log=lambda *a: None)
+    net = engine.Net(seed=3, ctx=ctx)
+    train.train(net, X, T, TG, epochs=2, batch=512, lr=1e-3, log=lambda *a: None)
+    return net
+
+
+def test_learned_mix_equals_alone(ctx, small_net):
+    jobs = [
+        (W.two_layer_crossing(), _params(16, 21, 20000, 8192)),
+        (W.wire_stack(3, 5, seed=6), _params(16, 22, 15000, 8192)),
+        (W.wire_stack(2, 6, seed=7), _params(21, 23, 10000, 8192)),
+    ]
+    opts = dict(slots=8192, audit_frac=0.05, conf_threshold=-1.0)
+    alone = []
+    for s, p in jobs:
+        with engine.Server(ctx, net=small_net, **opts) as srv:
+            alone.append(srv.wait(srv.submit(s, p), timeout=600))
+    with engine.Server(ctx, net=small_net, **opts) as srv:
+        ids = [srv.submit(s, p) for s, p in jobs]
+        res = [srv.wait(i, timeout=600) for i in ids]
+        st = srv.stats()
+    for r, a in zip(res, alone):
+        _same(r, a)
+    assert st["net_hops"] > 0 and st["audits"] > 0 and st["fdm_hops"] > 0
+    assert st["audit_kl_mean"] > 0.0
+
+
+def test_rejected_requests(ctx):
+    s = W.two_layer_crossing()
+    with engine.Server(ctx, slots=1024, hbm_budget=1 << 20, sizes=(16,)) as srv:
+        with pytest.raises(abi.DrwcError):
+            srv.submit(s, _params(21, 1, 1000, 1000))         # N not served
+        jid = srv.submit(s, _params(16, 1, 1 << 20, 1 << 20))  # records exceed the arena
+        with pytest.raises(abi.DrwcError) as e:
+            srv.wait(jid, timeout=60)
+        assert e.value.status == 3                              # DRWC_ERR_NOMEM
+        ok = srv.wait(srv.submit(s, _params(16, 2, 2000, 1000)), timeout=120)
+        assert ok.walks == 2000
