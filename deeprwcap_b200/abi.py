@@ -104,7 +104,7 @@ class ServerOpts(C.Structure):
                 ("n_sizes", C.c_int32), ("sizes", C.c_int32 * SERVER_MAX_SIZES),
                 ("steps_per_graph", C.c_int32), ("max_materials", C.c_int32),
                 ("max_nets", C.c_int32), ("conf_threshold", C.c_float), ("audit_frac", C.c_float),
-                ("timing", C.c_int32), ("reserved_", C.c_int32)]
+                ("timing", C.c_int32), ("uniform_table", C.c_int32)]
 
 
 class ServerStats(C.Structure):
@@ -114,7 +114,8 @@ class ServerStats(C.Structure):
         "graph_launches", "kernels_launched", "arena_bytes", "arena_used", "arena_peak")] + \
         [(n, C.c_double) for n in ("busy_seconds", "fdm_seconds", "net_seconds", "net_rows",
                                    "audit_kl_mean")] + \
-        [("fdm_iters", C.c_int64), ("fdm_sweeps", C.c_int64), ("fdm_bytes", C.c_double)]
+        [("fdm_iters", C.c_int64), ("fdm_sweeps", C.c_int64), ("fdm_bytes", C.c_double),
+         ("table_hops", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -48,6 +48,7 @@ constexpr int kSvMaxJobs = 64;
 constexpr int kSvNetN = DRWC_NET_N;
 constexpr int kSvDecRows = DRWC_NET_OUT;
 constexpr int kSvMaxSteps = 8;
+constexpr int kSvPrepIters = 64;  // prepare-loop passes per slot and step
 constexpr size_t kSvBsumStride = 3 * (DRWC_MAX_NETS + 2) + 8;  // doubles per (job, parity)
 
 struct SvJob {
@@ -89,7 +90,8 @@ struct SvSlots {
 
 enum SvStat {
     SV_HOPS = 0, SV_NET_HOPS, SV_FDM_HOPS, SV_FALLBACKS, SV_AUDITS, SV_WALKS_DONE,
-    SV_WALKS_DROPPED, SV_NET_ROWS, SV_FDM_ITERS, SV_FDM_SWEEPS, SV_FDM_BYTES, SV_NSTATS
+    SV_WALKS_DROPPED, SV_NET_ROWS, SV_FDM_ITERS, SV_FDM_SWEEPS, SV_FDM_BYTES, SV_TABLE_HOPS,
+    SV_NSTATS
 };
 
 struct SvArgs {
@@ -111,6 +113,11 @@ struct SvArgs {
     unsigned long long* stats;
     double* audit_kl;                   // [0] sum, [1] count
     double* bsum;
+    // homogeneous-cube fast path: per bucket and solver code, the panel values
+    // of the uniform-permittivity Green's function and their running sums
+    int table;
+    const double* tval[DRWC_SERVER_MAX_SIZES][4];
+    const double* tcdf[DRWC_SERVER_MAX_SIZES][4];
 };
 
 // ------------------------------------------------------------------ device
@@ -166,6 +173,80 @@ DRWC_DEV void sv_finish(const SvArgs& A, int slot, int net) {
     A.st.mode[slot] = 0;
 }
 
+// Material id of the cube when every cell centre of its N^3 grid has the same
+// one, else -1 (warp-wide; all lanes get the answer). Uses the cell-centre
+// coordinates the voxeliser computes for i = 0 and i = N-1, the layer rule
+// and the inclusive block bounds of mat_at, so a cube reported homogeneous
+// voxelises to a single material; blocks that merely touch the span of cell
+// centres make it inhomogeneous (conservative).
+DRWC_DEV int sv_homogeneous(const DevGeom& g, const double c[3], double a, int N) {
+    const int lane = threadIdx.x & 31;
+    const double t0 = dsub(ddiv(dadd(dmul(2.0, 0.0), 1.0), (double)N), 1.0);
+    const double t1 = dsub(ddiv(dadd(dmul(2.0, (double)(N - 1)), 1.0), (double)N), 1.0);
+    double lo[3], hi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = dadd(c[d], dmul(a, t0));
+        hi[d] = dadd(c[d], dmul(a, t1));
+    }
+    int m = 0;
+    if (g.n_layers > 0) {
+        int l0 = 0, l1 = 0;
+        for (int l = 0; l < g.n_layers; ++l) {
+            if (lo[2] >= g.zlo[l]) l0 = l;
+            if (hi[2] >= g.zlo[l]) l1 = l;
+        }
+        m = g.lmat[l0];
+        for (int l = l0 + 1; l <= l1; ++l)
+            if (g.lmat[l] != m) return -1;
+    }
+    bool clash = false;
+    for (int b = lane; b < g.n_diel; b += 32) {
+        if (g.dmat[b] == m) continue;
+        const double* D = g.diel + 7 * b;
+        clash |= D[0] <= hi[0] && D[3] >= lo[0] && D[1] <= hi[1] && D[4] >= lo[1] &&
+                 D[2] <= hi[2] && D[5] >= lo[2];
+    }
+    return __any_sync(0xffffffffu, clash) ? -1 : m;
+}
+
+// One hop of a homogeneous cube from the uniform-permittivity tables: the
+// surface values of a single-permittivity cube do not depend on that
+// permittivity, and its centre permittivity is the material's own, so the
+// draw needs no solve. Same Philox draws and weight formula as the FDM hop.
+DRWC_DEV void sv_table_hop(const SvArgs& A, int slot, const SvJob& J, int m) {
+    const int N = J.W.N, M = 6 * N * N;
+    const int h = A.st.hops[slot];
+    const bool first = h == 0;
+    const int code = first ? A.st.code[slot] : DRWC_GFT;
+    const double* cdf = A.tcdf[J.bucket][code];
+    const double* val = A.tval[J.bucket][code];
+    const long long w = A.st.walk[slot];
+    const double2 u2 = first ? philox_uniform2(J.W.seed, (uint64_t)w, 0, 1)
+                             : philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 0);
+    const double tot = cdf[M - 1];
+    const double target = (first ? u2.y : u2.x) * tot;
+    int lo = 0, hi = M - 1;  // first panel whose running sum passes the target
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (cdf[mid] > target) hi = mid;
+        else lo = mid + 1;
+    }
+    const int b = lo;
+    const double a = A.st.a[slot];
+    if (first) {
+        const double v = J.g.pal[m];
+        const double eps_w = ((N % 2) || code == DRWC_GFT) ? v : (v + v + v + v) / 4;
+        A.st.omega[slot] = first_hop_weight(J.G, A.st.sgn[slot], eps_w, tot, val[b], a);
+    }
+    double loc[3];
+    locate_f64(N, b, loc);
+    A.st.px[slot] = dadd(A.st.px[slot], dmul(a, loc[0]));
+    A.st.py[slot] = dadd(A.st.py[slot], dmul(a, loc[1]));
+    A.st.pz[slot] = dadd(A.st.pz[slot], dmul(a, loc[2]));
+    A.st.hops[slot] = h + 1;
+}
+
 __global__ void sv_reset_kernel(SvArgs A) {
     if (threadIdx.x < 2 + DRWC_SERVER_MAX_SIZES) A.cnt[threadIdx.x] = 0;
 }
@@ -176,7 +257,9 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
     const int lane = threadIdx.x & 31;
     if (slot >= A.S) return;
     int act = 0;
-    for (int tries = 0; tries < 4; ++tries) {
+    unsigned long long table_hops = 0;
+    // claims, finished walks and table hops per slot and step are bounded
+    for (int it = 0; it < kSvPrepIters; ++it) {
         int mode = A.st.mode[slot];
         if (mode == 1 && A.jobs[A.st.job[slot]].state != 1) {
             // the job has finished (or was cancelled): drop its walk
@@ -209,8 +292,21 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
             else { A.st.a[slot] = d; act = 1; }
         }
         act = __shfl_sync(0xffffffffu, act, 0);
+        if (act && A.table) {
+            __syncwarp();
+            const int m = sv_homogeneous(J.g, r, A.st.a[slot], J.W.N);
+            if (m >= 0) {
+                if (lane == 0) sv_table_hop(A, slot, J, m);
+                table_hops += 1;
+                act = 0;
+            }
+        }
         __syncwarp();
         if (act) break;
+    }
+    if (lane == 0 && table_hops) {
+        atomicAdd(A.stats + SV_TABLE_HOPS, table_hops);
+        atomicAdd(A.stats + SV_HOPS, table_hops);
     }
     if (lane == 0 && act) {
         const SvJob& J = A.jobs[A.st.job[slot]];
@@ -645,6 +741,44 @@ static int sv_fdm_launch(drwc_server* v, int b, cudaStream_t s) {
     });
 }
 
+// Tables of the homogeneous-cube fast path: panel values of the uniform
+// solutions (the warm-start tables, permittivity 1) in ggft panel order and
+// their running sums (|value| for the gradient codes, max(value, 0) for the
+// Green's function, the weights the FDM hop draws with).
+static int sv_tables(drwc_server* v) {
+    drwc_ctx* ctx = v->ctx;
+    for (int b = 0; b < v->o.n_sizes; ++b) {
+        const int N = v->o.sizes[b], NN = N * N, M = 6 * NN;
+        const double* w[4];
+        int rc = warm_tables(ctx, N, w);
+        if (rc) return rc;
+        std::vector<double> x((size_t)N * NN), hv(2 * (size_t)M);
+        for (int code = 0; code < 4; ++code) {
+            DRWC_CUDA_TRY(cudaMemcpy(x.data(), w[code], x.size() * 8, cudaMemcpyDeviceToHost));
+            double run = 0.0;
+            for (int q = 0; q < M; ++q) {
+                const int f = q / NN, tt = q % NN, a = tt % N, bb = tt / N;
+                int c;
+                switch (f) {
+                    case 0: c = a + bb * N; break;
+                    case 1: c = a + bb * N + (N - 1) * NN; break;
+                    case 2: c = a + bb * NN; break;
+                    case 3: c = a + (N - 1) * N + bb * NN; break;
+                    case 4: c = a * N + bb * NN; break;
+                    default: c = (N - 1) + a * N + bb * NN; break;
+                }
+                const double val = x[c];
+                run += code == DRWC_GFT ? std::max(val, 0.0) : std::fabs(val);
+                hv[q] = val;
+                hv[M + q] = run;
+            }
+            DRWC_CUDA_TRY(cudaMemcpy(const_cast<double*>(v->A.tval[b][code]), hv.data(),
+                                     2 * (size_t)M * 8, cudaMemcpyHostToDevice));
+        }
+    }
+    return DRWC_OK;
+}
+
 // Event nodes when captured (plain records otherwise): stage timing.
 static int sv_mark(drwc_server* v, cudaEvent_t e, cudaStream_t s) {
     if (!v->timing) return DRWC_OK;
@@ -1011,6 +1145,7 @@ static void sv_thread(drwc_server* v) {
         v->st.fdm_iters = (int64_t)h[SV_FDM_ITERS];
         v->st.fdm_sweeps = (int64_t)h[SV_FDM_SWEEPS];
         v->st.fdm_bytes = (double)h[SV_FDM_BYTES];
+        v->st.table_hops = (int64_t)h[SV_TABLE_HOPS];
         v->st.audit_kl_mean = v->h_akl[1] > 0 ? v->h_akl[0] / v->h_akl[1] : 0.0;
     }
     // stopped (destroy or an error): every job not done ends as failed
@@ -1044,11 +1179,12 @@ static int sv_alloc(drwc_server* v) {
         o_O = take(4 * (size_t)S * kSvDecRows);
         o_G = take(4 * (size_t)S * DRWC_NET_PANELS);
     }
-    size_t o_sy[DRWC_SERVER_MAX_SIZES], o_ss[DRWC_SERVER_MAX_SIZES];
+    size_t o_sy[DRWC_SERVER_MAX_SIZES], o_ss[DRWC_SERVER_MAX_SIZES], o_tab[DRWC_SERVER_MAX_SIZES];
     for (int b = 0; b < v->o.n_sizes; ++b) {
         const size_t nnn = (size_t)v->o.sizes[b] * v->o.sizes[b] * v->o.sizes[b];
         o_sy[b] = take(8 * (size_t)v->fdm_grid[b] * nnn);
         o_ss[b] = take(4 * (size_t)v->fdm_grid[b] * nnn);
+        o_tab[b] = take(8 * 4 * 2 * 6 * (size_t)v->o.sizes[b] * v->o.sizes[b]);
     }
     if (cudaMalloc(&v->dblock, off) != cudaSuccess) { cudaGetLastError(); return DRWC_ERR_NOMEM; }
     DRWC_CUDA_TRY(cudaMemset(v->dblock, 0, off));
@@ -1095,9 +1231,16 @@ static int sv_alloc(drwc_server* v) {
         A.O = (float*)(B + o_O);
         A.Gh = (float*)(B + o_G);
     }
+    A.table = v->o.uniform_table;
     for (int b = 0; b < v->o.n_sizes; ++b) {
         v->fdm_sy[b] = (double*)(B + o_sy[b]);
         v->fdm_ss[b] = (float*)(B + o_ss[b]);
+        const size_t M = 6 * (size_t)v->o.sizes[b] * v->o.sizes[b];
+        for (int code = 0; code < 4; ++code) {
+            double* t = (double*)(B + o_tab[b]) + (size_t)code * 2 * M;
+            A.tval[b][code] = t;
+            A.tcdf[b][code] = t + M;
+        }
     }
     // pinned mirrors
     size_t hoff = 0;
@@ -1154,6 +1297,7 @@ DRWC_API void drwc_server_opts_default(drwc_server_opts* o) {
     o->conf_threshold = -1.5f;
     o->audit_frac = 0.01f;
     o->timing = 0;
+    o->uniform_table = 0;
 }
 
 DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drwc_net* net,
@@ -1167,7 +1311,7 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drw
         o.hbm_budget < 4096 || o.n_sizes < 1 || o.n_sizes > DRWC_SERVER_MAX_SIZES ||
         o.steps_per_graph < 1 || o.steps_per_graph > kSvMaxSteps || o.max_materials < 1 ||
         o.max_materials > kMaxMaterials || o.max_nets < 1 || o.max_nets > DRWC_MAX_NETS ||
-        !(o.audit_frac >= 0.f && o.audit_frac <= 1.f))
+        !(o.audit_frac >= 0.f && o.audit_frac <= 1.f) || o.uniform_table < 0 || o.uniform_table > 1)
         return DRWC_ERR_INVALID;
     if (net && net_context(net) != ctx) return DRWC_ERR_INVALID;
     std::unique_ptr<drwc_server> v(new drwc_server());
@@ -1195,6 +1339,7 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drw
             if (!rc) rc = warm_tables(ctx, o.sizes[b], w);
         }
         if (!rc) rc = sv_alloc(v.get());
+        if (!rc) rc = sv_tables(v.get());
         if (!rc && net) rc = net_reserve_rows(net, o.slots);
         for (int b = 0; !rc && b < o.n_sizes; ++b) {
             if (cudaStreamCreateWithFlags(&v->side[b], cudaStreamNonBlocking) != cudaSuccess ||

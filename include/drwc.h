@@ -362,7 +362,10 @@ typedef struct drwc_server_opts {
     float conf_threshold;     /* network hops: route to FDM above this predicted log10 KL */
     float audit_frac;         /* network hops: fraction also solved by FDM */
     int32_t timing;           /* 1: time the FDM and network stages with graph event nodes */
-    int32_t reserved_;
+    int32_t uniform_table;    /* 1: a hop whose cube voxelises to one permittivity draws from
+                                 the precomputed uniform-permittivity Green's function (exact
+                                 for such cubes: their surface values do not depend on the
+                                 permittivity) instead of the network or the FDM solve */
 } drwc_server_opts;
 DRWC_API void drwc_server_opts_default(drwc_server_opts* o);
 /* net (nullable): with a network, hops of N = 16 jobs go through it
@@ -405,6 +408,7 @@ typedef struct drwc_server_stats {
     double audit_kl_mean;             /* mean KL(FDM || network) over audited hops */
     int64_t fdm_iters, fdm_sweeps;    /* FP32 CG iterations and FP64 sweeps of the FDM hops */
     double fdm_bytes;                 /* streamed-PCG algorithmic bytes of the FDM hops */
+    int64_t table_hops;               /* hops drawn from the uniform-permittivity tables */
 } drwc_server_stats;
 /* Returns the request thread's error code, if it stopped on one. */
 DRWC_API int drwc_server_stats_get(drwc_server* srv, drwc_server_stats* out);

@@ -114,3 +114,21 @@ def test_rejected_requests(ctx):
         assert e.value.status == 3                              # DRWC_ERR_NOMEM
         ok = srv.wait(srv.submit(s, _params(16, 2, 2000, 1000)), timeout=120)
         assert ok.walks == 2000
+
+
+def test_uniform_table_hops_follow_the_fdm_walk(ctx):
+    """Cubes of a single permittivity take their hop from the precomputed
+    uniform-permittivity Green's function. Their surface values equal the FDM
+    solution (it does not depend on the permittivity), and the hop uses the
+    same Philox draws, so the walks follow the FDM walks: the capacitance row
+    agrees far inside the statistical error."""
+    s = W.two_layer_crossing()
+    p = _params(16, 17, 1 << 16, 1 << 14)
+    ref = engine.extract(s, p, ctx)
+    with engine.Server(ctx, slots=8192, uniform_table=1) as srv:
+        r = srv.wait(srv.submit(s, p), timeout=300)
+        st = srv.stats()
+    assert st["table_hops"] > 0.2 * r.hops, st
+    assert st["fdm_hops"] + st["table_hops"] == st["hops"]
+    assert r.walks == ref.walks and abs(r.hops - ref.hops) <= 1e-4 * ref.hops
+    np.testing.assert_allclose(r.cap, ref.cap, rtol=1e-6, atol=1e-9 * abs(ref.cap[0]))
