@@ -202,6 +202,23 @@ def learned_section(ctx, args):
     t_fdm = time.perf_counter() - t1
     cap = lambda e, w: [float(w[e == j].sum() / len(w)) for j in range(s.n_nets + 1)]
     c1, c0 = cap(e1, w1), cap(e0, w0)
+    # the same job through the server: network + uniform-permittivity table
+    served = {}
+    for name, kw in (("served_learned", {}), ("served_learned_table", {"uniform_table": 1})):
+        pj = W.job_params_plain(N=16, seed=4242, tol=FDM_TOL, min_walks=nw, max_walks=nw,
+                                batch_walks=1 << 16)
+        with engine.Server(ctx, net=net, **kw) as srv:
+            t2 = time.perf_counter()
+            r = srv.wait(srv.submit(s, pj), timeout=3600)
+            dt = time.perf_counter() - t2
+            sst = srv.stats()
+        served[name] = {"seconds": dt, "hops": int(r.hops), "hops_per_s": r.hops / dt,
+                        "net_hops": sst["net_hops"], "fdm_hops": sst["fdm_hops"],
+                        "table_hops": sst["table_hops"], "fallbacks": sst["fallbacks"],
+                        "audits": sst["audits"], "audit_kl_mean": sst["audit_kl_mean"],
+                        "cap_fF": [float(x) for x in r.cap],
+                        "self_rel_diff_vs_fdm": abs(r.cap[0] - c0[0]) / abs(c0[0]),
+                        "self_rel_stderr": float(r.stderr[0] / abs(r.cap[0]))}
     # the network alone on a fixed batch (tensor-core fraction)
     B = 65536
     dev = torch.device("cuda", ctx.device)
@@ -221,10 +238,12 @@ def learned_section(ctx, args):
     flop = B * 2.0 * (512 * 16 * 27 + 64 * 32 * 432 + 8 * 64 * 864 + 512 * engine.NET_OUT)
     _, bf16, src = peaks()
     hl, hf = h1.sum() / st["seconds"], h0.sum() / t_fdm
-    return {"structure": "dense_stack (24 conductors, 5 layers, 10 blocks)", "walks": nw,
+    return net, {"structure": "dense_stack (24 conductors, 5 layers, 10 blocks)", "walks": nw,
             "train": {"samples": int(X.shape[0]), "epochs": args.train_epochs,
                       "seconds": t_train, "train_step_seconds": tsec, **ev},
             "learned_hops_per_s": hl, "fdm_hops_per_s": hf, "gain": hl / hf,
+            **served,
+            "gain_served_learned_table": served["served_learned_table"]["hops_per_s"] / hf,
             "net_hops": st["net_hops"], "fdm_hops": st["fdm_hops"],
             "fallbacks": st["fallbacks"], "audits": st["audits"],
             "audit_kl_mean": st["audit_kl"], "learned_launches": int(l_launch),
@@ -233,6 +252,83 @@ def learned_section(ctx, args):
             "nn_forward": {"cubes": B, "seconds": t_nn, "tflops": flop / t_nn / 1e12,
                            "peak_tflops": bf16, "frac": flop / t_nn / 1e12 / bf16,
                            "peak_source": src}}
+
+
+def serving_section(ctx, args, net):
+    """Config-4 stream (Poisson arrivals at 50 jobs/s; 2-4 layers x 4-16
+    wires; N in {16, 21, 23}; walks log-uniform in [1e5, --serve-walks-max])
+    through three arms on the same seeded jobs: drwc_frw_run one job at a
+    time in arrival order (the FDM-per-hop engine without serving), the
+    server with an FDM solve on every hop, and the server with the learned
+    network (N = 16 jobs) and the uniform-permittivity table for cubes of a
+    single permittivity. Latency = submission to result."""
+    from deeprwcap_b200 import engine
+    from deeprwcap_b200 import workloads as W
+    stream = W.serving_stream(n_jobs=args.serve_jobs, rate=50.0, seed=1,
+                              walks=(1e5, args.serve_walks_max))
+    hbm, _, _ = peaks()
+
+    def summary(lat, hops, wall, st=None):
+        lat = np.asarray(lat)
+        out = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+               "makespan_s": wall, "hops": int(hops), "hops_per_s": hops / wall}
+        if st is not None:
+            out.update({"busy_s": st["busy_seconds"], "hops_per_s_busy": st["hops"] / st["busy_seconds"],
+                        "fdm_hops": st["fdm_hops"], "net_hops": st["net_hops"],
+                        "table_hops": st["table_hops"], "fallbacks": st["fallbacks"],
+                        "audits": st["audits"], "audit_kl_mean": st["audit_kl_mean"],
+                        "graph_launches": st["graph_launches"],
+                        "kernels_launched": st["kernels_launched"],
+                        "max_running": st["max_running"], "arena_peak_bytes": st["arena_peak"],
+                        "fdm_alg_GBps_over_busy": st["fdm_bytes"] / st["busy_seconds"] / 1e9})
+        return out
+
+    # (1) one job at a time through drwc_frw_run, started when it arrives
+    t0 = time.perf_counter()
+    lat, hops = [], 0
+    for j in stream:
+        dt = t0 + j.arrival - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        r = engine.extract(j.structure, W.serve_params(j), ctx)
+        lat.append(time.perf_counter() - (t0 + j.arrival))
+        hops += r.hops
+    seq = summary(lat, hops, time.perf_counter() - t0)
+
+    def served(**opts):
+        with engine.Server(ctx, **opts) as srv:
+            t0 = time.perf_counter()
+            ids = []
+            for j in stream:
+                dt = t0 + j.arrival - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                ids.append(srv.submit(j.structure, W.serve_params(j)))
+            res = [srv.wait(i, timeout=3600) for i in ids]
+            wall = time.perf_counter() - t0
+            lat = [srv.times(i)[1] for i in ids]
+            st = srv.stats()
+        return summary(lat, sum(r.hops for r in res), wall, st), res
+
+    plain, res_p = served()
+    plain["fdm_roofline_frac_of_measured_hbm"] = plain["fdm_alg_GBps_over_busy"] / hbm
+    out = {"jobs": len(stream), "rate_jobs_per_s": 50.0,
+           "walks_range": [1e5, args.serve_walks_max],
+           "N_mix": {str(n): sum(1 for j in stream if j.N == n) for n in (16, 21, 23)},
+           "total_walks": int(sum(j.walks for j in stream)),
+           "sequential_frw_run": seq, "served_fdm": plain}
+    if net is not None:
+        learned, res_l = served(net=net, uniform_table=1)
+        # capacitance agreement of the learned+served form with the FDM walk, per job
+        self_diff = [abs(a.cap[0] - b.cap[0]) / abs(b.cap[0]) for a, b in zip(res_l, res_p)]
+        learned["self_cap_rel_diff_vs_fdm"] = {"max": float(max(self_diff)),
+                                               "mean": float(np.mean(self_diff))}
+        learned["self_cap_rel_stderr_fdm_mean"] = float(np.mean(
+            [b.stderr[0] / abs(b.cap[0]) for b in res_p]))
+        out["served_learned_table"] = learned
+        out["speedup_hops_per_s_vs_sequential_fdm"] = learned["hops_per_s"] / seq["hops_per_s"]
+        out["speedup_p50_vs_sequential_fdm"] = seq["p50_s"] / learned["p50_s"]
+    return out
 
 
 def run_b200(args, world, rank, local):
@@ -338,8 +434,14 @@ def run_b200(args, world, rank, local):
     # ---- learned transition kernels (network trained here on engine-generated
     #      FDM data) vs the FDM walk on the dense 24-conductor structure
     learned = None
+    net = None
     if rank == 0 and not args.no_learned:
-        learned = learned_section(ctx, args)
+        net, learned = learned_section(ctx, args)
+
+    # ---- serving: a Poisson stream of extraction jobs through the server
+    serving = None
+    if rank == 0 and not args.no_serve:
+        serving = serving_section(ctx, args, net)
 
     # ---- roofline of the dominant kernel (the per-hop FDM solve inside the walk kernel)
     hbm, bf16, src = peaks()
@@ -382,6 +484,7 @@ def run_b200(args, world, rank, local):
             "wall_s_timed": t_wall,
             "job": job_info,
             "learned": learned,
+            "serving": serving,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
@@ -514,6 +617,9 @@ def main():
     ap.add_argument("--train-epochs", type=int, default=4)
     ap.add_argument("--learned-walks", type=int, default=1 << 20)
     ap.add_argument("--cubes", type=int, default=8192)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-jobs", type=int, default=10)
+    ap.add_argument("--serve-walks-max", type=float, default=1e6)
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.workload == "fdm_batch":

@@ -287,20 +287,110 @@ DRWC_DEV void unrotate(int rot, const double v[3], double out[3]) {
 
 DRWC_DEV int rot_of_code(int code) { return code == DRWC_WVTX ? 1 : code == DRWC_WVTY ? 2 : 0; }
 
+// Separable voxelisation. The cell-centre coordinates c + a*t_i are monotone
+// in i on every axis (explicitly rounded FP64, as the CPU walk computes
+// them), so a dielectric block's inclusive bounds select a contiguous index
+// range per axis, and the layer rule gives one layer per z index. Per cube:
+// the 3N coordinates, the layer material of each z index and the index
+// ranges of the blocks that reach the cube (in block order: the first
+// containing block wins, as in mat_at); per voxel a few integer tests. The
+// result is mat_at's at every cell centre.
+constexpr int kVoxMaxBlocks = 32;  // blocks reaching one cube; beyond: mat_at per voxel
+
+template <int N>
+struct VoxScratch {
+    double crd[3][N];
+    int lm[N];
+    int rel[kVoxMaxBlocks][7];  // i0, i1, j0, j1, k0, k1 (original axes), material
+    int nrel;
+};
+
+template <int N>
+DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const double* tco,
+                          VoxScratch<N>& vs) {
+    const int t = threadIdx.x;
+    if (t < 3 * N) vs.crd[t / N][t % N] = dadd(c[t / N], dmul(a, tco[t % N]));
+    if (t == 0) vs.nrel = 0;
+    __syncthreads();
+    if (t < N) {
+        int li = 0;
+        for (int l = 0; l < g.n_layers; ++l) {
+            if (vs.crd[2][t] >= g.zlo[l]) li = l;
+            else break;
+        }
+        vs.lm[t] = g.n_layers > 0 ? g.lmat[li] : 0;
+    }
+    if (t < 32) {  // warp 0 keeps the blocks that reach the cube, in block order
+        for (int b0 = 0; b0 < g.n_diel; b0 += 32) {
+            const int b = b0 + t;
+            int r[6] = {0, -1, 0, -1, 0, -1};
+            bool hit = false;
+            if (b < g.n_diel) {
+                const double* D = g.diel + 7 * b;
+                hit = true;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    int i0 = N, i1 = -1;
+                    for (int i = 0; i < N; ++i) {
+                        const double x = vs.crd[d][i];
+                        if (x >= D[d] && x <= D[3 + d]) { i0 = min(i0, i); i1 = i; }
+                    }
+                    r[2 * d] = i0;
+                    r[2 * d + 1] = i1;
+                    hit &= i0 <= i1;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            const int base = vs.nrel;
+            if (hit) {
+                const int q = base + __popc(m & ((1u << t) - 1));
+                if (q < kVoxMaxBlocks) {
+#pragma unroll
+                    for (int e = 0; e < 6; ++e) vs.rel[q][e] = r[e];
+                    vs.rel[q][6] = g.dmat[b];
+                }
+            }
+            __syncwarp();
+            if (t == 0) vs.nrel = base + __popc(m);
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+}
+
+// Material of voxel (i, j, k) of the (possibly rotated) cube.
+template <int N>
+DRWC_DEV int vox_material(const DevGeom& g, const VoxScratch<N>& vs, const double c[3], double a,
+                          const double* tco, int i, int j, int k, int rot) {
+    int ox, oy, oz;
+    if (rot == 1) { ox = k; oy = i; oz = j; }
+    else if (rot == 2) { ox = j; oy = k; oz = i; }
+    else { ox = i; oy = j; oz = k; }
+    if (vs.nrel > kVoxMaxBlocks) {  // too many blocks reach this cube: test them all
+        double p[3];
+        rotated_point(c, a, tco, i, j, k, rot, p);
+        return mat_at(g, p);
+    }
+    for (int q = 0; q < vs.nrel; ++q) {
+        const int* r = vs.rel[q];
+        if (ox >= r[0] && ox <= r[1] && oy >= r[2] && oy <= r[3] && oz >= r[4] && oz <= r[5])
+            return r[6];
+    }
+    return vs.lm[oz];
+}
+
 // CTA-wide: voxelise one cube (rotated frame) into BF16 eps / max eps and,
-// optionally, FP64 eps; returns the centre permittivity of the gradient
-// convention (thread 0's value valid).
+// optionally, FP64 eps. vs: shared scratch (separable voxelisation).
 template <int N>
 DRWC_DEV void voxelise_net(const DevGeom& g, const double c[3], double a, int rot,
                            const double* tco, const double* palsm, uint8_t* matsm,
-                           __nv_bfloat16* X, double* eps64, float* red) {
+                           __nv_bfloat16* X, double* eps64, float* red, VoxScratch<N>& vs) {
     constexpr int NNN = N * N * N;
+    vox_prepare<N>(g, c, a, tco, vs);
     float mx = 0.f;
     for (int v = threadIdx.x; v < NNN; v += blockDim.x) {
         const int i = v % N, j = (v / N) % N, k = v / (N * N);
-        double p[3];
-        rotated_point(c, a, tco, i, j, k, rot, p);
-        const int m = mat_at(g, p);
+        const int m = vox_material<N>(g, vs, c, a, tco, i, j, k, rot);
         matsm[v] = (uint8_t)m;
         mx = fmaxf(mx, (float)palsm[m]);
     }

@@ -520,11 +520,14 @@ int net_forward_dyn(drwc_net* n, int Bmax, const unsigned* nrows, const bf16* X,
     if (Bmax > n->cap) return DRWC_ERR_INVALID;  // reserve first (not during capture)
     drwc_ctx* ctx = n->ctx;
     const bf16* pb = n->pb;
-    int rc = launch_umma_dyn<16>(ctx, Bmax * 512, nrows, 512, 16, 27,
+    int rc = DRWC_OK;
+    if (X) {  // else conv1's activations are already in a1 (net_conv1_operands)
+        rc = launch_umma_dyn<16>(ctx, Bmax * 512, nrows, 512, 16, 27,
                                  ConvGather<16, 1>{X, Bmax * 512},
                                  RowsBf16{pb + n->L.w1, 16, 27, 27, nullptr},
                                  EpiReluBf16{n->a1, n->p + n->L.b1, 16}, n->err);
-    if (rc) return rc;
+        if (rc) return rc;
+    }
     rc = launch_umma_dyn<32>(ctx, Bmax * 64, nrows, 64, 32, 27 * 16, ConvGather<8, 16>{n->a1, Bmax * 64},
                              RowsBf16{pb + n->L.w2, 32, 27 * 16, 27 * 16, nullptr},
                              EpiReluBf16{n->a2, n->p + n->L.b2, 32}, n->err);
@@ -545,6 +548,10 @@ int net_forward_dyn(drwc_net* n, int Bmax, const unsigned* nrows, const bf16* X,
 }
 
 int net_reserve_rows(drwc_net* n, int B) { return net_reserve(n, B); }
+
+NetConv1 net_conv1_operands(drwc_net* n) {
+    return NetConv1{n->pb + n->L.w1, n->p + n->L.b1, n->a1};
+}
 
 void net_hold(drwc_net* n, int delta) { n->holders += delta; }
 

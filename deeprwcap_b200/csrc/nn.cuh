@@ -6,6 +6,8 @@
 
 #include "host.cuh"
 
+#define DRWC_DEV_INLINE __device__ __forceinline__
+
 struct drwc_net;
 
 namespace drwc {
@@ -24,7 +26,8 @@ int net_forward_mapped(drwc_net* n, int B, const __nv_bfloat16* X, float* O, flo
 // Same on row counts read on the device (*nrows rows of X, *nrows_g rows
 // of the gradient head), for CUDA-graph replay: every launch covers Bmax
 // rows and tiles past the count exit at once. Call net_reserve_rows(Bmax)
-// beforehand (it allocates).
+// beforehand (it allocates). X = nullptr starts at conv2: the caller has
+// written conv1's activations (see conv1_cube below) into the net's a1.
 int net_forward_dyn(drwc_net* n, int Bmax, const unsigned* nrows, const __nv_bfloat16* X,
                     float* O, float* G, const int* gmap, const unsigned* nrows_g);
 int net_reserve_rows(drwc_net* n, int B);
@@ -32,5 +35,48 @@ int net_reserve_rows(drwc_net* n, int B);
 // ones fail with DRWC_ERR_INVALID until every holder lets go.
 void net_hold(drwc_net* n, int delta);
 drwc_ctx* net_context(drwc_net* n);
+
+// conv1 operands: BF16 weights [16][27] (tap = dz*9 + dy*3 + dx), FP32 bias,
+// and the activation buffer a1 [rows * 512][16] (channels last).
+struct NetConv1 {
+    const __nv_bfloat16* w1;
+    const float* b1;
+    __nv_bfloat16* a1;
+};
+NetConv1 net_conv1_operands(drwc_net* n);
+
+// conv1 of one 16^3 cube on the CUDA cores, CTA-wide: x (shared, BF16 eps /
+// max eps), w (shared, FP32 copies of the BF16 weights), b (shared, bias) ->
+// a1 rows [512][16] BF16 = ReLU(b + sum over taps of w * x), zero padding,
+// stride 2. The operands are the BF16 values the tensor-core layer reads and
+// every product is exact in FP32; only the FP32 summation order differs.
+// With one input channel its GEMM has K = 27, too thin for the tensor cores,
+// while 221K FMAs per cube run next to the voxelisation that produced x.
+DRWC_DEV_INLINE void conv1_cube(const __nv_bfloat16* x, const float* w, const float* b,
+                                __nv_bfloat16* __restrict__ a1) {
+    constexpr int D = 16, Do = 8, P = Do * Do * Do;
+    for (int p = threadIdx.x; p < P; p += blockDim.x) {
+        const int pz = p / (Do * Do), py = (p / Do) % Do, px = p % Do;
+        float xv[27];
+#pragma unroll
+        for (int tap = 0; tap < 27; ++tap) {
+            const int z = 2 * pz - 1 + tap / 9, y = 2 * py - 1 + (tap / 3) % 3,
+                      xx = 2 * px - 1 + tap % 3;
+            const bool in = z >= 0 && z < D && y >= 0 && y < D && xx >= 0 && xx < D;
+            xv[tap] = in ? __bfloat162float(x[(z * D + y) * D + xx]) : 0.f;
+        }
+        __align__(16) __nv_bfloat16 out[16];
+#pragma unroll
+        for (int co = 0; co < 16; ++co) {
+            float acc = 0.f;
+#pragma unroll
+            for (int tap = 0; tap < 27; ++tap) acc = fmaf(w[co * 27 + tap], xv[tap], acc);
+            out[co] = __float2bfloat16(fmaxf(acc + b[co], 0.f));
+        }
+        uint4* dst = reinterpret_cast<uint4*>(a1 + (size_t)p * 16);
+        dst[0] = reinterpret_cast<const uint4*>(out)[0];
+        dst[1] = reinterpret_cast<const uint4*>(out)[1];
+    }
+}
 
 }  // namespace drwc

@@ -7,7 +7,7 @@
 //     parameters, claim limit and the two batches of walk ids whose records
 //     it is collecting;
 //   * per-job counters (device-written): next walk id, finished walks per
-//     batch parity, walks in flight, reduced flags;
+//     batch of the claim window, walks in flight, reduced flags;
 //   * a pool of S walker slots (position, weight, hop count, job, walk id);
 //   * per-step work lists: network rows (N = 16 jobs when a network is
 //     loaded) and FDM rows bucketed by cube resolution.
@@ -49,7 +49,8 @@ constexpr int kSvNetN = DRWC_NET_N;
 constexpr int kSvDecRows = DRWC_NET_OUT;
 constexpr int kSvMaxSteps = 8;
 constexpr int kSvPrepIters = 64;  // prepare-loop passes per slot and step
-constexpr size_t kSvBsumStride = 3 * (DRWC_MAX_NETS + 2) + 8;  // doubles per (job, parity)
+constexpr int kSvWin = 4;         // batches of walk ids a job may have in flight
+constexpr size_t kSvBsumStride = 3 * (DRWC_MAX_NETS + 2) + 8;  // doubles per (job, window slot)
 
 struct SvJob {
     DevGeom g;
@@ -62,19 +63,19 @@ struct SvJob {
     long long total;   // walk ids [0, total)
     long long batch;   // walks per batch
     long long limit;   // ids below this may be claimed
-    long long bfirst[2];
-    long long bcount[2];
-    double* rec_w;     // 2 x batch records, parity p at p * batch
+    long long bfirst[kSvWin];  // first walk id of the batch in window slot q (batch k: q = k % kSvWin)
+    long long bcount[kSvWin];
+    double* rec_w;     // kSvWin x batch records, window slot q at q * batch
     int32_t* rec_end;
     int32_t* rec_hops;
 };
 
 struct SvCtr {
     unsigned long long next;
-    unsigned long long done[2];
+    unsigned long long done[kSvWin];
     unsigned long long inflight;  // two's complement
-    unsigned long long reduced[2];
-    unsigned long long pad[2];
+    unsigned long long reduced[kSvWin];
+    unsigned long long pad[7];
 };
 
 struct SvHdr {
@@ -103,11 +104,13 @@ struct SvArgs {
     SvSlots st;
     int* blist[DRWC_SERVER_MAX_SIZES];
     int* bkind[DRWC_SERVER_MAX_SIZES];  // bit 0 audit, bits 1.. network row
-    unsigned* cnt;                      // [0] network rows, [1] first-hop rows, [2 + b] bucket b
+    unsigned* cnt;                      // [0] network rows, [1] first-hop rows, [2 + b] rows of
+                                        // bucket b, [2 + MAX_SIZES + b] its next unclaimed row
     float conf_thresh, audit_frac;
     __nv_bfloat16* X;
     float* O;
     float* Gh;
+    NetConv1 c1;                        // conv1 runs inside the voxeliser
     int* alist;
     int* frow;
     unsigned long long* stats;
@@ -116,6 +119,7 @@ struct SvArgs {
     // homogeneous-cube fast path: per bucket and solver code, the panel values
     // of the uniform-permittivity Green's function and their running sums
     int table;
+    int fair;                           // claim policy (drwc_server_opts.fair_share)
     const double* tval[DRWC_SERVER_MAX_SIZES][4];
     const double* tcdf[DRWC_SERVER_MAX_SIZES][4];
 };
@@ -123,8 +127,11 @@ struct SvArgs {
 // ------------------------------------------------------------------ device
 DRWC_DEV long long sv_claim(const SvArgs& A, int slot, int* job_out) {
     const int n = A.hdr->n_act;
+    // act[] lists the running jobs oldest first: FIFO with backfill, or a
+    // rotation per slot for an even share
+    const int first = A.fair ? slot % max(n, 1) : 0;
     for (int q = 0; q < n; ++q) {
-        const int j = A.hdr->act[(slot + q) % n];
+        const int j = A.hdr->act[(first + q) % n];
         const SvJob& J = A.jobs[j];
         if (J.state != 1) continue;
         // keep the counter from running far past the limit; the host clamps it
@@ -159,7 +166,7 @@ DRWC_DEV void sv_finish(const SvArgs& A, int slot, int net) {
     const int j = A.st.job[slot];
     const SvJob& J = A.jobs[j];
     const long long w = A.st.walk[slot];
-    const int p = (int)((w / J.batch) & 1);
+    const int p = (int)((w / J.batch) % kSvWin);
     const long long i = w - J.bfirst[p];
     if (i >= 0 && i < J.bcount[p]) {  // always, as claims stop at the window's end
         const long long r = (long long)p * J.batch + i;
@@ -248,7 +255,7 @@ DRWC_DEV void sv_table_hop(const SvArgs& A, int slot, const SvJob& J, int m) {
 }
 
 __global__ void sv_reset_kernel(SvArgs A) {
-    if (threadIdx.x < 2 + DRWC_SERVER_MAX_SIZES) A.cnt[threadIdx.x] = 0;
+    if (threadIdx.x < 2 + 2 * DRWC_SERVER_MAX_SIZES) A.cnt[threadIdx.x] = 0;
 }
 
 // One warp per slot.
@@ -327,14 +334,21 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
     }
 }
 
-// One CTA (256 threads) per network row: the cube as network input.
+// One CTA (256 threads) per network row: the cube voxelised in shared
+// memory (eps / max eps, BF16) and the network's first layer applied to it,
+// so only conv1's activations reach global memory.
 __global__ void __launch_bounds__(256) sv_voxelise_kernel(SvArgs A) {
     constexpr int N = kSvNetN;
     __shared__ double tco[N];
     __shared__ double pal[kMaxMaterials];
     __shared__ uint8_t mat[N * N * N];
+    __shared__ __align__(16) __nv_bfloat16 xs[N * N * N];
+    __shared__ float w1[16 * 27], b1[16];
+    __shared__ VoxScratch<N> vs;
     __shared__ float red[32];
     centre_offsets<N>(tco);
+    for (int q = threadIdx.x; q < 16 * 27; q += blockDim.x) w1[q] = __bfloat162float(A.c1.w1[q]);
+    if (threadIdx.x < 16) b1[threadIdx.x] = A.c1.b1[threadIdx.x];
     const int na = (int)A.cnt[0];
     int loaded = -1;
     for (int row = blockIdx.x; row < na; row += gridDim.x) {
@@ -350,12 +364,12 @@ __global__ void __launch_bounds__(256) sv_voxelise_kernel(SvArgs A) {
         const bool first = A.st.hops[slot] == 0;
         const int rot = first ? rot_of_code(A.st.code[slot]) : 0;
         const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
-        voxelise_net<N>(J.g, c, A.st.a[slot], rot, tco, pal, mat, A.X + (size_t)row * N * N * N,
-                        nullptr, red);
+        voxelise_net<N>(J.g, c, A.st.a[slot], rot, tco, pal, mat, xs, nullptr, red, vs);
         if (first && threadIdx.x == 0) {
             const EpsPalette E{mat, pal, nullptr, nullptr, nullptr, 0};
             A.st.epsw[slot] = center_diel<N>(E, DRWC_WVTZ);
         }
+        conv1_cube(xs, w1, b1, A.c1.a1 + (size_t)row * 512 * 16);
         __syncthreads();
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.stats + SV_NET_ROWS, (unsigned long long)na);
@@ -468,9 +482,16 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
     double* ys = scratch_y + (size_t)blockIdx.x * D::NNN;
     float* ss = scratch_s + (size_t)blockIdx.x * D::NNN;
     const unsigned count = A.cnt[2 + bucket];
+    unsigned* next_item = A.cnt + 2 + DRWC_SERVER_MAX_SIZES + bucket;
+    __shared__ unsigned s_idx;
     int loaded = -1, P = 0;
     unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0;
-    for (unsigned idx = blockIdx.x; idx < count; idx += gridDim.x) {
+    for (;;) {
+        // rows are claimed one at a time: solve costs differ by cube
+        if (threadIdx.x == 0) s_idx = atomicAdd(next_item, 1u);
+        __syncthreads();
+        const unsigned idx = s_idx;
+        if (idx >= count) break;
         const int slot = A.blist[bucket][idx];
         const int kind = A.bkind[bucket][idx];
         const int j = A.st.job[slot];
@@ -559,15 +580,15 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
 }
 
 // Fixed-order sums of every batch whose walks have all finished: block
-// (job, parity) x entry; entry n_entries + 1 sums the hop counts.
+// (job, window slot) x entry; entry n_entries + 1 sums the hop counts.
 __global__ void __launch_bounds__(256) sv_reduce_kernel(SvArgs A) {
-    const int j = blockIdx.x >> 1, p = blockIdx.x & 1, e = blockIdx.y;
+    const int j = blockIdx.x / kSvWin, p = blockIdx.x % kSvWin, e = blockIdx.y;
     const SvJob& J = A.jobs[j];
     if (J.state != 1 || e > J.n_entries + 1) return;
     const SvCtr& C = A.ctr[j];
     const long long n = J.bcount[p];
     if (n <= 0 || C.reduced[p] || (long long)C.done[p] < n) return;
-    double* out = A.bsum + ((size_t)j * 2 + p) * kSvBsumStride;
+    double* out = A.bsum + ((size_t)j * kSvWin + p) * kSvBsumStride;
     const long long base = (long long)p * J.batch;
     if (e <= J.n_entries) {
         reduce_entry(e, J.n_entries, n, J.rec_end + base, J.rec_w + base, out);
@@ -589,8 +610,8 @@ __global__ void __launch_bounds__(256) sv_reduce_kernel(SvArgs A) {
 
 __global__ void sv_mark_kernel(SvArgs A) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * kSvMaxJobs) return;
-    const int j = t >> 1, p = t & 1;
+    if (t >= kSvWin * kSvMaxJobs) return;
+    const int j = t / kSvWin, p = t % kSvWin;
     const SvJob& J = A.jobs[j];
     if (J.state != 1) return;
     SvCtr& C = A.ctr[j];
@@ -816,7 +837,7 @@ static int sv_step(drwc_server* v, int k) {
         if ((rc = sv_mark(v, v->ev_t[k][0], s))) return rc;
         sv_voxelise_kernel<<<g2, 256, 0, s>>>(A);
         if ((rc = launch_check(ctx))) return rc;
-        rc = net_forward_dyn(v->net, A.S, A.cnt, A.X, A.O, A.Gh, A.frow, A.cnt + 1);
+        rc = net_forward_dyn(v->net, A.S, A.cnt, nullptr, A.O, A.Gh, A.frow, A.cnt + 1);
         if (rc) return rc;
         if ((rc = sv_mark(v, v->ev_t[k][1], s))) return rc;
         sv_sample_kernel<<<g2, 256, 0, s>>>(A);
@@ -839,10 +860,10 @@ static int sv_round_body(drwc_server* v) {
         if (rc) return rc;
     }
     cudaStream_t s = v->ctx->stream;
-    sv_reduce_kernel<<<dim3(2 * kSvMaxJobs, v->o.max_nets + 3), 256, 0, s>>>(v->A);
+    sv_reduce_kernel<<<dim3(kSvWin * kSvMaxJobs, v->o.max_nets + 3), 256, 0, s>>>(v->A);
     int rc = launch_check(v->ctx);
     if (rc) return rc;
-    sv_mark_kernel<<<1, 2 * kSvMaxJobs, 0, s>>>(v->A);
+    sv_mark_kernel<<<1, kSvWin * kSvMaxJobs, 0, s>>>(v->A);
     return launch_check(v->ctx);
 }
 
@@ -875,12 +896,14 @@ static double sv_secs(std::chrono::steady_clock::time_point a, std::chrono::stea
     return std::chrono::duration<double>(b - a).count();
 }
 
-// Footprint of a job in the arena: its structure blob and two batches of records.
+// Footprint of a job in the arena: its structure blob and the records of
+// the batches its claim window spans (16 B per walk).
 static size_t sv_footprint(const SvHostJob* J, size_t* blob_bytes) {
     const size_t blob = (J->hg.blob.size() + 255) / 256 * 256;
     *blob_bytes = blob;
-    const size_t b = (size_t)J->p.batch_walks;
-    return blob + 2 * b * 8 + 2 * b * 4 + 2 * b * 4 + 256;
+    const size_t b = (size_t)std::min<long long>(J->p.batch_walks, J->p.max_walks);
+    const size_t nb = (size_t)std::min<long long>(kSvWin, (J->p.max_walks + b - 1) / b);
+    return blob + nb * b * 16 + 256;
 }
 
 // Admit queued jobs in arrival order (caller holds v->mu and the context lock).
@@ -911,7 +934,9 @@ static int sv_admit(drwc_server* v) {
         DRWC_CUDA_TRY(cudaMemcpyAsync(base, J->hg.blob.data(), J->hg.blob.size(),
                                       cudaMemcpyHostToDevice, v->ctx->stream));
         bind_geom(&J->hg, base);
-        const long long batch = J->p.batch_walks, total = J->p.max_walks;
+        const long long total = J->p.max_walks;
+        const long long batch = std::min<long long>(J->p.batch_walks, total);
+        const long long nb = std::min<long long>(kSvWin, (total + batch - 1) / batch);
         SvJob& T = v->h_jobs[t];
         std::memset(&T, 0, sizeof T);
         T.g = J->hg.dev;
@@ -923,14 +948,16 @@ static int sv_admit(drwc_server* v) {
         T.n_entries = J->s.n_nets + 1;
         T.total = total;
         T.batch = batch;
-        T.limit = std::min(2 * batch, total);
-        T.bfirst[0] = 0;
-        T.bcount[0] = std::min(batch, total);
-        T.bfirst[1] = batch < total ? batch : -1;
-        T.bcount[1] = batch < total ? std::min(batch, total - batch) : 0;
+        T.limit = std::min(kSvWin * batch, total);
+        for (int q = 0; q < kSvWin; ++q) {
+            const bool in = q * batch < total;
+            T.bfirst[q] = in ? q * batch : -1;
+            T.bcount[q] = in ? std::min(batch, total - q * batch) : 0;
+        }
+        // records: weights, end nets, hop counts for nb window slots
         T.rec_w = (double*)(base + blob);
-        T.rec_end = (int32_t*)(base + blob + 2 * batch * 8);
-        T.rec_hops = T.rec_end + 2 * batch;
+        T.rec_end = (int32_t*)(base + blob + nb * batch * 8);
+        T.rec_hops = T.rec_end + nb * batch;
         std::memset(&v->h_ctr[t], 0, sizeof(SvCtr));
         J->table = t;
         J->arena_off = off;
@@ -949,6 +976,7 @@ static int sv_admit(drwc_server* v) {
     H.n_act = 0;
     for (int q = 0; q < kSvMaxJobs; ++q)
         if (v->table[q] && !v->table[q]->draining) H.act[H.n_act++] = q;
+    std::sort(H.act, H.act + H.n_act, [&](int a, int b) { return v->table[a]->id < v->table[b]->id; });
     v->st.max_running = std::max<int64_t>(v->st.max_running, H.n_act);
     return DRWC_OK;
 }
@@ -971,9 +999,9 @@ static void sv_fold(drwc_server* v, int t) {
     };
     for (;;) {
         const long long k = J->next_batch;
-        const int par = (int)(k & 1);
+        const int par = (int)(k % kSvWin);
         if (T.bcount[par] <= 0 || T.bfirst[par] != k * T.batch || !C.reduced[par]) break;
-        const double* sums = v->h_bsum + ((size_t)t * 2 + par) * kSvBsumStride;
+        const double* sums = v->h_bsum + ((size_t)t * kSvWin + par) * kSvBsumStride;
         for (int e = 0; e <= ne; ++e) {
             kadd(J->S[e], J->Sc[e], sums[3 * e]);
             kadd(J->S2[e], J->S2c[e], sums[3 * e + 1]);
@@ -1034,8 +1062,8 @@ static void sv_fold(drwc_server* v, int t) {
             v->cv.notify_all();
             return;
         }
-        // parity par now holds batch k + 2; the window grows by one batch
-        const long long k2 = k + 2;
+        // window slot par now holds batch k + kSvWin; the window moves by one batch
+        const long long k2 = k + kSvWin;
         if (k2 * T.batch < T.total) {
             T.bfirst[par] = k2 * T.batch;
             T.bcount[par] = std::min(T.batch, T.total - k2 * T.batch);
@@ -1045,7 +1073,7 @@ static void sv_fold(drwc_server* v, int t) {
         }
         C.done[par] = 0;
         C.reduced[par] = 0;
-        T.limit = std::min((k + 3) * T.batch, T.total);
+        T.limit = std::min((k + 1 + kSvWin) * T.batch, T.total);
     }
 }
 
@@ -1075,7 +1103,7 @@ static int sv_round(drwc_server* v) {
     ctx->launches.fetch_add(v->kernels_per_graph);
     DRWC_CUDA_TRY(cudaMemcpyAsync(v->h_ctr, v->d_ctr, sizeof(SvCtr) * kSvMaxJobs,
                                   cudaMemcpyDeviceToHost, s));
-    DRWC_CUDA_TRY(cudaMemcpyAsync(v->h_bsum, v->d_bsum, sizeof(double) * kSvBsumStride * 2 * kSvMaxJobs,
+    DRWC_CUDA_TRY(cudaMemcpyAsync(v->h_bsum, v->d_bsum, sizeof(double) * kSvBsumStride * kSvWin * kSvMaxJobs,
                                   cudaMemcpyDeviceToHost, s));
     DRWC_CUDA_TRY(cudaMemcpyAsync(v->h_stats, v->d_stats, sizeof(unsigned long long) * SV_NSTATS,
                                   cudaMemcpyDeviceToHost, s));
@@ -1168,14 +1196,14 @@ static int sv_alloc(drwc_server* v) {
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t r = off; off += (bytes + 255) / 256 * 256; return r; };
     const size_t o_jobs = take(sizeof(SvJob) * kSvMaxJobs), o_ctr = take(sizeof(SvCtr) * kSvMaxJobs),
-                 o_hdr = take(sizeof(SvHdr)), o_bsum = take(8 * kSvBsumStride * 2 * kSvMaxJobs),
+                 o_hdr = take(sizeof(SvHdr)), o_bsum = take(8 * kSvBsumStride * kSvWin * kSvMaxJobs),
                  o_stats = take(8 * SV_NSTATS), o_akl = take(16), o_cnt = take(64),
                  o_dbl = take(8 * (size_t)S * 7), o_walk = take(8 * (size_t)S),
                  o_int = take(4 * (size_t)S * 5), o_lists = take(4 * (size_t)S * 2),
                  o_b = take(4 * (size_t)S * 2 * DRWC_SERVER_MAX_SIZES);
     size_t o_X = 0, o_O = 0, o_G = 0;
     if (v->net) {
-        o_X = take(2 * (size_t)S * kSvNetN * kSvNetN * kSvNetN);
+        o_X = take(256);  // network inputs stay in shared memory
         o_O = take(4 * (size_t)S * kSvDecRows);
         o_G = take(4 * (size_t)S * DRWC_NET_PANELS);
     }
@@ -1232,6 +1260,7 @@ static int sv_alloc(drwc_server* v) {
         A.Gh = (float*)(B + o_G);
     }
     A.table = v->o.uniform_table;
+    A.fair = v->o.fair_share;
     for (int b = 0; b < v->o.n_sizes; ++b) {
         v->fdm_sy[b] = (double*)(B + o_sy[b]);
         v->fdm_ss[b] = (float*)(B + o_ss[b]);
@@ -1246,7 +1275,7 @@ static int sv_alloc(drwc_server* v) {
     size_t hoff = 0;
     auto htake = [&](size_t bytes) { size_t r = hoff; hoff += (bytes + 255) / 256 * 256; return r; };
     const size_t h_jobs = htake(sizeof(SvJob) * kSvMaxJobs), h_ctr = htake(sizeof(SvCtr) * kSvMaxJobs),
-                 h_hdr = htake(sizeof(SvHdr)), h_bsum = htake(8 * kSvBsumStride * 2 * kSvMaxJobs),
+                 h_hdr = htake(sizeof(SvHdr)), h_bsum = htake(8 * kSvBsumStride * kSvWin * kSvMaxJobs),
                  h_stats = htake(8 * SV_NSTATS), h_akl = htake(16);
     if (cudaMallocHost(&v->hblock, hoff) != cudaSuccess) { cudaGetLastError(); return DRWC_ERR_NOMEM; }
     std::memset(v->hblock, 0, hoff);
@@ -1298,6 +1327,7 @@ DRWC_API void drwc_server_opts_default(drwc_server_opts* o) {
     o->audit_frac = 0.01f;
     o->timing = 0;
     o->uniform_table = 0;
+    o->fair_share = 0;
 }
 
 DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drwc_net* net,
@@ -1311,7 +1341,8 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drw
         o.hbm_budget < 4096 || o.n_sizes < 1 || o.n_sizes > DRWC_SERVER_MAX_SIZES ||
         o.steps_per_graph < 1 || o.steps_per_graph > kSvMaxSteps || o.max_materials < 1 ||
         o.max_materials > kMaxMaterials || o.max_nets < 1 || o.max_nets > DRWC_MAX_NETS ||
-        !(o.audit_frac >= 0.f && o.audit_frac <= 1.f) || o.uniform_table < 0 || o.uniform_table > 1)
+        !(o.audit_frac >= 0.f && o.audit_frac <= 1.f) || o.uniform_table < 0 || o.uniform_table > 1 ||
+        o.fair_share < 0 || o.fair_share > 1)
         return DRWC_ERR_INVALID;
     if (net && net_context(net) != ctx) return DRWC_ERR_INVALID;
     std::unique_ptr<drwc_server> v(new drwc_server());
@@ -1341,6 +1372,7 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drw
         if (!rc) rc = sv_alloc(v.get());
         if (!rc) rc = sv_tables(v.get());
         if (!rc && net) rc = net_reserve_rows(net, o.slots);
+        if (!rc && net) v->A.c1 = net_conv1_operands(net);  // a1 as reserved for `slots` rows
         for (int b = 0; !rc && b < o.n_sizes; ++b) {
             if (cudaStreamCreateWithFlags(&v->side[b], cudaStreamNonBlocking) != cudaSuccess ||
                 cudaEventCreateWithFlags(&v->ev_join[b], cudaEventDisableTiming) != cudaSuccess)

@@ -26,6 +26,7 @@
 namespace drwc {
 
 constexpr int kUmmaM = 128;
+constexpr int kUmmaThreads = 128;                // threads of a GEMM-tile CTA
 constexpr int kUmmaBK = 64;                      // K per shared-memory stage (4 MMAs)
 constexpr uint32_t kWaitTicks = 1000000;         // try_wait suspend hint (ns)
 constexpr int kWaitRounds = 20000;               // => bounded wait of about 20 s
@@ -161,6 +162,26 @@ DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, 
     const int ktiles = (K + kUmmaBK - 1) / kUmmaBK;
     uint32_t uses[2] = {0, 0};
     bool ok = true;
+    // Operand chunks of a K stage: A 128 rows x 8 chunks of 8 BF16, B BN rows x
+    // 8 chunks, spread over the 128 threads. Each thread gathers its chunks of
+    // stage kt + 1 into registers right after the MMAs of stage kt are issued,
+    // so the global loads overlap the tensor cores and the next barrier wait.
+    constexpr int AV = kUmmaM * 8 / kUmmaThreads, BV = (BN * 8 + kUmmaThreads - 1) / kUmmaThreads;
+    uint4 ra[AV], rb[BV];
+    auto gather = [&](int kt) {
+        const int k0 = kt * kUmmaBK;
+#pragma unroll
+        for (int i = 0; i < AV; ++i) {
+            const int v = t + i * kUmmaThreads;
+            la(m0 + (v >> 3), k0 + (v & 7) * 8, &ra[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < BV; ++i) {
+            const int v = t + i * kUmmaThreads;
+            if (v < BN * 8) lb(n0 + (v >> 3), k0 + (v & 7) * 8, &rb[i]);
+        }
+    };
+    if (ktiles > 0) gather(0);
     for (int kt = 0; kt < ktiles; ++kt) {
         const int s = kt & 1;
         // the MMAs that last read this stage must be done before refilling it
@@ -168,18 +189,16 @@ DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, 
             ok &= mbar_wait(&bar[s], (uses[s] - 1) & 1);
         }
         const int k0 = kt * kUmmaBK;
-        // A: 128 rows x 8 chunks of 8 BF16; B: BN rows x 8 chunks
-        for (int v = t; v < kUmmaM * 8; v += blockDim.x) {
-            const int row = v >> 3, ch = v & 7;
-            uint4 val;
-            la(m0 + row, k0 + ch * 8, &val);
-            *reinterpret_cast<uint4*>(sa[s] + umma_tile_off(row, ch * 8, kUmmaM)) = val;
+#pragma unroll
+        for (int i = 0; i < AV; ++i) {
+            const int v = t + i * kUmmaThreads;
+            *reinterpret_cast<uint4*>(sa[s] + umma_tile_off(v >> 3, (v & 7) * 8, kUmmaM)) = ra[i];
         }
-        for (int v = t; v < BN * 8; v += blockDim.x) {
-            const int row = v >> 3, ch = v & 7;
-            uint4 val;
-            lb(n0 + row, k0 + ch * 8, &val);
-            *reinterpret_cast<uint4*>(sb[s] + umma_tile_off(row, ch * 8, BN)) = val;
+#pragma unroll
+        for (int i = 0; i < BV; ++i) {
+            const int v = t + i * kUmmaThreads;
+            if (v < BN * 8)
+                *reinterpret_cast<uint4*>(sb[s] + umma_tile_off(v >> 3, (v & 7) * 8, BN)) = rb[i];
         }
         umma_fence_proxy_async();
         __syncthreads();
@@ -194,6 +213,7 @@ DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, 
             umma_commit(&bar[s]);
         }
         uses[s] += 1;
+        if (kt + 1 < ktiles) gather(kt + 1);
     }
     // all MMAs done: the last commit covers every earlier MMA of this thread
     {

@@ -531,6 +531,7 @@ __global__ void __launch_bounds__(256) records_kernel(DevGeom g, int n, const do
     __shared__ double pal[kMaxMaterials];
     __shared__ uint8_t mat[N * N * N];
     __shared__ float red[32];
+    __shared__ VoxScratch<N> vs;
     for (int v = threadIdx.x; v < g.n_mat; v += blockDim.x) pal[v] = g.pal[v];
     centre_offsets<N>(tco);
     __syncthreads();
@@ -538,7 +539,7 @@ __global__ void __launch_bounds__(256) records_kernel(DevGeom g, int n, const do
         const double c[3] = {rec[4 * (size_t)r], rec[4 * (size_t)r + 1], rec[4 * (size_t)r + 2]};
         const double a = rec[4 * (size_t)r + 3];
         voxelise_net<N>(g, c, a, rot_of_code(code[r]), tco, pal, mat, X + (size_t)r * N * N * N,
-                        eps64 ? eps64 + (size_t)r * N * N * N : nullptr, red);
+                        eps64 ? eps64 + (size_t)r * N * N * N : nullptr, red, vs);
     }
 }
 
@@ -824,6 +825,7 @@ __global__ void __launch_bounds__(256) lw_voxelise_kernel(LwArgs A) {
     __shared__ double pal[kMaxMaterials];
     __shared__ uint8_t mat[N * N * N];
     __shared__ float red[32];
+    __shared__ VoxScratch<N> vs;
     for (int v = threadIdx.x; v < A.g.n_mat; v += blockDim.x) pal[v] = A.g.pal[v];
     centre_offsets<N>(tco);
     __syncthreads();
@@ -834,7 +836,7 @@ __global__ void __launch_bounds__(256) lw_voxelise_kernel(LwArgs A) {
         const int rot = first ? rot_of_code(A.st.code[slot]) : 0;
         const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
         voxelise_net<N>(A.g, c, A.st.a[slot], rot, tco, pal, mat, A.X + (size_t)row * N * N * N,
-                        nullptr, red);
+                        nullptr, red, vs);
         if (first && threadIdx.x == 0) {
             // centre permittivity of the gradient convention, in the rotated
             // frame where the gradient axis is z

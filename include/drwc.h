@@ -366,6 +366,10 @@ typedef struct drwc_server_opts {
                                  the precomputed uniform-permittivity Green's function (exact
                                  for such cubes: their surface values do not depend on the
                                  permittivity) instead of the network or the FDM solve */
+    int32_t fair_share;       /* 0: free slots go to the oldest running job first (first in,
+                                 first out, later jobs fill what it leaves); 1: slots rotate
+                                 over the running jobs (an even share) */
+    int32_t reserved_;
 } drwc_server_opts;
 DRWC_API void drwc_server_opts_default(drwc_server_opts* o);
 /* net (nullable): with a network, hops of N = 16 jobs go through it
