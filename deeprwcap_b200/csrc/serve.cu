@@ -49,7 +49,7 @@ constexpr int kSvNetN = DRWC_NET_N;
 constexpr int kSvDecRows = DRWC_NET_OUT;
 constexpr int kSvMaxSteps = 8;
 constexpr int kSvPrepIters = 64;  // prepare-loop passes per slot and step
-constexpr int kSvWin = 4;         // batches of walk ids a job may have in flight
+constexpr int kSvWin = 8;         // record slots per job: batches of walk ids in flight
 constexpr size_t kSvBsumStride = 3 * (DRWC_MAX_NETS + 2) + 8;  // doubles per (job, window slot)
 
 struct SvJob {
@@ -63,9 +63,9 @@ struct SvJob {
     long long total;   // walk ids [0, total)
     long long batch;   // walks per batch
     long long limit;   // ids below this may be claimed
-    long long bfirst[kSvWin];  // first walk id of the batch in window slot q (batch k: q = k % kSvWin)
+    long long bfirst[kSvWin];  // first walk id of the batch held by record slot q (-1: free)
     long long bcount[kSvWin];
-    double* rec_w;     // kSvWin x batch records, window slot q at q * batch
+    double* rec_w;     // records: slot q at q * batch
     int32_t* rec_end;
     int32_t* rec_hops;
 };
@@ -166,9 +166,12 @@ DRWC_DEV void sv_finish(const SvArgs& A, int slot, int net) {
     const int j = A.st.job[slot];
     const SvJob& J = A.jobs[j];
     const long long w = A.st.walk[slot];
-    const int p = (int)((w / J.batch) % kSvWin);
+    // the slot holding the walk's batch (every id below the claim limit has one)
+    int p = 0;
+    for (int q = 1; q < kSvWin; ++q)
+        if (w >= J.bfirst[q] && w < J.bfirst[q] + J.bcount[q]) p = q;
     const long long i = w - J.bfirst[p];
-    if (i >= 0 && i < J.bcount[p]) {  // always, as claims stop at the window's end
+    if (i >= 0 && i < J.bcount[p]) {
         const long long r = (long long)p * J.batch + i;
         J.rec_end[r] = net;
         J.rec_hops[r] = A.st.hops[slot];
@@ -674,7 +677,9 @@ struct SvHostJob {
     size_t arena_off = 0, arena_bytes = 0, blob_bytes = 0;
     bool draining = false;
     std::vector<double> S, Sc, S2, S2c;
-    long long walks = 0, lost = 0, next_batch = 0;
+    long long walks = 0, lost = 0, next_batch = 0;  // next_batch: next to fold
+    long long next_assign = 0;                       // next batch to get a record slot
+    std::map<long long, std::vector<double>> pending; // reduced, not yet folded
     unsigned long long hops = 0;
     drwc_job_result result{};
     std::chrono::steady_clock::time_point t_submit, t_admit, t_done;
@@ -954,6 +959,7 @@ static int sv_admit(drwc_server* v) {
             T.bfirst[q] = in ? q * batch : -1;
             T.bcount[q] = in ? std::min(batch, total - q * batch) : 0;
         }
+        J->next_assign = nb;
         // records: weights, end nets, hop counts for nb window slots
         T.rec_w = (double*)(base + blob);
         T.rec_end = (int32_t*)(base + blob + nb * batch * 8);
@@ -997,18 +1003,42 @@ static void sv_fold(drwc_server* v, int t) {
         else c += (x - u) + s;
         s = u;
     };
+    // every reduced batch: keep its sums, free its record slot for the next
+    // unassigned batch (a long walk holds back only its own slot)
+    for (int q = 0; q < kSvWin; ++q) {
+        if (T.bcount[q] <= 0 || !C.reduced[q]) continue;
+        const long long kq = T.bfirst[q] / T.batch;
+        const double* sums = v->h_bsum + ((size_t)t * kSvWin + q) * kSvBsumStride;
+        std::vector<double>& keep = J->pending[kq];
+        keep.assign(sums, sums + 3 * (ne + 1) + 1);
+        keep.push_back((double)T.bcount[q]);
+        const long long kn = J->next_assign;
+        if (kn * T.batch < T.total) {
+            T.bfirst[q] = kn * T.batch;
+            T.bcount[q] = std::min(T.batch, T.total - kn * T.batch);
+            J->next_assign = kn + 1;
+        } else {
+            T.bfirst[q] = -1;
+            T.bcount[q] = 0;
+        }
+        C.done[q] = 0;
+        C.reduced[q] = 0;
+    }
+    T.limit = std::min(J->next_assign * T.batch, T.total);
+    // fold in batch order, exactly as drwc_frw_run does
     for (;;) {
+        auto it = J->pending.find(J->next_batch);
+        if (it == J->pending.end()) break;
+        const std::vector<double> sums = std::move(it->second);
+        J->pending.erase(it);
         const long long k = J->next_batch;
-        const int par = (int)(k % kSvWin);
-        if (T.bcount[par] <= 0 || T.bfirst[par] != k * T.batch || !C.reduced[par]) break;
-        const double* sums = v->h_bsum + ((size_t)t * kSvWin + par) * kSvBsumStride;
         for (int e = 0; e <= ne; ++e) {
             kadd(J->S[e], J->Sc[e], sums[3 * e]);
             kadd(J->S2[e], J->S2c[e], sums[3 * e + 1]);
         }
         J->lost += (long long)sums[3 * ne + 2];
         J->hops += (unsigned long long)sums[3 * (ne + 1)];
-        J->walks += T.bcount[par];
+        J->walks += (long long)sums[3 * (ne + 1) + 1];
         J->next_batch = k + 1;
         bool finished = J->walks >= p.max_walks;
         int converged = 0;
@@ -1062,18 +1092,6 @@ static void sv_fold(drwc_server* v, int t) {
             v->cv.notify_all();
             return;
         }
-        // window slot par now holds batch k + kSvWin; the window moves by one batch
-        const long long k2 = k + kSvWin;
-        if (k2 * T.batch < T.total) {
-            T.bfirst[par] = k2 * T.batch;
-            T.bcount[par] = std::min(T.batch, T.total - k2 * T.batch);
-        } else {
-            T.bfirst[par] = -1;
-            T.bcount[par] = 0;
-        }
-        C.done[par] = 0;
-        C.reduced[par] = 0;
-        T.limit = std::min((k + 1 + kSvWin) * T.batch, T.total);
     }
 }
 

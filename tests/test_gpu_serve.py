@@ -55,9 +55,9 @@ def test_served_job_equals_frw_run(ctx):
 def test_mix_equals_alone_with_admission_by_footprint(ctx):
     jobs = _jobs()
     alone = [engine.extract(s, p, ctx) for s, p in jobs]
-    # each job needs its structure + the records of its 4-batch claim window
-    # (8192 walks x 16 B x 4): two fit, three do not
-    budget = 2 * (4 * 8192 * 16 + 64 * 1024)
+    # each job needs its structure + 16 B of records per walk of the batches it
+    # can hold at once (4-5 batches of 8192 here): two fit, three do not
+    budget = 1400 * 1024
     with engine.Server(ctx, slots=16384, max_jobs=8, hbm_budget=budget) as srv:
         ids = []
         for s, p in jobs:
