@@ -49,6 +49,19 @@ template <int D, int C>
 struct ConvGather {
     const bf16* __restrict__ x;
     int rows;  // B * Do^3
+    // with 8k input channels a chunk is 8 channels of one tap: 16 contiguous bytes
+    static constexpr bool kChunks = C % 8 == 0;
+    DRWC_DEV bool chunks_ok() const { return (reinterpret_cast<uintptr_t>(x) & 15) == 0; }
+    DRWC_DEV const void* chunk(int r, int k8) const {
+        constexpr int Do = D / 2, P = Do * Do * Do, K = 27 * C;
+        if (r >= rows || k8 >= K) return nullptr;
+        const int b = r / P, p = r % P;
+        const int pz = p / (Do * Do), py = (p / Do) % Do, px = p % Do;
+        const int tap = k8 / C, ci = k8 % C;
+        const int z = 2 * pz - 1 + tap / 9, y = 2 * py - 1 + (tap / 3) % 3, xx = 2 * px - 1 + tap % 3;
+        if (z < 0 || z >= D || y < 0 || y >= D || xx < 0 || xx >= D) return nullptr;
+        return x + ((((int64_t)b * D + z) * D + y) * D + xx) * C + ci;
+    }
     DRWC_DEV void operator()(int r, int k8, uint4* out) const {
         constexpr int Do = D / 2, P = Do * Do * Do, K = 27 * C;
         if (r >= rows || k8 >= K) { *out = make_uint4(0, 0, 0, 0); return; }
@@ -89,6 +102,7 @@ template <int D, int C>
 struct Im2colT {
     const bf16* __restrict__ x;
     int nrows;  // B * Do^3 (the reduction length)
+    static constexpr bool kChunks = false;
     DRWC_DEV void operator()(int kk, int r8, uint4* out) const {
         constexpr int Do = D / 2, P = Do * Do * Do, K = 27 * C;
         __align__(16) bf16 tmp[8];
@@ -118,6 +132,7 @@ template <int D, int CO>
 struct ConvTGather {
     const bf16* __restrict__ dz;  // [B * Do^3, CO]
     int rows;                     // B * D^3
+    static constexpr bool kChunks = false;
     DRWC_DEV void operator()(int r, int k8, uint4* out) const {
         constexpr int Do = D / 2, P = Do * Do * Do, Q = D * D * D, K = 27 * CO;
         static_assert(CO % 8 == 0, "output channels per chunk");
@@ -140,6 +155,7 @@ struct ConvTGather {
 template <int CI, int CO>
 struct WeightT {
     const bf16* __restrict__ w;  // [CO][27*CI]
+    static constexpr bool kChunks = false;
     DRWC_DEV void operator()(int ci, int k8, uint4* out) const {
         __align__(16) bf16 tmp[8];
         const int tap = k8 / CO, co0 = k8 % CO;
@@ -220,6 +236,15 @@ template <class L>
 struct KSlice {
     L inner;
     int koff, kend;
+    static constexpr bool kChunks = L::kChunks;
+    DRWC_DEV bool chunks_ok() const {
+        if constexpr (L::kChunks) return inner.chunks_ok() && koff % 8 == 0 && kend % 8 == 0;
+        else return false;
+    }
+    DRWC_DEV const void* chunk(int r, int k8) const {
+        if (k8 + koff >= kend) return nullptr;
+        return loader_chunk(inner, r, k8 + koff);
+    }
     DRWC_DEV void operator()(int r, int k8, uint4* out) const {
         const int k = k8 + koff;
         if (k >= kend) { *out = make_uint4(0, 0, 0, 0); return; }

@@ -13,6 +13,14 @@ struct RowLoader {
     const __nv_bfloat16* __restrict__ p;
     int rows, cols;
     int64_t ld;
+    static constexpr bool kChunks = true;
+    DRWC_DEV bool chunks_ok() const {
+        return cols % 8 == 0 && ld % 8 == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+    }
+    DRWC_DEV const void* chunk(int r, int k8) const {
+        if (r >= rows || k8 >= cols) return nullptr;
+        return p + (int64_t)r * ld + k8;
+    }
     DRWC_DEV void operator()(int r, int k8, uint4* out) const {
         if (r >= rows || k8 >= cols) { *out = make_uint4(0, 0, 0, 0); return; }
         const __nv_bfloat16* src = p + (int64_t)r * ld + k8;

@@ -122,31 +122,65 @@ DRWC_DEV uint32_t umma_tile_off(int row, int k, int rows) {
                       (row & 7) * 16 + (k & 7) * 2);
 }
 
-// Shared memory a CTA of umma_gemm<BN> needs.
+// Shared-memory stages of a tile: enough K stages in flight to cover the
+// global latency at two CTAs per SM.
+template <int BN>
+constexpr int umma_stages() {
+    return BN >= 128 ? 3 : 4;
+}
+
+// Shared memory a CTA of umma_gemm<BN> needs: the stages, their mbarriers
+// and the TMEM address slot.
 template <int BN>
 constexpr size_t umma_smem_bytes() {
-    return 2 * (size_t)(kUmmaM + BN) * kUmmaBK * 2 + 64;
+    return (size_t)umma_stages<BN>() * (kUmmaM + BN) * kUmmaBK * 2 + 8 * 8 + 16;
+}
+
+DRWC_DEV void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src),
+                 "r"(src_bytes)
+                 : "memory");
+}
+DRWC_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+DRWC_DEV void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// A valid global address for zero-filled copies (no byte is read from it).
+static __device__ __align__(16) uint4 umma_zero16;
+
+// Loader protocol. Every loader is a functor (row, k8, uint4* out) writing the
+// 8 BF16 values of columns k8..k8+7 of an operand row (zeros outside). A
+// loader whose every such chunk is 16 contiguous, 16-byte aligned bytes of
+// global memory (or all zeros) also sets kChunks = true and provides
+// chunk(row, k8) -> source address or nullptr (zeros) and chunks_ok() (its
+// run-time alignment conditions); tiles whose two loaders both qualify fill
+// their stages with cp.async instead of through registers.
+template <class L>
+DRWC_DEV const void* loader_chunk(const L& l, int r, int k8) {
+    if constexpr (L::kChunks) return l.chunk(r, k8);
+    else return nullptr;
 }
 
 // C tile = A[m0:m0+128, :] * B[n0:n0+BN, :]^T.
-//   la(row, k8, out) / lb(row, k8, out): write the 8 BF16 values of columns
-//   k8..k8+7 of operand row `row` (zeros outside the matrix) as a uint4.
+//   la(row, k8, out) / lb(row, k8, out): loaders (above).
 //   epi(row, col0, v[32]): consume 32 FP32 accumulator values of one row.
 // err: device flag set on a wait timeout.
 template <int BN, class LA, class LB, class EPI>
 DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, const LB& lb,
                              const EPI& epi, int* err, unsigned char* smem) {
+    constexpr int S = umma_stages<BN>();
     constexpr int STAGE_A = kUmmaM * kUmmaBK * 2, STAGE_B = BN * kUmmaBK * 2;
-    unsigned char* sa[2] = {smem, smem + STAGE_A + STAGE_B};
-    unsigned char* sb[2] = {smem + STAGE_A, smem + 2 * STAGE_A + STAGE_B};
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + 2 * (STAGE_A + STAGE_B));
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 2);
+    auto stA = [&](int st) { return smem + st * (STAGE_A + STAGE_B); };
+    auto stB = [&](int st) { return smem + st * (STAGE_A + STAGE_B) + STAGE_A; };
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S * (STAGE_A + STAGE_B));
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 8);
     constexpr uint32_t TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
 
     if (t == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int q = 0; q < S; ++q) mbar_init(&bar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -160,70 +194,114 @@ DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, 
     const uint32_t tmem = *tslot;
 
     const int ktiles = (K + kUmmaBK - 1) / kUmmaBK;
-    uint32_t uses[2] = {0, 0};
+    uint32_t uses[S];
+#pragma unroll
+    for (int q = 0; q < S; ++q) uses[q] = 0;
     bool ok = true;
     // Operand chunks of a K stage: A 128 rows x 8 chunks of 8 BF16, B BN rows x
-    // 8 chunks, spread over the 128 threads. Each thread gathers its chunks of
-    // stage kt + 1 into registers right after the MMAs of stage kt are issued,
-    // so the global loads overlap the tensor cores and the next barrier wait.
+    // 8 chunks, spread over the 128 threads.
     constexpr int AV = kUmmaM * 8 / kUmmaThreads, BV = (BN * 8 + kUmmaThreads - 1) / kUmmaThreads;
-    uint4 ra[AV], rb[BV];
-    auto gather = [&](int kt) {
+    auto mma_stage = [&](int kt, int st) {  // thread 0
+        tc_fence_after();
         const int k0 = kt * kUmmaBK;
-#pragma unroll
-        for (int i = 0; i < AV; ++i) {
-            const int v = t + i * kUmmaThreads;
-            la(m0 + (v >> 3), k0 + (v & 7) * 8, &ra[i]);
+        const int ksteps = min(kUmmaBK, K - k0 + 15) / 16;  // K steps with data
+        for (int ks = 0; ks < ksteps && ks < kUmmaBK / 16; ++ks) {
+            const uint64_t da = umma_smem_desc(smem_u32(stA(st) + ks * kUmmaM * 32), 128, 256);
+            const uint64_t db = umma_smem_desc(smem_u32(stB(st) + ks * BN * 32), 128, 256);
+            umma_bf16(tmem, da, db, umma_idesc_bf16<BN>(), (kt > 0 || ks > 0) ? 1u : 0u);
         }
-#pragma unroll
-        for (int i = 0; i < BV; ++i) {
-            const int v = t + i * kUmmaThreads;
-            if (v < BN * 8) lb(n0 + (v >> 3), k0 + (v & 7) * 8, &rb[i]);
-        }
+        umma_commit(&bar[st]);
     };
-    if (ktiles > 0) gather(0);
-    for (int kt = 0; kt < ktiles; ++kt) {
-        const int s = kt & 1;
-        // the MMAs that last read this stage must be done before refilling it
-        if (kt >= 2) {
-            ok &= mbar_wait(&bar[s], (uses[s] - 1) & 1);
-        }
-        const int k0 = kt * kUmmaBK;
+    bool async_path = false;
+    if constexpr (LA::kChunks && LB::kChunks) async_path = la.chunks_ok() && lb.chunks_ok();
+    if (async_path) {
+        // cp.async pipeline: S - 1 stages in flight ahead of the MMAs; a stage
+        // is refilled once the MMAs that read it have committed.
+        auto issue = [&](int kt) {
+            const int st = kt % S, k0 = kt * kUmmaBK;
 #pragma unroll
-        for (int i = 0; i < AV; ++i) {
-            const int v = t + i * kUmmaThreads;
-            *reinterpret_cast<uint4*>(sa[s] + umma_tile_off(v >> 3, (v & 7) * 8, kUmmaM)) = ra[i];
-        }
-#pragma unroll
-        for (int i = 0; i < BV; ++i) {
-            const int v = t + i * kUmmaThreads;
-            if (v < BN * 8)
-                *reinterpret_cast<uint4*>(sb[s] + umma_tile_off(v >> 3, (v & 7) * 8, BN)) = rb[i];
-        }
-        umma_fence_proxy_async();
-        __syncthreads();
-        if (t == 0) {
-            tc_fence_after();
-            const int ksteps = min(kUmmaBK, K - k0 + 15) / 16;  // K steps with data
-            for (int ks = 0; ks < ksteps && ks < kUmmaBK / 16; ++ks) {
-                const uint64_t da = umma_smem_desc(smem_u32(sa[s] + ks * kUmmaM * 32), 128, 256);
-                const uint64_t db = umma_smem_desc(smem_u32(sb[s] + ks * BN * 32), 128, 256);
-                umma_bf16(tmem, da, db, umma_idesc_bf16<BN>(), (kt > 0 || ks > 0) ? 1u : 0u);
+            for (int i = 0; i < AV; ++i) {
+                const int v = t + i * kUmmaThreads;
+                const void* src = loader_chunk(la, m0 + (v >> 3), k0 + (v & 7) * 8);
+                cp_async16(smem_u32(stA(st) + umma_tile_off(v >> 3, (v & 7) * 8, kUmmaM)),
+                           src ? src : (const void*)&umma_zero16, src ? 16u : 0u);
             }
-            umma_commit(&bar[s]);
+#pragma unroll
+            for (int i = 0; i < BV; ++i) {
+                const int v = t + i * kUmmaThreads;
+                if (v < BN * 8) {
+                    const void* src = loader_chunk(lb, n0 + (v >> 3), k0 + (v & 7) * 8);
+                    cp_async16(smem_u32(stB(st) + umma_tile_off(v >> 3, (v & 7) * 8, BN)),
+                               src ? src : (const void*)&umma_zero16, src ? 16u : 0u);
+                }
+            }
+        };
+#pragma unroll
+        for (int kt = 0; kt < S - 1; ++kt) {
+            if (kt < ktiles) issue(kt);
+            cp_async_commit();
         }
-        uses[s] += 1;
-        if (kt + 1 < ktiles) gather(kt + 1);
-    }
-    // all MMAs done: the last commit covers every earlier MMA of this thread
-    {
-        const int s_last = (ktiles - 1) & 1;
-        ok &= mbar_wait(&bar[s_last], (uses[s_last] - 1) & 1);
-        if (ktiles >= 2) {
-            const int s_prev = ktiles & 1;
-            ok &= mbar_wait(&bar[s_prev], (uses[s_prev] - 1) & 1);
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const int st = kt % S;
+            cp_async_wait<S - 2>();  // this thread's copies of stage kt have landed
+            umma_fence_proxy_async();
+            __syncthreads();
+            if (t == 0) mma_stage(kt, st);
+            uses[st] += 1;
+            const int kn = kt + S - 1;  // refill the stage tile kt - 1 used
+            if (kn < ktiles) {
+                const int sn = kn % S;
+                if (uses[sn] > 0) ok &= mbar_wait(&bar[sn], (uses[sn] - 1) & 1);
+                issue(kn);
+            }
+            cp_async_commit();
+        }
+        cp_async_wait<0>();
+    } else {
+        // register path: the next stage is gathered into registers while the
+        // MMAs of this one run; two stages alternate
+        uint4 ra[AV], rb[BV];
+        auto gather = [&](int kt) {
+            const int k0 = kt * kUmmaBK;
+#pragma unroll
+            for (int i = 0; i < AV; ++i) {
+                const int v = t + i * kUmmaThreads;
+                la(m0 + (v >> 3), k0 + (v & 7) * 8, &ra[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < BV; ++i) {
+                const int v = t + i * kUmmaThreads;
+                if (v < BN * 8) lb(n0 + (v >> 3), k0 + (v & 7) * 8, &rb[i]);
+            }
+        };
+        if (ktiles > 0) gather(0);
+        for (int kt = 0; kt < ktiles; ++kt) {
+            const int st = kt & 1;
+            // the MMAs that last read this stage must be done before refilling it
+            if (uses[st] > 0) ok &= mbar_wait(&bar[st], (uses[st] - 1) & 1);
+#pragma unroll
+            for (int i = 0; i < AV; ++i) {
+                const int v = t + i * kUmmaThreads;
+                *reinterpret_cast<uint4*>(stA(st) + umma_tile_off(v >> 3, (v & 7) * 8, kUmmaM)) = ra[i];
+            }
+#pragma unroll
+            for (int i = 0; i < BV; ++i) {
+                const int v = t + i * kUmmaThreads;
+                if (v < BN * 8)
+                    *reinterpret_cast<uint4*>(stB(st) + umma_tile_off(v >> 3, (v & 7) * 8, BN)) = rb[i];
+            }
+            umma_fence_proxy_async();
+            __syncthreads();
+            if (t == 0) mma_stage(kt, st);
+            uses[st] += 1;
+            if (kt + 1 < ktiles) gather(kt + 1);
         }
     }
+    // all MMAs done: wait for the last commit of every stage used (at most one
+    // phase of each barrier is outstanding)
+#pragma unroll
+    for (int q = 0; q < S; ++q)
+        if (uses[q] > 0) ok &= mbar_wait(&bar[q], (uses[q] - 1) & 1);
     tc_fence_after();
     if (!ok && err) atomicExch(err, 1);
     // epilogue: warp w reads accumulator lanes (rows) 32w .. 32w+31
@@ -261,6 +339,14 @@ struct RowsBf16 {
     int rows, cols;
     int64_t ld;
     const int* __restrict__ map;
+    static constexpr bool kChunks = true;
+    DRWC_DEV bool chunks_ok() const {
+        return cols % 8 == 0 && ld % 8 == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+    }
+    DRWC_DEV const void* chunk(int r, int k8) const {
+        if (r >= rows || k8 >= cols) return nullptr;
+        return p + (map ? (int64_t)map[r] : (int64_t)r) * ld + k8;
+    }
     DRWC_DEV void operator()(int r, int k8, uint4* out) const {
         if (r >= rows || k8 >= cols) { *out = make_uint4(0, 0, 0, 0); return; }
         const int64_t rr = map ? map[r] : r;
@@ -282,6 +368,7 @@ struct ColsBf16 {
     const __nv_bfloat16* __restrict__ p;
     int rows, cols;      // operand shape (rows = S columns, cols = S rows)
     int64_t ld;          // S leading dimension
+    static constexpr bool kChunks = false;
     DRWC_DEV void operator()(int r, int k8, uint4* out) const {
         __align__(16) __nv_bfloat16 tmp[8];
 #pragma unroll

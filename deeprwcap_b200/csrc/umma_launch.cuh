@@ -28,6 +28,15 @@ template <class L>
 struct RowClamp {
     L inner;
     int M;
+    static constexpr bool kChunks = L::kChunks;
+    DRWC_DEV bool chunks_ok() const {
+        if constexpr (L::kChunks) return inner.chunks_ok();
+        else return false;
+    }
+    DRWC_DEV const void* chunk(int r, int k8) const {
+        if (r >= M) return nullptr;
+        return loader_chunk(inner, r, k8);
+    }
     DRWC_DEV void operator()(int r, int k8, uint4* out) const {
         if (r >= M) { *out = make_uint4(0, 0, 0, 0); return; }
         inner(r, k8, out);
