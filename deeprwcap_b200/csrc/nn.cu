@@ -176,6 +176,21 @@ struct EpiReluBf16 {
     int N;
     DRWC_DEV void operator()(int row, int col0, const float* v) const {
         bf16* dst = out + (int64_t)row * N;
+        if (col0 + 32 <= N && ((reinterpret_cast<uintptr_t>(dst + col0) & 15) == 0)) {
+            // 32 values = four 16-byte stores
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                __align__(16) __nv_bfloat162 h[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int i = 8 * q + 2 * e;
+                    h[e] = __floats2bfloat162_rn(fmaxf(v[i] + bias[col0 + i], 0.f),
+                                                 fmaxf(v[i + 1] + bias[col0 + i + 1], 0.f));
+                }
+                reinterpret_cast<uint4*>(dst + col0)[q] = *reinterpret_cast<const uint4*>(h);
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
             const int c = col0 + i;
@@ -193,6 +208,18 @@ struct EpiF32 {
     const int* __restrict__ rowmap;  // output row = rowmap[row] when set
     DRWC_DEV void operator()(int row, int col0, const float* v) const {
         float* dst = out + (int64_t)(rowmap ? rowmap[row] : row) * ld;
+        if (col0 + 32 <= N && ((reinterpret_cast<uintptr_t>(dst + col0) & 15) == 0)) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                float4 o;
+                o.x = v[4 * q] + (bias ? bias[col0 + 4 * q] : 0.f);
+                o.y = v[4 * q + 1] + (bias ? bias[col0 + 4 * q + 1] : 0.f);
+                o.z = v[4 * q + 2] + (bias ? bias[col0 + 4 * q + 2] : 0.f);
+                o.w = v[4 * q + 3] + (bias ? bias[col0 + 4 * q + 3] : 0.f);
+                reinterpret_cast<float4*>(dst + col0)[q] = o;
+            }
+            return;
+        }
 #pragma unroll
         for (int i = 0; i < 32; ++i) {
             const int c = col0 + i;

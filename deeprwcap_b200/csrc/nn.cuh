@@ -46,33 +46,41 @@ struct NetConv1 {
 NetConv1 net_conv1_operands(drwc_net* n);
 
 // conv1 of one 16^3 cube on the CUDA cores, CTA-wide: x (shared, BF16 eps /
-// max eps), w (shared, FP32 copies of the BF16 weights), b (shared, bias) ->
+// max eps), w4 (shared, FP32 copies of the BF16 weights, tap-major: w4[tap *
+// 4 + g] holds output channels 4g..4g+3 of that tap), b (shared, bias) ->
 // a1 rows [512][16] BF16 = ReLU(b + sum over taps of w * x), zero padding,
 // stride 2. The operands are the BF16 values the tensor-core layer reads and
 // every product is exact in FP32; only the FP32 summation order differs.
 // With one input channel its GEMM has K = 27, too thin for the tensor cores,
 // while 221K FMAs per cube run next to the voxelisation that produced x.
-DRWC_DEV_INLINE void conv1_cube(const __nv_bfloat16* x, const float* w, const float* b,
+DRWC_DEV_INLINE void conv1_cube(const __nv_bfloat16* x, const float4* w4, const float* b,
                                 __nv_bfloat16* __restrict__ a1) {
     constexpr int D = 16, Do = 8, P = Do * Do * Do;
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
         const int pz = p / (Do * Do), py = (p / Do) % Do, px = p % Do;
-        float xv[27];
+        float acc[16];
 #pragma unroll
-        for (int tap = 0; tap < 27; ++tap) {
+        for (int co = 0; co < 16; ++co) acc[co] = 0.f;
+#pragma unroll 3
+        for (int tap = 0; tap < 27; ++tap) {  // partly unrolled: weights stream from shared
             const int z = 2 * pz - 1 + tap / 9, y = 2 * py - 1 + (tap / 3) % 3,
                       xx = 2 * px - 1 + tap % 3;
             const bool in = z >= 0 && z < D && y >= 0 && y < D && xx >= 0 && xx < D;
-            xv[tap] = in ? __bfloat162float(x[(z * D + y) * D + xx]) : 0.f;
-        }
-        __align__(16) __nv_bfloat16 out[16];
+            const float xv = in ? __bfloat162float(x[(z * D + y) * D + xx]) : 0.f;
 #pragma unroll
-        for (int co = 0; co < 16; ++co) {
-            float acc = 0.f;
-#pragma unroll
-            for (int tap = 0; tap < 27; ++tap) acc = fmaf(w[co * 27 + tap], xv[tap], acc);
-            out[co] = __float2bfloat16(fmaxf(acc + b[co], 0.f));
+            for (int g = 0; g < 4; ++g) {
+                const float4 w = w4[tap * 4 + g];
+                acc[4 * g] = fmaf(w.x, xv, acc[4 * g]);
+                acc[4 * g + 1] = fmaf(w.y, xv, acc[4 * g + 1]);
+                acc[4 * g + 2] = fmaf(w.z, xv, acc[4 * g + 2]);
+                acc[4 * g + 3] = fmaf(w.w, xv, acc[4 * g + 3]);
+            }
         }
+        __align__(16) __nv_bfloat162 out[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            out[q] = __floats2bfloat162_rn(fmaxf(acc[2 * q] + b[2 * q], 0.f),
+                                           fmaxf(acc[2 * q + 1] + b[2 * q + 1], 0.f));
         uint4* dst = reinterpret_cast<uint4*>(a1 + (size_t)p * 16);
         dst[0] = reinterpret_cast<const uint4*>(out)[0];
         dst[1] = reinterpret_cast<const uint4*>(out)[1];

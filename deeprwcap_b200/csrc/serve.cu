@@ -340,17 +340,22 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
 // One CTA (256 threads) per network row: the cube voxelised in shared
 // memory (eps / max eps, BF16) and the network's first layer applied to it,
 // so only conv1's activations reach global memory.
-__global__ void __launch_bounds__(256) sv_voxelise_kernel(SvArgs A) {
+__global__ void __launch_bounds__(256, 3) sv_voxelise_kernel(SvArgs A) {
     constexpr int N = kSvNetN;
     __shared__ double tco[N];
     __shared__ double pal[kMaxMaterials];
     __shared__ uint8_t mat[N * N * N];
     __shared__ __align__(16) __nv_bfloat16 xs[N * N * N];
-    __shared__ float w1[16 * 27], b1[16];
+    __shared__ float4 w4[27 * 4];
+    __shared__ float b1[16];
     __shared__ VoxScratch<N> vs;
     __shared__ float red[32];
     centre_offsets<N>(tco);
-    for (int q = threadIdx.x; q < 16 * 27; q += blockDim.x) w1[q] = __bfloat162float(A.c1.w1[q]);
+    // weights [co][tap] -> tap-major float4 groups of 4 output channels
+    for (int q = threadIdx.x; q < 16 * 27; q += blockDim.x) {
+        const int co = q / 27, tap = q % 27;
+        reinterpret_cast<float*>(w4)[tap * 16 + co] = __bfloat162float(A.c1.w1[q]);
+    }
     if (threadIdx.x < 16) b1[threadIdx.x] = A.c1.b1[threadIdx.x];
     const int na = (int)A.cnt[0];
     int loaded = -1;
@@ -372,7 +377,7 @@ __global__ void __launch_bounds__(256) sv_voxelise_kernel(SvArgs A) {
             const EpsPalette E{mat, pal, nullptr, nullptr, nullptr, 0};
             A.st.epsw[slot] = center_diel<N>(E, DRWC_WVTZ);
         }
-        conv1_cube(xs, w1, b1, A.c1.a1 + (size_t)row * 512 * 16);
+        conv1_cube(xs, w4, b1, A.c1.a1 + (size_t)row * 512 * 16);
         __syncthreads();
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.stats + SV_NET_ROWS, (unsigned long long)na);
@@ -1387,6 +1392,10 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drw
             const double* w[4];
             if (!rc) rc = warm_tables(ctx, o.sizes[b], w);
         }
+        if (!rc && cudaFuncSetAttribute(sv_voxelise_kernel,
+                                        cudaFuncAttributePreferredSharedMemoryCarveout, 50) !=
+                       cudaSuccess)
+            rc = DRWC_ERR_CUDA;  // room for four voxeliser CTAs per SM
         if (!rc) rc = sv_alloc(v.get());
         if (!rc) rc = sv_tables(v.get());
         if (!rc && net) rc = net_reserve_rows(net, o.slots);

@@ -167,31 +167,65 @@ DRWC_DEV const void* loader_chunk(const L& l, int r, int k8) {
 //   la(row, k8, out) / lb(row, k8, out): loaders (above).
 //   epi(row, col0, v[32]): consume 32 FP32 accumulator values of one row.
 // err: device flag set on a wait timeout.
+// tmem_cols: the TMEM columns one tile needs (allocated with tcgen05.alloc).
+template <int BN>
+constexpr uint32_t umma_tmem_cols() {
+    return BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
+}
+
+// TMEM allocation of a CTA (warp 0 allocates and gives up the permit to
+// allocate again, which lets the SM place further CTAs); all threads read the
+// address back from the shared slot.
+template <int BN>
+DRWC_DEV uint32_t umma_tmem_alloc(uint32_t* tslot) {
+    if ((threadIdx.x >> 5) == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tslot)), "r"(umma_tmem_cols<BN>()));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    return *tslot;
+}
+
+template <int BN>
+DRWC_DEV void umma_tmem_free(uint32_t tmem) {
+    tc_fence_before();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(umma_tmem_cols<BN>()));
+}
+
+// Address of the TMEM slot inside a tile CTA's shared memory.
+template <int BN>
+DRWC_DEV uint32_t* umma_tslot(unsigned char* smem) {
+    return reinterpret_cast<uint32_t*>(smem + umma_stages<BN>() * (kUmmaM + BN) * kUmmaBK * 2 + 8 * 8);
+}
+
+// tmem_given: a TMEM accumulator the caller allocated (umma_tmem_alloc) and
+// keeps across tiles; 0xffffffff: this call allocates and frees its own.
 template <int BN, class LA, class LB, class EPI>
 DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, const LB& lb,
-                             const EPI& epi, int* err, unsigned char* smem) {
+                             const EPI& epi, int* err, unsigned char* smem,
+                             uint32_t tmem_given = 0xffffffffu) {
     constexpr int S = umma_stages<BN>();
     constexpr int STAGE_A = kUmmaM * kUmmaBK * 2, STAGE_B = BN * kUmmaBK * 2;
     auto stA = [&](int st) { return smem + st * (STAGE_A + STAGE_B); };
     auto stB = [&](int st) { return smem + st * (STAGE_A + STAGE_B) + STAGE_A; };
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S * (STAGE_A + STAGE_B));
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 8);
-    constexpr uint32_t TCOLS = BN <= 32 ? 32 : BN <= 64 ? 64 : BN <= 128 ? 128 : 256;
     const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
 
     if (t == 0) {
         for (int q = 0; q < S; ++q) mbar_init(&bar[q], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     ::"r"(smem_u32(tslot)), "r"(TCOLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem = *tslot;
+    const bool own = tmem_given == 0xffffffffu;
+    uint32_t tmem = tmem_given;
+    if (own) tmem = umma_tmem_alloc<BN>(tslot);  // (synchronises the CTA)
+    else __syncthreads();                         // barriers initialised before use
 
     const int ktiles = (K + kUmmaBK - 1) / kUmmaBK;
     uint32_t uses[S];
@@ -311,11 +345,10 @@ DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, 
         tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
         if (ok && row < M && n0 + c < N) epi(row, n0 + c, v);
     }
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) {
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                     "r"(TCOLS));
+    if (own) umma_tmem_free<BN>(tmem);
+    else {
+        tc_fence_before();
+        __syncthreads();  // the accumulator is read before the next tile's MMAs
     }
 }
 

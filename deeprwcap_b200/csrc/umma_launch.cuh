@@ -15,6 +15,8 @@ inline int launch_umma(drwc_ctx* ctx, int M, int N, int K, const LA& la, const L
         DRWC_CUDA_TRY(cudaFuncSetAttribute(umma_kernel<BN, LA, LB, EPI>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)umma_smem_bytes<BN>()));
+        DRWC_CUDA_TRY(cudaFuncSetAttribute(umma_kernel<BN, LA, LB, EPI>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout, 100));
         attr = true;
     }
     dim3 grid((M + kUmmaM - 1) / kUmmaM, (N + BN - 1) / BN);
@@ -44,8 +46,10 @@ struct RowClamp {
 };
 
 // GEMM whose row count is read on the device: M = min(Mmax, *mcount * mmul).
-// The grid covers Mmax; tiles past M return before touching shared or tensor
-// memory, so the launch can sit in a CUDA graph while M changes per replay.
+// A grid of a few CTAs per SM walks the 128-row tiles (tile = blockIdx.x,
+// +gridDim.x, ...); each tile runs the whole tile routine, so the launch can
+// sit in a CUDA graph while M changes per replay without paying for a grid
+// sized to Mmax when few rows are present.
 template <int BN, class LA, class LB, class EPI>
 __global__ void __launch_bounds__(128) umma_dyn_kernel(int Mmax, const unsigned* __restrict__ mcount,
                                                        int mmul, int N, int K, LA la, LB lb,
@@ -53,24 +57,38 @@ __global__ void __launch_bounds__(128) umma_dyn_kernel(int Mmax, const unsigned*
     extern __shared__ __align__(1024) unsigned char umma_smem[];
     const long long m = (long long)(*mcount) * mmul;
     const int M = m < Mmax ? (int)m : Mmax;
-    if ((int)blockIdx.x * kUmmaM >= M) return;
+    const int ntiles = (M + kUmmaM - 1) / kUmmaM;
+    if ((int)blockIdx.x >= ntiles) return;
     RowClamp<LA> ca{la, M};
-    umma_gemm_tile<BN>(M, N, K, blockIdx.x * kUmmaM, blockIdx.y * BN, ca, lb, epi, err, umma_smem);
+    const uint32_t tmem = umma_tmem_alloc<BN>(umma_tslot<BN>(umma_smem));
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+        umma_gemm_tile<BN>(M, N, K, tile * kUmmaM, blockIdx.y * BN, ca, lb, epi, err, umma_smem,
+                           tmem);
+    umma_tmem_free<BN>(tmem);
 }
 
 template <int BN, class LA, class LB, class EPI>
 inline int launch_umma_dyn(drwc_ctx* ctx, int Mmax, const unsigned* mcount, int mmul, int N,
                            int K, const LA& la, const LB& lb, const EPI& epi, int* err) {
     if (Mmax <= 0 || N <= 0) return DRWC_OK;
-    static bool attr = false;
-    if (!attr) {
+    static int per_sm = 0;
+    if (!per_sm) {
         DRWC_CUDA_TRY(cudaFuncSetAttribute(umma_dyn_kernel<BN, LA, LB, EPI>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)umma_smem_bytes<BN>()));
-        attr = true;
+        DRWC_CUDA_TRY(cudaFuncSetAttribute(umma_dyn_kernel<BN, LA, LB, EPI>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        DRWC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+            &per_sm, umma_dyn_kernel<BN, LA, LB, EPI>, 128, umma_smem_bytes<BN>()));
+        if (per_sm < 1) per_sm = 1;
     }
-    dim3 grid((Mmax + kUmmaM - 1) / kUmmaM, (N + BN - 1) / BN);
-    umma_dyn_kernel<BN, LA, LB, EPI><<<grid, 128, umma_smem_bytes<BN>(), ctx->stream>>>(
+    const int ntiles = (Mmax + kUmmaM - 1) / kUmmaM, ncol = (N + BN - 1) / BN;
+    // about four CTAs per SM over the whole grid (the column tiles share the
+    // SMs); CTAs beyond the resident ones wait for a slot, so the number only
+    // sets how finely the tiles are dealt out
+    const int target = std::max(per_sm, 4) * ctx->sm_count;
+    const int gx = std::max(1, std::min(ntiles, (target + ncol - 1) / ncol));
+    umma_dyn_kernel<BN, LA, LB, EPI><<<dim3(gx, ncol), 128, umma_smem_bytes<BN>(), ctx->stream>>>(
         Mmax, mcount, mmul, N, K, la, lb, epi, err);
     return launch_check(ctx);
 }
