@@ -223,7 +223,7 @@ def learned_section(ctx, args):
     B = 65536
     dev = torch.device("cuda", ctx.device)
     Xb = X[:B].contiguous()
-    O = torch.empty(B, engine.NET_OUT, device=dev)
+    O = torch.empty(B, net.out_row, device=dev)
     torch.cuda.synchronize()
     net.forward(Xb, O)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

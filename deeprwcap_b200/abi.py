@@ -41,7 +41,8 @@ EXPORTS = [
     "drwc_first_hop_batch", "drwc_job_params_default", "drwc_frw_run", "drwc_frw_walks",
     "drwc_job_create", "drwc_job_destroy", "drwc_job_walks_device", "drwc_job_h2d_bytes",
     "drwc_fdm_solve_noalloc", "drwc_gemm_bf16",
-    "drwc_net_create", "drwc_net_destroy", "drwc_net_param_count", "drwc_net_get_params",
+    "drwc_net_create", "drwc_net_destroy", "drwc_net_dims", "drwc_net_param_count",
+    "drwc_net_get_params",
     "drwc_net_set_params", "drwc_net_gradients", "drwc_net_forward", "drwc_net_train_step",
     "drwc_frw_harvest", "drwc_records_voxelise", "drwc_cubes_random", "drwc_learned_opts_default",
     "drwc_frw_walks_learned",
@@ -188,15 +189,17 @@ def load():
                                       C.c_float, C.c_float, C.c_int, vp]
     L.drwc_frw_harvest.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams), i64, i64,
                                    i32, vp, vp, C.POINTER(i32)]
-    L.drwc_records_voxelise.argtypes = [vp, C.POINTER(Structure), C.c_int, vp, vp, vp, vp]
-    L.drwc_cubes_random.argtypes = [vp, C.c_int, C.c_uint64, C.c_float, vp, vp]
+    L.drwc_records_voxelise.argtypes = [vp, C.POINTER(Structure), C.c_int, C.c_int, vp, vp, vp, vp]
+    L.drwc_cubes_random.argtypes = [vp, C.c_int, C.c_int, C.c_uint64, C.c_float, vp, vp]
+    L.drwc_net_dims.argtypes = [vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32),
+                                C.POINTER(i32), C.POINTER(i32)]
     L.drwc_learned_opts_default.argtypes = [C.POINTER(LearnedOpts)]
     L.drwc_learned_opts_default.restype = None
     L.drwc_frw_walks_learned.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams), vp,
                                          C.POINTER(LearnedOpts), i64, i64, vp, vp, vp, vp]
     L.drwc_server_opts_default.argtypes = [C.POINTER(ServerOpts)]
     L.drwc_server_opts_default.restype = None
-    L.drwc_server_create.argtypes = [vp, C.POINTER(ServerOpts), vp, C.POINTER(vp)]
+    L.drwc_server_create.argtypes = [vp, C.POINTER(ServerOpts), C.POINTER(vp), i32, C.POINTER(vp)]
     L.drwc_server_destroy.argtypes = [vp]
     L.drwc_server_submit.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams),
                                      C.POINTER(i64)]

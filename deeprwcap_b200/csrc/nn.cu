@@ -1,17 +1,21 @@
 // Learned transition kernels: a small 3-D convolutional network on a cube's
-// N^3 permittivity (N = 16), with BF16 operands and FP32 accumulation on the
+// N^3 permittivity (N = 16, 21 or 23), with BF16 operands and FP32 accumulation on the
 // tensor cores (tcgen05 GEMM tiles of umma.cuh), FP32 master weights and a
 // hand-written backward pass and AdamW update.
 //
-//   input   X  [B, 16^3]            eps / max eps of the cube, BF16
-//   conv1   1 -> 16, 3^3, stride 2, pad 1, ReLU     A1 [B*8^3, 16]
-//   conv2  16 -> 32, 3^3, stride 2, pad 1, ReLU     A2 [B*4^3, 32]
-//   conv3  32 -> 64, 3^3, stride 2, pad 1, ReLU     A3 [B*2^3, 64] = F [B, 512]
-//   heads   O = F Wd^T + bd  [B, 1552]: 1536 Poisson-kernel logits (softmax over
-//           the 6N^2 panels, ggft panel order) and 1 confidence output (the
-//           predicted log10 KL divergence to the FDM Green's function);
-//           G = F Wg^T + bg  [B, 1536]: the centre-gradient surface values
-//           along z (WVTZ), scaled; other axes rotate the cube first.
+//   input   X  [B, N^3]             eps / max eps of the cube, BF16
+//   conv1   1 -> 16, 3^3, stride 2, pad 1, ReLU     A1 [B*D2^3, 16]
+//   conv2  16 -> 32, 3^3, stride 2, pad 1, ReLU     A2 [B*D3^3, 32]
+//   conv3  32 -> 64, 3^3, stride 2, pad 1, ReLU     A3 [B*D4^3, 64] = F [B, 64*D4^3]
+//           (D_{l+1} = (D_l - 1) / 2 + 1: N = 16 -> 8, 4, 2; 21 -> 11, 6, 3;
+//           23 -> 12, 6, 3)
+//   heads   O = F Wd^T + bd  [B, DEC]: 6N^2 Poisson-kernel logits (softmax over
+//           the panels, ggft panel order) and 1 confidence output (the
+//           predicted log10 KL divergence to the FDM Green's function), DEC =
+//           6N^2 + 1 rounded up to 16 (1552 at N = 16);
+//           G = F Wg^T + bg  [B, GLD]: the 6N^2 centre-gradient surface values
+//           along z (WVTZ), scaled, rows padded to GLD = 6N^2 rounded up to
+//           16; other axes rotate the cube first.
 //
 // Layers are implicit GEMMs: rows are output positions (channels-last), K is
 // (tap, input channel) with the channel fastest, so an 8-wide K chunk of a
@@ -35,10 +39,28 @@
 
 namespace drwc {
 
-constexpr int kNetN = 16;
-constexpr int kNP = 6 * kNetN * kNetN;   // 1536 panels
-constexpr int kDecRows = kNP + 16;       // Poisson logits + confidence (+ padding)
-constexpr int kFeat = 512;
+// Layer sizes of the network for cube resolution N.
+template <int N>
+struct NetDims {
+    static constexpr int D1 = N, D2 = (D1 - 1) / 2 + 1, D3 = (D2 - 1) / 2 + 1,
+                         D4 = (D3 - 1) / 2 + 1;
+    static constexpr int P2 = D2 * D2 * D2, P3 = D3 * D3 * D3, P4 = D4 * D4 * D4;
+    static constexpr int NP = 6 * N * N;               // panels
+    static constexpr int DEC = (NP + 1 + 15) / 16 * 16; // Poisson logits + confidence, padded
+    static constexpr int GLD = (NP + 15) / 16 * 16;     // gradient-head row stride
+    static constexpr int FEAT = 64 * P4;
+};
+
+// Calls f(std::integral_constant<int, N>) for a served network resolution.
+template <class F>
+inline int net_dispatch(int N, F&& f) {
+    switch (N) {
+        case 16: return f(std::integral_constant<int, 16>{});
+        case 21: return f(std::integral_constant<int, 21>{});
+        case 23: return f(std::integral_constant<int, 23>{});
+        default: return DRWC_ERR_INVALID;
+    }
+}
 
 using bf16 = __nv_bfloat16;
 
@@ -53,7 +75,7 @@ struct ConvGather {
     static constexpr bool kChunks = C % 8 == 0;
     DRWC_DEV bool chunks_ok() const { return (reinterpret_cast<uintptr_t>(x) & 15) == 0; }
     DRWC_DEV const void* chunk(int r, int k8) const {
-        constexpr int Do = D / 2, P = Do * Do * Do, K = 27 * C;
+        constexpr int Do = (D - 1) / 2 + 1, P = Do * Do * Do, K = 27 * C;
         if (r >= rows || k8 >= K) return nullptr;
         const int b = r / P, p = r % P;
         const int pz = p / (Do * Do), py = (p / Do) % Do, px = p % Do;
@@ -63,7 +85,7 @@ struct ConvGather {
         return x + ((((int64_t)b * D + z) * D + y) * D + xx) * C + ci;
     }
     DRWC_DEV void operator()(int r, int k8, uint4* out) const {
-        constexpr int Do = D / 2, P = Do * Do * Do, K = 27 * C;
+        constexpr int Do = (D - 1) / 2 + 1, P = Do * Do * Do, K = 27 * C;
         if (r >= rows || k8 >= K) { *out = make_uint4(0, 0, 0, 0); return; }
         const int b = r / P, p = r % P;
         const int pz = p / (Do * Do), py = (p / Do) % Do, px = p % Do;
@@ -104,7 +126,7 @@ struct Im2colT {
     int nrows;  // B * Do^3 (the reduction length)
     static constexpr bool kChunks = false;
     DRWC_DEV void operator()(int kk, int r8, uint4* out) const {
-        constexpr int Do = D / 2, P = Do * Do * Do, K = 27 * C;
+        constexpr int Do = (D - 1) / 2 + 1, P = Do * Do * Do, K = 27 * C;
         __align__(16) bf16 tmp[8];
         const int tap = kk / C, ci = kk % C;
         const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
@@ -134,7 +156,7 @@ struct ConvTGather {
     int rows;                     // B * D^3
     static constexpr bool kChunks = false;
     DRWC_DEV void operator()(int r, int k8, uint4* out) const {
-        constexpr int Do = D / 2, P = Do * Do * Do, Q = D * D * D, K = 27 * CO;
+        constexpr int Do = (D - 1) / 2 + 1, P = Do * Do * Do, Q = D * D * D, K = 27 * CO;
         static_assert(CO % 8 == 0, "output channels per chunk");
         if (r >= rows || k8 >= K) { *out = make_uint4(0, 0, 0, 0); return; }
         const int b = r / Q, q = r % Q;
@@ -335,9 +357,10 @@ __global__ void colsum_bf16_kernel(const bf16* __restrict__ m, int rows, int N,
 //            c* = log10(KL + 1e-8), dO[b, 1536] = 2 wc (O - c*) / B.
 //   Gradient (when G given): dG = 2 wg (G - T) / (B * 1536).
 // loss[0..2] += CE, confidence MSE, gradient MSE (means over the batch).
-__global__ void loss_kernel(int B, const float* __restrict__ O, const float* __restrict__ T,
-                            const float* __restrict__ G, const float* __restrict__ TG, float wc,
-                            float wg, bf16* __restrict__ dO, bf16* __restrict__ dG,
+__global__ void loss_kernel(int B, int kNP, int kDecRows, int gld, const float* __restrict__ O,
+                            const float* __restrict__ T, const float* __restrict__ G,
+                            const float* __restrict__ TG, float wc, float wg,
+                            bf16* __restrict__ dO, bf16* __restrict__ dG,
                             float* __restrict__ loss, float* __restrict__ kl_out) {
     const int b = blockIdx.x;
     if (b >= B) return;
@@ -397,7 +420,7 @@ __global__ void loss_kernel(int B, const float* __restrict__ O, const float* __r
         if (kl_out) kl_out[b] = k;
     }
     if (G) {
-        const float* g = G + (int64_t)b * kNP;
+        const float* g = G + (int64_t)b * gld;
         const float* tg = TG + (int64_t)b * kNP;
         float sq = 0.f;
         for (int j = threadIdx.x; j < kNP; j += blockDim.x) {
@@ -454,8 +477,9 @@ __global__ void sumsq_kernel(const float* __restrict__ g, int64_t n, float* __re
 
 // ----------------------------------------------------------------- the net
 struct ParamLayout {
-    int64_t w1, b1, w2, b2, w3, b3, wd, bd, wg, bg, total;
-    ParamLayout() {
+    int64_t w1 = 0, b1 = 0, w2 = 0, b2 = 0, w3 = 0, b3 = 0, wd = 0, bd = 0, wg = 0, bg = 0, total = 0;
+    ParamLayout() = default;
+    ParamLayout(int kNP, int kDecRows, int kFeat) {
         int64_t o = 0;
         auto take = [&](int64_t n) { int64_t r = o; o += (n + 63) / 64 * 64; return r; };
         w1 = take(16 * 27); b1 = take(16);
@@ -473,6 +497,8 @@ using namespace drwc;
 
 struct drwc_net {
     drwc_ctx* ctx = nullptr;
+    int N = 16;                          // cube resolution
+    int np = 0, dec = 0, gld = 0, feat = 0, p2 = 0, p3 = 0, p4 = 0;  // NetDims<N>
     ParamLayout L;
     float* p = nullptr;    // FP32 master weights
     bf16* pb = nullptr;    // BF16 working copy
@@ -501,38 +527,45 @@ static int net_reserve(drwc_net* n, int B) {
     fr(n->tmpf); fr(n->O); fr(n->G);
     const int cap = std::max(B, 64);
     auto al = [&](void** q, size_t bytes) { return cudaMalloc(q, bytes) == cudaSuccess; };
-    bool ok = al((void**)&n->a1, (size_t)cap * 512 * 16 * 2) && al((void**)&n->a2, (size_t)cap * 64 * 32 * 2) &&
-              al((void**)&n->a3, (size_t)cap * 8 * 64 * 2) && al((void**)&n->dO, (size_t)cap * kDecRows * 2) &&
-              al((void**)&n->dG, (size_t)cap * kNP * 2) && al((void**)&n->dF, (size_t)cap * kFeat * 2) &&
-              al((void**)&n->dz2, (size_t)cap * 64 * 32 * 2) && al((void**)&n->dz1, (size_t)cap * 512 * 16 * 2) &&
-              al((void**)&n->tmpf, (size_t)cap * kFeat * 4 + 256) && al((void**)&n->O, (size_t)cap * kDecRows * 4) &&
-              al((void**)&n->G, (size_t)cap * kNP * 4);
+    bool ok = al((void**)&n->a1, (size_t)cap * n->p2 * 16 * 2) && al((void**)&n->a2, (size_t)cap * n->p3 * 32 * 2) &&
+              al((void**)&n->a3, (size_t)cap * n->p4 * 64 * 2) && al((void**)&n->dO, (size_t)cap * n->dec * 2) &&
+              al((void**)&n->dG, (size_t)cap * n->np * 2) && al((void**)&n->dF, (size_t)cap * n->feat * 2) &&
+              al((void**)&n->dz2, (size_t)cap * n->p3 * 32 * 2) && al((void**)&n->dz1, (size_t)cap * n->p2 * 16 * 2) &&
+              al((void**)&n->tmpf, (size_t)cap * n->feat * 4 + 256) && al((void**)&n->O, (size_t)cap * n->dec * 4) &&
+              al((void**)&n->G, (size_t)cap * n->gld * 4);
     if (!ok) { cudaGetLastError(); n->cap = 0; return DRWC_ERR_NOMEM; }
     n->cap = cap;
     return DRWC_OK;
 }
 
-// Encoder: X [B, 4096] BF16 -> A3 [B, 512] BF16.
-static int net_encode(drwc_net* n, int B, const bf16* X) {
+// Encoder: X [B, N^3] BF16 -> A3 [B, FEAT] BF16.
+template <int N>
+static int net_encode_t(drwc_net* n, int B, const bf16* X) {
+    using S = NetDims<N>;
     drwc_ctx* ctx = n->ctx;
     const bf16* pb = n->pb;
     int rc;
-    rc = launch_umma<16>(ctx, B * 512, 16, 27, ConvGather<16, 1>{X, B * 512},
+    rc = launch_umma<16>(ctx, B * S::P2, 16, 27, ConvGather<S::D1, 1>{X, B * S::P2},
                          RowsBf16{pb + n->L.w1, 16, 27, 27, nullptr},
                          EpiReluBf16{n->a1, n->p + n->L.b1, 16}, n->err);
     if (rc) return rc;
-    rc = launch_umma<32>(ctx, B * 64, 32, 27 * 16, ConvGather<8, 16>{n->a1, B * 64},
+    rc = launch_umma<32>(ctx, B * S::P3, 32, 27 * 16, ConvGather<S::D2, 16>{n->a1, B * S::P3},
                          RowsBf16{pb + n->L.w2, 32, 27 * 16, 27 * 16, nullptr},
                          EpiReluBf16{n->a2, n->p + n->L.b2, 32}, n->err);
     if (rc) return rc;
-    return launch_umma<64>(ctx, B * 8, 64, 27 * 32, ConvGather<4, 32>{n->a2, B * 8},
+    return launch_umma<64>(ctx, B * S::P4, 64, 27 * 32, ConvGather<S::D3, 32>{n->a2, B * S::P4},
                            RowsBf16{pb + n->L.w3, 64, 27 * 32, 27 * 32, nullptr},
                            EpiReluBf16{n->a3, n->p + n->L.b3, 64}, n->err);
+}
+
+static int net_encode(drwc_net* n, int B, const bf16* X) {
+    return net_dispatch(n->N, [&](auto nc) { return net_encode_t<decltype(nc)::value>(n, B, X); });
 }
 
 static int net_heads(drwc_net* n, int rows, const int* rowmap, float* O, float* G,
                      const int* rowmap_g, int rows_g) {
     drwc_ctx* ctx = n->ctx;
+    const int kNP = n->np, kDecRows = n->dec, kFeat = n->feat;
     int rc = DRWC_OK;
     if (O) {
         rc = launch_umma<128>(ctx, rows, kDecRows, kFeat,
@@ -545,7 +578,7 @@ static int net_heads(drwc_net* n, int rows, const int* rowmap, float* O, float* 
         rc = launch_umma<128>(ctx, rows_g, kNP, kFeat,
                               RowsBf16{n->a3, rows_g, kFeat, kFeat, rowmap_g},
                               RowsBf16{n->pb + n->L.wg, kNP, kFeat, kFeat, nullptr},
-                              EpiF32{G, n->p + n->L.bg, kNP, kNP, nullptr}, n->err);
+                              EpiF32{G, n->p + n->L.bg, kNP, n->gld, nullptr}, n->err);
     }
     return rc;
 }
@@ -567,36 +600,47 @@ int net_forward_mapped(drwc_net* n, int B, const bf16* X, float* O, float* G, co
     return net_heads(n, B, nullptr, O, G, gmap, rows_g);
 }
 
-int net_forward_dyn(drwc_net* n, int Bmax, const unsigned* nrows, const bf16* X, float* O,
-                    float* G, const int* gmap, const unsigned* nrows_g) {
-    if (Bmax > n->cap) return DRWC_ERR_INVALID;  // reserve first (not during capture)
+template <int N>
+static int net_forward_dyn_t(drwc_net* n, int Bmax, const unsigned* nrows, const bf16* X,
+                             float* O, float* G, const int* gmap, const unsigned* nrows_g) {
+    using S = NetDims<N>;
     drwc_ctx* ctx = n->ctx;
     const bf16* pb = n->pb;
     int rc = DRWC_OK;
     if (X) {  // else conv1's activations are already in a1 (net_conv1_operands)
-        rc = launch_umma_dyn<16>(ctx, Bmax * 512, nrows, 512, 16, 27,
-                                 ConvGather<16, 1>{X, Bmax * 512},
+        rc = launch_umma_dyn<16>(ctx, Bmax * S::P2, nrows, S::P2, 16, 27,
+                                 ConvGather<S::D1, 1>{X, Bmax * S::P2},
                                  RowsBf16{pb + n->L.w1, 16, 27, 27, nullptr},
                                  EpiReluBf16{n->a1, n->p + n->L.b1, 16}, n->err);
         if (rc) return rc;
     }
-    rc = launch_umma_dyn<32>(ctx, Bmax * 64, nrows, 64, 32, 27 * 16, ConvGather<8, 16>{n->a1, Bmax * 64},
+    rc = launch_umma_dyn<32>(ctx, Bmax * S::P3, nrows, S::P3, 32, 27 * 16,
+                             ConvGather<S::D2, 16>{n->a1, Bmax * S::P3},
                              RowsBf16{pb + n->L.w2, 32, 27 * 16, 27 * 16, nullptr},
                              EpiReluBf16{n->a2, n->p + n->L.b2, 32}, n->err);
     if (rc) return rc;
-    rc = launch_umma_dyn<64>(ctx, Bmax * 8, nrows, 8, 64, 27 * 32, ConvGather<4, 32>{n->a2, Bmax * 8},
+    rc = launch_umma_dyn<64>(ctx, Bmax * S::P4, nrows, S::P4, 64, 27 * 32,
+                             ConvGather<S::D3, 32>{n->a2, Bmax * S::P4},
                              RowsBf16{pb + n->L.w3, 64, 27 * 32, 27 * 32, nullptr},
                              EpiReluBf16{n->a3, n->p + n->L.b3, 64}, n->err);
     if (rc) return rc;
-    rc = launch_umma_dyn<128>(ctx, Bmax, nrows, 1, kDecRows, kFeat,
-                              RowsBf16{n->a3, Bmax, kFeat, kFeat, nullptr},
-                              RowsBf16{n->pb + n->L.wd, kDecRows, kFeat, kFeat, nullptr},
-                              EpiF32{O, n->p + n->L.bd, kDecRows, kDecRows, nullptr}, n->err);
+    rc = launch_umma_dyn<128>(ctx, Bmax, nrows, 1, S::DEC, S::FEAT,
+                              RowsBf16{n->a3, Bmax, S::FEAT, S::FEAT, nullptr},
+                              RowsBf16{n->pb + n->L.wd, S::DEC, S::FEAT, S::FEAT, nullptr},
+                              EpiF32{O, n->p + n->L.bd, S::DEC, S::DEC, nullptr}, n->err);
     if (rc) return rc;
-    return launch_umma_dyn<128>(ctx, Bmax, nrows_g, 1, kNP, kFeat,
-                                RowsBf16{n->a3, Bmax, kFeat, kFeat, gmap},
-                                RowsBf16{n->pb + n->L.wg, kNP, kFeat, kFeat, nullptr},
-                                EpiF32{G, n->p + n->L.bg, kNP, kNP, nullptr}, n->err);
+    return launch_umma_dyn<128>(ctx, Bmax, nrows_g, 1, S::NP, S::FEAT,
+                                RowsBf16{n->a3, Bmax, S::FEAT, S::FEAT, gmap},
+                                RowsBf16{n->pb + n->L.wg, S::NP, S::FEAT, S::FEAT, nullptr},
+                                EpiF32{G, n->p + n->L.bg, S::NP, S::GLD, nullptr}, n->err);
+}
+
+int net_forward_dyn(drwc_net* n, int Bmax, const unsigned* nrows, const bf16* X, float* O,
+                    float* G, const int* gmap, const unsigned* nrows_g) {
+    if (Bmax > n->cap) return DRWC_ERR_INVALID;  // reserve first (not during capture)
+    return net_dispatch(n->N, [&](auto nc) {
+        return net_forward_dyn_t<decltype(nc)::value>(n, Bmax, nrows, X, O, G, gmap, nrows_g);
+    });
 }
 
 int net_reserve_rows(drwc_net* n, int B) { return net_reserve(n, B); }
@@ -609,17 +653,28 @@ void net_hold(drwc_net* n, int delta) { n->holders += delta; }
 
 drwc_ctx* net_context(drwc_net* n) { return n->ctx; }
 
+int net_size(drwc_net* n) { return n->N; }
+
 }  // namespace drwc
 
 extern "C" {
 
 DRWC_API int drwc_net_create(drwc_ctx* ctx, int N, uint64_t seed, drwc_net** out) {
-    if (!ctx || !out || N != kNetN) return DRWC_ERR_INVALID;
+    if (!ctx || !out || (N != 16 && N != 21 && N != 23)) return DRWC_ERR_INVALID;
     *out = nullptr;
     std::lock_guard<std::mutex> lock(ctx->mu);
     DRWC_CUDA_TRY(cudaSetDevice(ctx->device));
     drwc_net* n = new drwc_net();
     n->ctx = ctx;
+    n->N = N;
+    net_dispatch(N, [&](auto nc) {
+        using S = NetDims<decltype(nc)::value>;
+        n->np = S::NP; n->dec = S::DEC; n->gld = S::GLD; n->feat = S::FEAT;
+        n->p2 = S::P2; n->p3 = S::P3; n->p4 = S::P4;
+        return DRWC_OK;
+    });
+    n->L = ParamLayout(n->np, n->dec, n->feat);
+    const int kNP = n->np, kFeat = n->feat;
     const int64_t T = n->L.total;
     bool ok = cudaMalloc(&n->p, T * 4) == cudaSuccess && cudaMalloc(&n->pb, T * 2) == cudaSuccess &&
               cudaMalloc(&n->g, T * 4) == cudaSuccess && cudaMalloc(&n->m, T * 4) == cudaSuccess &&
@@ -661,6 +716,17 @@ DRWC_API int drwc_net_destroy(drwc_net* n) {
     return DRWC_OK;
 }
 
+DRWC_API int drwc_net_dims(drwc_net* n, int32_t* N, int32_t* panels, int32_t* out_row,
+                           int32_t* grad_row, int32_t* features) {
+    if (!n) return DRWC_ERR_INVALID;
+    if (N) *N = n->N;
+    if (panels) *panels = n->np;
+    if (out_row) *out_row = n->dec;
+    if (grad_row) *grad_row = n->gld;
+    if (features) *features = n->feat;
+    return DRWC_OK;
+}
+
 DRWC_API int drwc_net_param_count(drwc_net* n, int64_t* count) {
     if (!n || !count) return DRWC_ERR_INVALID;
     *count = n->L.total;
@@ -696,8 +762,8 @@ DRWC_API int drwc_net_gradients(drwc_net* n, float* host) {
     return DRWC_OK;
 }
 
-// Forward: X [B, 4096] BF16 (device) -> O [B, 1552] FP32 (Poisson logits +
-// confidence) and, when G is set, G [B, 1536] FP32 (gradient head).
+// Forward: X [B, N^3] BF16 (device) -> O [B, out_row] FP32 (Poisson logits +
+// confidence) and, when G is set, G [B, grad_row] FP32 (gradient head).
 DRWC_API int drwc_net_forward(drwc_net* n, int B, const void* X, float* O, float* G) {
     if (!n || B < 0 || (B > 0 && !X)) return DRWC_ERR_INVALID;
     if (B == 0) return DRWC_OK;
@@ -722,6 +788,7 @@ DRWC_API int drwc_net_train_step(drwc_net* n, int B, const void* X, const float*
     if (rc) return rc;
     const bf16* x = (const bf16*)X;
     const ParamLayout& L = n->L;
+    const int kNP = n->np, kDecRows = n->dec, kFeat = n->feat;
     // ---- forward
     rc = net_encode(n, B, x);
     if (rc) return rc;
@@ -730,9 +797,13 @@ DRWC_API int drwc_net_train_step(drwc_net* n, int B, const void* X, const float*
     float* loss = n->tmpf + (size_t)n->cap * kFeat;  // 3 floats + norm
     DRWC_CUDA_TRY(cudaMemsetAsync(loss, 0, 64, ctx->stream));
     DRWC_CUDA_TRY(cudaMemsetAsync(n->g, 0, L.total * 4, ctx->stream));
-    loss_kernel<<<B, 256, 0, ctx->stream>>>(B, n->O, T, TG ? n->G : nullptr, TG, w_conf, w_grad,
-                                             n->dO, n->dG, loss, nullptr);
+    loss_kernel<<<B, 256, 0, ctx->stream>>>(B, kNP, kDecRows, n->gld, n->O, T,
+                                             TG ? n->G : nullptr, TG, w_conf, w_grad, n->dO, n->dG,
+                                             loss, nullptr);
     if ((rc = launch_check(ctx))) return rc;
+    rc = net_dispatch(n->N, [&](auto nc) -> int {
+    using S = NetDims<decltype(nc)::value>;
+    int rc = DRWC_OK;
     // ---- heads: weight / bias gradients, dF
     const int spl = std::max(1, std::min(64, B / 64));
     rc = launch_splitk<128>(ctx, kDecRows, kFeat, B, spl, ColsBf16{n->dO, kDecRows, B, kDecRows},
@@ -768,34 +839,36 @@ DRWC_API int drwc_net_train_step(drwc_net* n, int B, const void* X, const float*
     if ((rc = launch_check(ctx))) return rc;
     const bf16* dz3 = n->dF;  // [B*8, 64]
     // ---- conv3: dW3, db3, dZ2
-    const int r3 = B * 8, r2 = B * 64, r1 = B * 512;
+    const int r3 = B * S::P4, r2 = B * S::P3, r1 = B * S::P2;
     rc = launch_splitk<128>(ctx, 64, 27 * 32, r3, std::max(1, std::min(128, r3 / 256)),
-                            ColsBf16{dz3, 64, r3, 64}, Im2colT<4, 32>{n->a2, r3},
+                            ColsBf16{dz3, 64, r3, 64}, Im2colT<S::D3, 32>{n->a2, r3},
                             EpiAtomicF32{n->g + L.w3, 27 * 32}, n->err);
     if (rc) return rc;
     colsum_bf16_kernel<<<dim3(1, (r3 + 255) / 256), 64, 0, ctx->stream>>>(dz3, r3, 64, n->g + L.b3);
     if ((rc = launch_check(ctx))) return rc;
-    rc = launch_umma<32>(ctx, r2, 32, 27 * 64, ConvTGather<4, 64>{dz3, r2},
+    rc = launch_umma<32>(ctx, r2, 32, 27 * 64, ConvTGather<S::D3, 64>{dz3, r2},
                          WeightT<32, 64>{n->pb + L.w3}, EpiReluGrad{n->dz2, n->a2, 32}, n->err);
     if (rc) return rc;
     // ---- conv2: dW2, db2, dZ1
     rc = launch_splitk<32>(ctx, 32, 27 * 16, r2, std::max(1, std::min(256, r2 / 512)),
-                           ColsBf16{n->dz2, 32, r2, 32}, Im2colT<8, 16>{n->a1, r2},
+                           ColsBf16{n->dz2, 32, r2, 32}, Im2colT<S::D2, 16>{n->a1, r2},
                            EpiAtomicF32{n->g + L.w2, 27 * 16}, n->err);
     // note: M = 32 output channels -> a 128-row tile with 96 zero rows
     if (rc) return rc;
     colsum_bf16_kernel<<<dim3(1, (r2 + 255) / 256), 32, 0, ctx->stream>>>(n->dz2, r2, 32, n->g + L.b2);
     if ((rc = launch_check(ctx))) return rc;
-    rc = launch_umma<16>(ctx, r1, 16, 27 * 32, ConvTGather<8, 32>{n->dz2, r1},
+    rc = launch_umma<16>(ctx, r1, 16, 27 * 32, ConvTGather<S::D2, 32>{n->dz2, r1},
                          WeightT<16, 32>{n->pb + L.w2}, EpiReluGrad{n->dz1, n->a1, 16}, n->err);
     if (rc) return rc;
     // ---- conv1: dW1, db1
     rc = launch_splitk<32>(ctx, 16, 27, r1, std::max(1, std::min(512, r1 / 1024)),
-                           ColsBf16{n->dz1, 16, r1, 16}, Im2colT<16, 1>{x, r1},
+                           ColsBf16{n->dz1, 16, r1, 16}, Im2colT<S::D1, 1>{x, r1},
                            EpiAtomicF32{n->g + L.w1, 27}, n->err);
     if (rc) return rc;
     colsum_bf16_kernel<<<dim3(1, (r1 + 255) / 256), 32, 0, ctx->stream>>>(n->dz1, r1, 16, n->g + L.b1);
-    if ((rc = launch_check(ctx))) return rc;
+    return launch_check(ctx);
+    });
+    if (rc) return rc;
     // ---- clip + AdamW
     float host_loss[4] = {0, 0, 0, 0};
     sumsq_kernel<<<512, 256, 0, ctx->stream>>>(n->g, L.total, loss + 3);

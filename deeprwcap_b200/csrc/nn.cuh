@@ -35,6 +35,7 @@ int net_reserve_rows(drwc_net* n, int B);
 // ones fail with DRWC_ERR_INVALID until every holder lets go.
 void net_hold(drwc_net* n, int delta);
 drwc_ctx* net_context(drwc_net* n);
+int net_size(drwc_net* n);  // cube resolution N of the network
 
 // conv1 operands: BF16 weights [16][27] (tap = dz*9 + dy*3 + dx), FP32 bias,
 // and the activation buffer a1 [rows * 512][16] (channels last).
@@ -45,17 +46,19 @@ struct NetConv1 {
 };
 NetConv1 net_conv1_operands(drwc_net* n);
 
-// conv1 of one 16^3 cube on the CUDA cores, CTA-wide: x (shared, BF16 eps /
+// conv1 of one D^3 cube on the CUDA cores, CTA-wide: x (shared, BF16 eps /
 // max eps), w4 (shared, FP32 copies of the BF16 weights, tap-major: w4[tap *
 // 4 + g] holds output channels 4g..4g+3 of that tap), b (shared, bias) ->
-// a1 rows [512][16] BF16 = ReLU(b + sum over taps of w * x), zero padding,
-// stride 2. The operands are the BF16 values the tensor-core layer reads and
-// every product is exact in FP32; only the FP32 summation order differs.
-// With one input channel its GEMM has K = 27, too thin for the tensor cores,
-// while 221K FMAs per cube run next to the voxelisation that produced x.
+// a1 rows [Do^3][16] BF16 = ReLU(b + sum over taps of w * x), zero padding,
+// stride 2 (Do = (D - 1) / 2 + 1). The operands are the BF16 values the
+// tensor-core layer reads and every product is exact in FP32; only the FP32
+// summation order differs. With one input channel its GEMM has K = 27, too
+// thin for the tensor cores, while the FMAs run next to the voxelisation
+// that produced x.
+template <int D>
 DRWC_DEV_INLINE void conv1_cube(const __nv_bfloat16* x, const float4* w4, const float* b,
                                 __nv_bfloat16* __restrict__ a1) {
-    constexpr int D = 16, Do = 8, P = Do * Do * Do;
+    constexpr int Do = (D - 1) / 2 + 1, P = Do * Do * Do;
     for (int p = threadIdx.x; p < P; p += blockDim.x) {
         const int pz = p / (Do * Do), py = (p / Do) % Do, px = p % Do;
         float acc[16];
@@ -86,5 +89,6 @@ DRWC_DEV_INLINE void conv1_cube(const __nv_bfloat16* x, const float4* w4, const 
         dst[1] = reinterpret_cast<const uint4*>(out)[1];
     }
 }
+
 
 }  // namespace drwc

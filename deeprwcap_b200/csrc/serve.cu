@@ -45,8 +45,6 @@
 namespace drwc {
 
 constexpr int kSvMaxJobs = 64;
-constexpr int kSvNetN = DRWC_NET_N;
-constexpr int kSvDecRows = DRWC_NET_OUT;
 constexpr int kSvMaxSteps = 8;
 constexpr int kSvPrepIters = 64;  // prepare-loop passes per slot and step
 constexpr int kSvWin = 8;         // record slots per job: batches of walk ids in flight
@@ -104,15 +102,18 @@ struct SvArgs {
     SvSlots st;
     int* blist[DRWC_SERVER_MAX_SIZES];
     int* bkind[DRWC_SERVER_MAX_SIZES];  // bit 0 audit, bits 1.. network row
-    unsigned* cnt;                      // [0] network rows, [1] first-hop rows, [2 + b] rows of
-                                        // bucket b, [2 + MAX_SIZES + b] its next unclaimed row
+    // per bucket b: cnt[4b] network rows, [4b + 1] first-hop rows, [4b + 2] FDM
+    // rows, [4b + 3] the next unclaimed FDM row
+    unsigned* cnt;
     float conf_thresh, audit_frac;
-    __nv_bfloat16* X;
-    float* O;
-    float* Gh;
-    NetConv1 c1;                        // conv1 runs inside the voxeliser
-    int* alist;
-    int* frow;
+    // network of bucket b (when it has one): rows, outputs, conv1 operands
+    int* alist[DRWC_SERVER_MAX_SIZES];
+    int* frow[DRWC_SERVER_MAX_SIZES];
+    float* O[DRWC_SERVER_MAX_SIZES];
+    float* Gh[DRWC_SERVER_MAX_SIZES];
+    int out_row[DRWC_SERVER_MAX_SIZES];
+    int grad_row[DRWC_SERVER_MAX_SIZES];
+    NetConv1 c1[DRWC_SERVER_MAX_SIZES];  // conv1 runs inside the voxeliser
     unsigned long long* stats;
     double* audit_kl;                   // [0] sum, [1] count
     double* bsum;
@@ -258,7 +259,7 @@ DRWC_DEV void sv_table_hop(const SvArgs& A, int slot, const SvJob& J, int m) {
 }
 
 __global__ void sv_reset_kernel(SvArgs A) {
-    if (threadIdx.x < 2 + 2 * DRWC_SERVER_MAX_SIZES) A.cnt[threadIdx.x] = 0;
+    if (threadIdx.x < 4 * DRWC_SERVER_MAX_SIZES) A.cnt[threadIdx.x] = 0;
 }
 
 // One warp per slot.
@@ -320,17 +321,17 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
     }
     if (lane == 0 && act) {
         const SvJob& J = A.jobs[A.st.job[slot]];
+        const int b = J.bucket;
         if (J.use_net) {
-            const unsigned idx = atomicAdd(&A.cnt[0], 1u);
-            A.alist[idx] = slot;
+            const unsigned idx = atomicAdd(&A.cnt[4 * b], 1u);
+            A.alist[b][idx] = slot;
             if (A.st.hops[slot] == 0) {
-                const unsigned f = atomicAdd(&A.cnt[1], 1u);
-                A.frow[f] = (int)idx;
+                const unsigned f = atomicAdd(&A.cnt[4 * b + 1], 1u);
+                A.frow[b][f] = (int)idx;
                 A.st.grow[slot] = (int)f;
             }
         } else {
-            const int b = J.bucket;
-            const unsigned idx = atomicAdd(&A.cnt[2 + b], 1u);
+            const unsigned idx = atomicAdd(&A.cnt[4 * b + 2], 1u);
             A.blist[b][idx] = slot;
             A.bkind[b][idx] = 0;
         }
@@ -340,8 +341,9 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
 // One CTA (256 threads) per network row: the cube voxelised in shared
 // memory (eps / max eps, BF16) and the network's first layer applied to it,
 // so only conv1's activations reach global memory.
-__global__ void __launch_bounds__(256, 3) sv_voxelise_kernel(SvArgs A) {
-    constexpr int N = kSvNetN;
+template <int N>
+__global__ void __launch_bounds__(256, 4) sv_voxelise_kernel(SvArgs A, int bucket) {
+    constexpr int Do = (N - 1) / 2 + 1;
     __shared__ double tco[N];
     __shared__ double pal[kMaxMaterials];
     __shared__ uint8_t mat[N * N * N];
@@ -354,13 +356,13 @@ __global__ void __launch_bounds__(256, 3) sv_voxelise_kernel(SvArgs A) {
     // weights [co][tap] -> tap-major float4 groups of 4 output channels
     for (int q = threadIdx.x; q < 16 * 27; q += blockDim.x) {
         const int co = q / 27, tap = q % 27;
-        reinterpret_cast<float*>(w4)[tap * 16 + co] = __bfloat162float(A.c1.w1[q]);
+        reinterpret_cast<float*>(w4)[tap * 16 + co] = __bfloat162float(A.c1[bucket].w1[q]);
     }
-    if (threadIdx.x < 16) b1[threadIdx.x] = A.c1.b1[threadIdx.x];
-    const int na = (int)A.cnt[0];
+    if (threadIdx.x < 16) b1[threadIdx.x] = A.c1[bucket].b1[threadIdx.x];
+    const int na = (int)A.cnt[4 * bucket];
     int loaded = -1;
     for (int row = blockIdx.x; row < na; row += gridDim.x) {
-        const int slot = A.alist[row];
+        const int slot = A.alist[bucket][row];
         const int j = A.st.job[slot];
         const SvJob& J = A.jobs[j];
         if (j != loaded) {
@@ -377,7 +379,7 @@ __global__ void __launch_bounds__(256, 3) sv_voxelise_kernel(SvArgs A) {
             const EpsPalette E{mat, pal, nullptr, nullptr, nullptr, 0};
             A.st.epsw[slot] = center_diel<N>(E, DRWC_WVTZ);
         }
-        conv1_cube(xs, w4, b1, A.c1.a1 + (size_t)row * 512 * 16);
+        conv1_cube<N>(xs, w4, b1, A.c1[bucket].a1 + (size_t)row * (Do * Do * Do) * 16);
         __syncthreads();
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.stats + SV_NET_ROWS, (unsigned long long)na);
@@ -385,30 +387,33 @@ __global__ void __launch_bounds__(256, 3) sv_voxelise_kernel(SvArgs A) {
 
 // One CTA (256 threads) per network row: draw from the prediction, or route
 // the hop to the FDM bucket of its job.
-__global__ void __launch_bounds__(256) sv_sample_kernel(SvArgs A) {
-    constexpr int N = kSvNetN, M = 6 * N * N, NT = 256;
+template <int N>
+__global__ void __launch_bounds__(256) sv_sample_kernel(SvArgs A, int bucket) {
+    constexpr int M = 6 * N * N, NT = 256;
+    const int ldo = A.out_row[bucket], ldg = A.grad_row[bucket];
+    const float* __restrict__ Ob = A.O[bucket];
+    const float* __restrict__ Gb = A.Gh[bucket];
     __shared__ double wv[M];
     __shared__ double red[2 * (NT / 32) + 16];
     __shared__ int route;
-    const int na = (int)A.cnt[0];
+    const int na = (int)A.cnt[4 * bucket];
     unsigned long long my_net = 0;
     for (int row = blockIdx.x; row < na; row += gridDim.x) {
-        const int slot = A.alist[row];
+        const int slot = A.alist[bucket][row];
         const SvJob& J = A.jobs[A.st.job[slot]];
         const long long w = A.st.walk[slot];
         const int h = A.st.hops[slot];
         const bool first = h == 0;
         if (threadIdx.x == 0) {
-            const float conf = A.O[(size_t)row * kSvDecRows + M];
+            const float conf = Ob[(size_t)row * ldo + M];
             const bool audit =
                 philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 2).x < (double)A.audit_frac;
             const bool fallback = conf > A.conf_thresh;
             route = 0;
             if (audit || fallback) {
-                const int b = J.bucket;
-                const unsigned idx = atomicAdd(&A.cnt[2 + b], 1u);
-                A.blist[b][idx] = slot;
-                A.bkind[b][idx] = (audit ? 1 : 0) | (row << 1);
+                const unsigned idx = atomicAdd(&A.cnt[4 * bucket + 2], 1u);
+                A.blist[bucket][idx] = slot;
+                A.bkind[bucket][idx] = (audit ? 1 : 0) | (row << 1);
                 route = 1;
                 atomicAdd(A.stats + (audit ? SV_AUDITS : SV_FALLBACKS), 1ull);
             }
@@ -418,13 +423,13 @@ __global__ void __launch_bounds__(256) sv_sample_kernel(SvArgs A) {
         double tot = 0.0;
         int b;
         if (first) {
-            const float* g = A.Gh + (size_t)A.st.grow[slot] * M;
+            const float* g = Gb + (size_t)A.st.grow[slot] * ldg;
             for (int q = threadIdx.x; q < M; q += NT) wv[q] = (double)g[q] / (double)kGradScale;
             __syncthreads();
             const double u = philox_uniform2(J.W.seed, (uint64_t)w, 0, 1).y;
             b = cta_sample<NT>(wv, M, true, u, red, &tot);
         } else {
-            const float* o = A.O + (size_t)row * kSvDecRows;
+            const float* o = Ob + (size_t)row * ldo;
             float mx = -1e30f;
             for (int q = threadIdx.x; q < M; q += NT) mx = fmaxf(mx, o[q]);
             for (int s = 16; s > 0; s >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, s));
@@ -489,8 +494,8 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
     centre_offsets<N>(tco);
     double* ys = scratch_y + (size_t)blockIdx.x * D::NNN;
     float* ss = scratch_s + (size_t)blockIdx.x * D::NNN;
-    const unsigned count = A.cnt[2 + bucket];
-    unsigned* next_item = A.cnt + 2 + DRWC_SERVER_MAX_SIZES + bucket;
+    const unsigned count = A.cnt[4 * bucket + 2];
+    unsigned* next_item = A.cnt + 4 * bucket + 3;
     __shared__ unsigned s_idx;
     int loaded = -1, P = 0;
     unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0;
@@ -534,7 +539,7 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
         __syncthreads();
         if ((kind & 1) && !first) {
             // audit: KL(FDM || network) over the panels
-            const float* o = A.O + (size_t)(kind >> 1) * kSvDecRows;
+            const float* o = A.O[bucket] + (size_t)(kind >> 1) * A.out_row[bucket];
             const double ls = block_lse<D::NW>(o, M, sm.red);
             __syncthreads();
             double kl = 0.0;
@@ -696,10 +701,10 @@ using namespace drwc;
 
 struct drwc_server {
     drwc_ctx* ctx = nullptr;
-    drwc_net* net = nullptr;
+    drwc_net* bnet[DRWC_SERVER_MAX_SIZES] = {};  // network of each bucket, if any
+    bool any_net = false;
     drwc_server_opts o{};
     int bucket_of_N[DRWC_N_MAX + 1];
-    int net_bucket = -1;
     // device
     void* dblock = nullptr;
     void* arena_dev = nullptr;
@@ -823,6 +828,10 @@ static int sv_mark(drwc_server* v, cudaEvent_t e, cudaStream_t s) {
 }
 
 // One step on the context stream (captured into the graph).
+// One step on the context stream (captured into the graph). FDM buckets
+// without a network fork onto their own branches right after prepare; the
+// network stages run on the main stream, bucket after bucket, and each such
+// bucket's FDM hops (fallbacks and audits) fork once its sampler has routed.
 static int sv_step(drwc_server* v, int k) {
     drwc_ctx* ctx = v->ctx;
     cudaStream_t s = ctx->stream;
@@ -832,35 +841,43 @@ static int sv_step(drwc_server* v, int k) {
     if ((rc = launch_check(ctx))) return rc;
     sv_prepare_kernel<<<(A.S * 32 + 255) / 256, 256, 0, s>>>(A);
     if ((rc = launch_check(ctx))) return rc;
-    DRWC_CUDA_TRY(cudaEventRecord(v->ev_fork, s));
-    // buckets that do not wait for the network fork now
-    for (int b = 0; b < v->o.n_sizes; ++b) {
-        if (b == v->net_bucket) continue;
+    auto fork_fdm = [&](int b) -> int {
+        DRWC_CUDA_TRY(cudaEventRecord(v->ev_fork, s));
         DRWC_CUDA_TRY(cudaStreamWaitEvent(v->side[b], v->ev_fork, 0));
-        if ((rc = sv_mark(v, v->ev_t[k][2 + 2 * b], v->side[b]))) return rc;
-        if ((rc = sv_fdm_launch(v, b, v->side[b]))) return rc;
-        if ((rc = sv_mark(v, v->ev_t[k][3 + 2 * b], v->side[b]))) return rc;
+        int r = sv_mark(v, v->ev_t[k][2 + 2 * b], v->side[b]);
+        if (!r) r = sv_fdm_launch(v, b, v->side[b]);
+        if (!r) r = sv_mark(v, v->ev_t[k][3 + 2 * b], v->side[b]);
+        if (r) return r;
         DRWC_CUDA_TRY(cudaEventRecord(v->ev_join[b], v->side[b]));
-    }
-    if (v->net) {
-        const int g2 = std::min(A.S, ctx->sm_count * 16);
-        if ((rc = sv_mark(v, v->ev_t[k][0], s))) return rc;
-        sv_voxelise_kernel<<<g2, 256, 0, s>>>(A);
-        if ((rc = launch_check(ctx))) return rc;
-        rc = net_forward_dyn(v->net, A.S, A.cnt, nullptr, A.O, A.Gh, A.frow, A.cnt + 1);
-        if (rc) return rc;
-        if ((rc = sv_mark(v, v->ev_t[k][1], s))) return rc;
-        sv_sample_kernel<<<g2, 256, 0, s>>>(A);
-        if ((rc = launch_check(ctx))) return rc;
-        const int b = v->net_bucket;
-        if ((rc = sv_mark(v, v->ev_t[k][2 + 2 * b], s))) return rc;
-        if ((rc = sv_fdm_launch(v, b, s))) return rc;
-        if ((rc = sv_mark(v, v->ev_t[k][3 + 2 * b], s))) return rc;
-    }
+        return DRWC_OK;
+    };
+    for (int b = 0; b < v->o.n_sizes; ++b)
+        if (!v->bnet[b] && (rc = fork_fdm(b))) return rc;
+    if (v->any_net && (rc = sv_mark(v, v->ev_t[k][0], s))) return rc;
     for (int b = 0; b < v->o.n_sizes; ++b) {
-        if (b == v->net_bucket) continue;
-        DRWC_CUDA_TRY(cudaStreamWaitEvent(s, v->ev_join[b], 0));
+        if (!v->bnet[b]) continue;
+        const int g2 = std::min(A.S, ctx->sm_count * 16);
+        rc = dispatch_N(v->o.sizes[b], [&](auto nc) -> int {
+            constexpr int NC = decltype(nc)::value;
+            if constexpr (NC == 16 || NC == 21 || NC == 23) {
+                sv_voxelise_kernel<NC><<<g2, 256, 0, s>>>(A, b);
+                int r = launch_check(ctx);
+                if (r) return r;
+                r = net_forward_dyn(v->bnet[b], A.S, A.cnt + 4 * b, nullptr, A.O[b], A.Gh[b],
+                                    A.frow[b], A.cnt + 4 * b + 1);
+                if (r) return r;
+                sv_sample_kernel<NC><<<g2, 256, 0, s>>>(A, b);
+                return launch_check(ctx);
+            } else {
+                return DRWC_ERR_INVALID;
+            }
+        });
+        if (rc) return rc;
+        if ((rc = fork_fdm(b))) return rc;
     }
+    if (v->any_net && (rc = sv_mark(v, v->ev_t[k][1], s))) return rc;
+    for (int b = 0; b < v->o.n_sizes; ++b)
+        DRWC_CUDA_TRY(cudaStreamWaitEvent(s, v->ev_join[b], 0));
     return DRWC_OK;
 }
 
@@ -953,7 +970,7 @@ static int sv_admit(drwc_server* v) {
         T.G = J->G;
         T.W = J->W;
         T.state = 1;
-        T.use_net = v->net && J->p.N == kSvNetN;
+        T.use_net = v->bnet[v->bucket_of_N[J->p.N]] != nullptr;
         T.bucket = v->bucket_of_N[J->p.N];
         T.n_entries = J->s.n_nets + 1;
         T.total = total;
@@ -1137,7 +1154,7 @@ static int sv_round(drwc_server* v) {
         v->st.busy_seconds += ms * 1e-3;
     if (v->timing) {
         for (int k = 0; k < v->o.steps_per_graph; ++k) {
-            if (v->net && cudaEventElapsedTime(&ms, v->ev_t[k][0], v->ev_t[k][1]) == cudaSuccess)
+            if (v->any_net && cudaEventElapsedTime(&ms, v->ev_t[k][0], v->ev_t[k][1]) == cudaSuccess)
                 v->st.net_seconds += ms * 1e-3;
             for (int b = 0; b < v->o.n_sizes; ++b)
                 if (cudaEventElapsedTime(&ms, v->ev_t[k][2 + 2 * b], v->ev_t[k][3 + 2 * b]) ==
@@ -1222,13 +1239,19 @@ static int sv_alloc(drwc_server* v) {
                  o_hdr = take(sizeof(SvHdr)), o_bsum = take(8 * kSvBsumStride * kSvWin * kSvMaxJobs),
                  o_stats = take(8 * SV_NSTATS), o_akl = take(16), o_cnt = take(64),
                  o_dbl = take(8 * (size_t)S * 7), o_walk = take(8 * (size_t)S),
-                 o_int = take(4 * (size_t)S * 5), o_lists = take(4 * (size_t)S * 2),
+                 o_int = take(4 * (size_t)S * 5),
                  o_b = take(4 * (size_t)S * 2 * DRWC_SERVER_MAX_SIZES);
-    size_t o_X = 0, o_O = 0, o_G = 0;
-    if (v->net) {
-        o_X = take(256);  // network inputs stay in shared memory
-        o_O = take(4 * (size_t)S * kSvDecRows);
-        o_G = take(4 * (size_t)S * DRWC_NET_PANELS);
+    size_t o_O[DRWC_SERVER_MAX_SIZES] = {}, o_G[DRWC_SERVER_MAX_SIZES] = {},
+           o_al[DRWC_SERVER_MAX_SIZES] = {};
+    for (int b = 0; b < v->o.n_sizes; ++b) {
+        if (!v->bnet[b]) continue;
+        int32_t orow = 0, grow = 0;
+        drwc_net_dims(v->bnet[b], nullptr, nullptr, &orow, &grow, nullptr);
+        v->A.out_row[b] = orow;
+        v->A.grad_row[b] = grow;
+        o_O[b] = take(4 * (size_t)S * orow);
+        o_G[b] = take(4 * (size_t)S * grow);
+        o_al[b] = take(4 * (size_t)S * 2);
     }
     size_t o_sy[DRWC_SERVER_MAX_SIZES], o_ss[DRWC_SERVER_MAX_SIZES], o_tab[DRWC_SERVER_MAX_SIZES];
     for (int b = 0; b < v->o.n_sizes; ++b) {
@@ -1268,8 +1291,6 @@ static int sv_alloc(drwc_server* v) {
     int* ii = (int*)(B + o_int);
     A.st.hops = ii; A.st.mode = ii + S; A.st.code = ii + 2 * S; A.st.job = ii + 3 * S;
     A.st.grow = ii + 4 * S;
-    A.alist = (int*)(B + o_lists);
-    A.frow = A.alist + S;
     int* bl = (int*)(B + o_b);
     for (int b = 0; b < DRWC_SERVER_MAX_SIZES; ++b) {
         A.blist[b] = bl + (size_t)2 * b * S;
@@ -1277,10 +1298,12 @@ static int sv_alloc(drwc_server* v) {
     }
     A.conf_thresh = v->o.conf_threshold;
     A.audit_frac = v->o.audit_frac;
-    if (v->net) {
-        A.X = (__nv_bfloat16*)(B + o_X);
-        A.O = (float*)(B + o_O);
-        A.Gh = (float*)(B + o_G);
+    for (int b = 0; b < v->o.n_sizes; ++b) {
+        if (!v->bnet[b]) continue;
+        A.O[b] = (float*)(B + o_O[b]);
+        A.Gh[b] = (float*)(B + o_G[b]);
+        A.alist[b] = (int*)(B + o_al[b]);
+        A.frow[b] = A.alist[b] + S;
     }
     A.table = v->o.uniform_table;
     A.fair = v->o.fair_share;
@@ -1353,8 +1376,8 @@ DRWC_API void drwc_server_opts_default(drwc_server_opts* o) {
     o->fair_share = 0;
 }
 
-DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drwc_net* net,
-                                drwc_server** out) {
+DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts,
+                                drwc_net* const* nets, int32_t n_nets, drwc_server** out) {
     if (!ctx || !out) return DRWC_ERR_INVALID;
     *out = nullptr;
     drwc_server_opts o;
@@ -1367,10 +1390,10 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drw
         !(o.audit_frac >= 0.f && o.audit_frac <= 1.f) || o.uniform_table < 0 || o.uniform_table > 1 ||
         o.fair_share < 0 || o.fair_share > 1)
         return DRWC_ERR_INVALID;
-    if (net && net_context(net) != ctx) return DRWC_ERR_INVALID;
+    if (n_nets < 0 || n_nets > DRWC_SERVER_MAX_SIZES || (n_nets > 0 && !nets))
+        return DRWC_ERR_INVALID;
     std::unique_ptr<drwc_server> v(new drwc_server());
     v->ctx = ctx;
-    v->net = net;
     v->o = o;
     v->timing = o.timing != 0;
     for (int n = 0; n <= DRWC_N_MAX; ++n) v->bucket_of_N[n] = -1;
@@ -1378,9 +1401,17 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drw
         const int N = o.sizes[b];
         if (!n_supported(N) || v->bucket_of_N[N] >= 0) return DRWC_ERR_INVALID;
         v->bucket_of_N[N] = b;
-        if (net && N == kSvNetN) v->net_bucket = b;
     }
-    if (net && v->net_bucket < 0) return DRWC_ERR_INVALID;  // the network serves N = 16 jobs
+    // each network serves the jobs of its own resolution
+    for (int q = 0; q < n_nets; ++q) {
+        drwc_net* net = nets[q];
+        if (!net || net_context(net) != ctx) return DRWC_ERR_INVALID;
+        const int N = net_size(net);
+        const int b = N <= DRWC_N_MAX ? v->bucket_of_N[N] : -1;
+        if (b < 0 || v->bnet[b]) return DRWC_ERR_INVALID;
+        v->bnet[b] = net;
+        v->any_net = true;
+    }
     {
         std::lock_guard<std::mutex> lock(ctx->mu);
         DRWC_CUDA_TRY(cudaSetDevice(ctx->device));
@@ -1392,14 +1423,22 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drw
             const double* w[4];
             if (!rc) rc = warm_tables(ctx, o.sizes[b], w);
         }
-        if (!rc && cudaFuncSetAttribute(sv_voxelise_kernel,
-                                        cudaFuncAttributePreferredSharedMemoryCarveout, 50) !=
-                       cudaSuccess)
-            rc = DRWC_ERR_CUDA;  // room for four voxeliser CTAs per SM
+        for (int b = 0; !rc && b < o.n_sizes; ++b) {
+            if (!v->bnet[b]) continue;
+            // room for four voxeliser CTAs per SM
+            cudaError_t e = cudaSuccess;
+            if (o.sizes[b] == 16)
+                e = cudaFuncSetAttribute(sv_voxelise_kernel<16>, cudaFuncAttributePreferredSharedMemoryCarveout, 50);
+            else if (o.sizes[b] == 21)
+                e = cudaFuncSetAttribute(sv_voxelise_kernel<21>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            else if (o.sizes[b] == 23)
+                e = cudaFuncSetAttribute(sv_voxelise_kernel<23>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+            if (e != cudaSuccess) rc = DRWC_ERR_CUDA;
+            if (!rc) rc = net_reserve_rows(v->bnet[b], o.slots);
+            if (!rc) v->A.c1[b] = net_conv1_operands(v->bnet[b]);  // a1 as reserved for `slots` rows
+        }
         if (!rc) rc = sv_alloc(v.get());
         if (!rc) rc = sv_tables(v.get());
-        if (!rc && net) rc = net_reserve_rows(net, o.slots);
-        if (!rc && net) v->A.c1 = net_conv1_operands(net);  // a1 as reserved for `slots` rows
         for (int b = 0; !rc && b < o.n_sizes; ++b) {
             if (cudaStreamCreateWithFlags(&v->side[b], cudaStreamNonBlocking) != cudaSuccess ||
                 cudaEventCreateWithFlags(&v->ev_join[b], cudaEventDisableTiming) != cudaSuccess)
@@ -1413,7 +1452,8 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drw
             for (int q = 0; q < 2 + 2 * o.n_sizes; ++q)
                 if (cudaEventCreate(&v->ev_t[k][q]) != cudaSuccess) rc = DRWC_ERR_CUDA;
         if (!rc) rc = sv_capture(v.get());
-        if (!rc && net) net_hold(net, 1);
+        for (int b = 0; !rc && b < o.n_sizes; ++b)
+            if (v->bnet[b]) net_hold(v->bnet[b], 1);
         if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = DRWC_ERR_CUDA;
         if (rc) {
             cudaGetLastError();
@@ -1441,7 +1481,8 @@ DRWC_API int drwc_server_destroy(drwc_server* v) {
         std::lock_guard<std::mutex> lock(v->ctx->mu);
         cudaSetDevice(v->ctx->device);
         cudaStreamSynchronize(v->ctx->stream);
-        if (v->net) net_hold(v->net, -1);
+        for (int b = 0; b < DRWC_SERVER_MAX_SIZES; ++b)
+            if (v->bnet[b]) net_hold(v->bnet[b], -1);
         sv_free(v);
     }
     delete v;

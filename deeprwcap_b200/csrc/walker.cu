@@ -664,10 +664,11 @@ DRWC_API int drwc_frw_harvest(drwc_ctx* ctx, const drwc_structure* s, const drwc
     return rc;
 }
 
-DRWC_API int drwc_records_voxelise(drwc_ctx* ctx, const drwc_structure* s, int n,
+DRWC_API int drwc_records_voxelise(drwc_ctx* ctx, const drwc_structure* s, int N, int n,
                                    const double* rec, const int32_t* code, void* X,
                                    double* eps64) {
     if (!ctx || n < 0 || (n > 0 && (!rec || !code || !X))) return DRWC_ERR_INVALID;
+    if (N != 16 && N != 21 && N != 23) return DRWC_ERR_INVALID;
     if (n == 0) return DRWC_OK;
     std::lock_guard<std::mutex> lock(ctx->mu);
     DRWC_CUDA_TRY(cudaSetDevice(ctx->device));
@@ -676,22 +677,31 @@ DRWC_API int drwc_records_voxelise(drwc_ctx* ctx, const drwc_structure* s, int n
     HostGeom hg;
     rc = upload_geom(ctx, s, &hg);
     if (rc) return rc;
-    records_kernel<16><<<std::min(n, ctx->sm_count * 8), 256, 0, ctx->stream>>>(
-        hg.dev, n, rec, code, (__nv_bfloat16*)X, eps64);
+    const int grid = std::min(n, ctx->sm_count * 8);
+    if (N == 16)
+        records_kernel<16><<<grid, 256, 0, ctx->stream>>>(hg.dev, n, rec, code, (__nv_bfloat16*)X, eps64);
+    else if (N == 21)
+        records_kernel<21><<<grid, 256, 0, ctx->stream>>>(hg.dev, n, rec, code, (__nv_bfloat16*)X, eps64);
+    else
+        records_kernel<23><<<grid, 256, 0, ctx->stream>>>(hg.dev, n, rec, code, (__nv_bfloat16*)X, eps64);
     rc = launch_check(ctx);
     if (rc) return rc;
     DRWC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
     return DRWC_OK;
 }
 
-DRWC_API int drwc_cubes_random(drwc_ctx* ctx, int n, uint64_t seed, float noise_frac, void* X,
-                               double* eps64) {
+DRWC_API int drwc_cubes_random(drwc_ctx* ctx, int N, int n, uint64_t seed, float noise_frac,
+                               void* X, double* eps64) {
     if (!ctx || n < 0 || (n > 0 && (!X || !eps64))) return DRWC_ERR_INVALID;
+    if (N != 16 && N != 21 && N != 23) return DRWC_ERR_INVALID;
     if (n == 0) return DRWC_OK;
     std::lock_guard<std::mutex> lock(ctx->mu);
     DRWC_CUDA_TRY(cudaSetDevice(ctx->device));
-    random_cubes_kernel<16><<<std::min(n, ctx->sm_count * 8), 256, 0, ctx->stream>>>(
-        n, seed, noise_frac, (__nv_bfloat16*)X, eps64);
+    const int grid = std::min(n, ctx->sm_count * 8);
+    __nv_bfloat16* x = (__nv_bfloat16*)X;
+    if (N == 16) random_cubes_kernel<16><<<grid, 256, 0, ctx->stream>>>(n, seed, noise_frac, x, eps64);
+    else if (N == 21) random_cubes_kernel<21><<<grid, 256, 0, ctx->stream>>>(n, seed, noise_frac, x, eps64);
+    else random_cubes_kernel<23><<<grid, 256, 0, ctx->stream>>>(n, seed, noise_frac, x, eps64);
     return launch_check(ctx);
 }
 
@@ -1032,7 +1042,8 @@ DRWC_API int drwc_frw_walks_learned(drwc_ctx* ctx, const drwc_structure* s,
                                     double* stats) {
     if (!ctx || !net || walk0 < 0 || nwalks <= 0 || !end_net || !hops || !weight)
         return DRWC_ERR_INVALID;
-    if (net_context(net) != ctx || !p || p->N != DRWC_NET_N) return DRWC_ERR_INVALID;
+    if (net_context(net) != ctx || !p || p->N != DRWC_NET_N || net_size(net) != DRWC_NET_N)
+        return DRWC_ERR_INVALID;
     drwc_learned_opts o;
     drwc_learned_opts_default(&o);
     if (opts) o = *opts;

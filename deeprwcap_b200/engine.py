@@ -395,11 +395,22 @@ NET_OUT = 1552
 NET_PANELS = 1536
 
 
-def _param_layout():
+def net_dims(N: int) -> dict:
+    """Layer sizes of the network for cube resolution N (mirrors NetDims in nn.cu)."""
+    d = [N]
+    for _ in range(3):
+        d.append((d[-1] - 1) // 2 + 1)
+    np_ = 6 * N * N
+    return {"N": N, "D": d, "panels": np_, "out_row": (np_ + 1 + 15) // 16 * 16,
+            "grad_row": (np_ + 15) // 16 * 16, "features": 64 * d[3] ** 3}
+
+
+def _param_layout(N: int = 16):
     """Offsets of the flat FP32 parameter vector (mirrors ParamLayout in nn.cu)."""
+    dm = net_dims(N)
     names = [("w1", 16 * 27), ("b1", 16), ("w2", 32 * 432), ("b2", 32), ("w3", 64 * 864),
-             ("b3", 64), ("wd", NET_OUT * 512), ("bd", NET_OUT), ("wg", NET_PANELS * 512),
-             ("bg", NET_PANELS)]
+             ("b3", 64), ("wd", dm["out_row"] * dm["features"]), ("bd", dm["out_row"]),
+             ("wg", dm["panels"] * dm["features"]), ("bg", dm["panels"])]
     off, lay = 0, {}
     for name, n in names:
         lay[name] = (off, n)
@@ -410,11 +421,14 @@ def _param_layout():
 class Net:
     """The learned transition network (device-resident; see include/drwc.h)."""
 
-    def __init__(self, seed: int = 0, ctx: Context | None = None):
+    def __init__(self, seed: int = 0, ctx: Context | None = None, N: int = 16):
         self.ctx = ctx or default_context()
         h = C.c_void_p()
-        check(self.ctx.lib.drwc_net_create(self.ctx.h, 16, seed, C.byref(h)), "drwc_net_create")
+        check(self.ctx.lib.drwc_net_create(self.ctx.h, int(N), seed, C.byref(h)), "drwc_net_create")
         self.h = h
+        v = [C.c_int32() for _ in range(5)]
+        check(self.ctx.lib.drwc_net_dims(h, *[C.byref(x) for x in v]), "drwc_net_dims")
+        self.N, self.panels, self.out_row, self.grad_row, self.features = (x.value for x in v)
         n = C.c_int64()
         check(self.ctx.lib.drwc_net_param_count(h, C.byref(n)), "drwc_net_param_count")
         self.nparams = n.value
@@ -435,7 +449,7 @@ class Net:
         return out
 
     def forward(self, X, O, G=None) -> None:
-        """X: [B, 4096] bfloat16 device tensor; O: [B, 1552] float32; G: [B, 1536]."""
+        """X: [B, N^3] bfloat16 device tensor; O: [B, out_row] float32; G: [B, grad_row]."""
         torch_ready()
         check(self.ctx.lib.drwc_net_forward(self.h, int(X.shape[0]), ptr(X), ptr(O), ptr(G)),
               "drwc_net_forward")
@@ -507,19 +521,21 @@ def harvest(structure, params, walk0: int, nwalks: int, cap: int, ctx: Context |
     return rec[:cnt.value], code[:cnt.value]
 
 
-def records_voxelise(structure, rec, code, X, eps64=None, ctx: Context | None = None):
+def records_voxelise(structure, rec, code, X, eps64=None, ctx: Context | None = None, N: int = 16):
+    """Logged cubes -> network inputs X [n, N^3] (BF16) and FP64 permittivity."""
     ctx = ctx or default_context()
     s = structure.to_c() if hasattr(structure, "to_c") else structure
     torch_ready()
-    check(ctx.lib.drwc_records_voxelise(ctx.h, C.byref(s), int(rec.shape[0]), ptr(rec), ptr(code),
-                                        ptr(X), ptr(eps64)), "drwc_records_voxelise")
+    check(ctx.lib.drwc_records_voxelise(ctx.h, C.byref(s), int(N), int(rec.shape[0]), ptr(rec),
+                                        ptr(code), ptr(X), ptr(eps64)), "drwc_records_voxelise")
 
 
 def cubes_random(n: int, seed: int, X, eps64, noise_frac: float = 0.1,
-                 ctx: Context | None = None):
+                 ctx: Context | None = None, N: int = 16):
+    """Random transition cubes at resolution N: X [n, N^3] BF16, eps64 FP64."""
     ctx = ctx or default_context()
     torch_ready()
-    check(ctx.lib.drwc_cubes_random(ctx.h, int(n), seed, noise_frac, ptr(X), ptr(eps64)),
+    check(ctx.lib.drwc_cubes_random(ctx.h, int(N), int(n), seed, noise_frac, ptr(X), ptr(eps64)),
           "drwc_cubes_random")
     ctx.synchronize()
 
@@ -559,18 +575,20 @@ class Server:
     """The persistent multi-job extraction server (drwc_server_* in
     include/drwc.h): jobs are submitted from the host, admitted by device
     footprint and run concurrently on the device; results come back per job.
-    With ``net`` the hops of N = 16 jobs go through the learned network."""
+    ``net``: a Net or a list of Nets of different resolutions; the hops of a
+    job whose N has a network go through it."""
 
-    def __init__(self, ctx: Context | None = None, net: "Net | None" = None, **opts):
-        self.ctx = ctx or (net.ctx if net is not None else default_context())
+    def __init__(self, ctx: Context | None = None, net=None, **opts):
+        nets = [] if net is None else (list(net) if isinstance(net, (list, tuple)) else [net])
+        self.ctx = ctx or (nets[0].ctx if nets else default_context())
         self.opts = server_opts(**opts)
         h = C.c_void_p()
+        arr = (C.c_void_p * max(1, len(nets)))(*[n.h for n in nets])
         torch_ready()
-        check(self.ctx.lib.drwc_server_create(self.ctx.h, C.byref(self.opts),
-                                              net.h if net is not None else None, C.byref(h)),
-              "drwc_server_create")
+        check(self.ctx.lib.drwc_server_create(self.ctx.h, C.byref(self.opts), arr, len(nets),
+                                              C.byref(h)), "drwc_server_create")
         self.h = h
-        self.net = net
+        self.nets = nets  # the server holds them
 
     def submit(self, structure, params) -> int:
         s = structure.to_c() if hasattr(structure, "to_c") else structure

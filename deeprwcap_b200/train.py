@@ -1,6 +1,6 @@
 """Train the learned transition network on FDM data the engine generates.
 
-    python -m deeprwcap_b200.train [--samples 1048576] [--epochs 3] [--out PATH]
+    python -m deeprwcap_b200.train [--N 16|21|23] [--samples 1048576] [--epochs 3] [--out PATH]
 
 Training data (all on the device):
   * transition cubes logged from real walks (drwc_frw_harvest) on the
@@ -34,11 +34,10 @@ DEFAULT_CKPT = Path(__file__).resolve().parent / "models" / "net_n16.npz"
 
 
 def build_dataset(ctx, n_total: int, walk_frac: float = 0.5, seed: int = 0, chunk: int = 32768,
-                  log=print):
-    """X [n, 4096] bf16, T [n, 1536] f32, TG [n, 1536] f32 (device tensors)."""
+                  log=print, N: int = 16):
+    """X [n, N^3] bf16, T [n, 6N^2] f32, TG [n, 6N^2] f32 (device tensors)."""
     import torch
     dev = torch.device("cuda", ctx.device)
-    N = 16
     n_walk = int(n_total * walk_frac)
     n_rand = n_total - n_walk
     X = torch.empty(n_total, N ** 3, dtype=torch.bfloat16, device=dev)
@@ -70,7 +69,7 @@ def build_dataset(ctx, n_total: int, walk_frac: float = 0.5, seed: int = 0, chun
             n = int(rec.shape[0])
             if n == 0:
                 continue
-            engine.records_voxelise(s, rec, code, X[pos:pos + n], eps[:n], ctx=ctx)
+            engine.records_voxelise(s, rec, code, X[pos:pos + n], eps[:n], ctx=ctx, N=N)
             solve_chunk(pos, pos + n)
             pos += n
             got += n
@@ -78,7 +77,7 @@ def build_dataset(ctx, n_total: int, walk_frac: float = 0.5, seed: int = 0, chun
     done = 0
     while done < n_rand:
         n = min(chunk, n_rand - done)
-        engine.cubes_random(n, seed * 7919 + done, X[pos:pos + n], eps[:n], ctx=ctx)
+        engine.cubes_random(n, seed * 7919 + done, X[pos:pos + n], eps[:n], ctx=ctx, N=N)
         solve_chunk(pos, pos + n)
         pos += n
         done += n
@@ -92,18 +91,19 @@ def evaluate(net, X, T, TG, batch: int = 4096):
     import torch
     dev = X.device
     kls, g_err = [], []
-    O = torch.empty(batch, engine.NET_OUT, device=dev)
-    G = torch.empty(batch, engine.NET_PANELS, device=dev)
+    P = net.panels
+    O = torch.empty(batch, net.out_row, device=dev)
+    G = torch.empty(batch, net.grad_row, device=dev)
     for lo in range(0, X.shape[0], batch):
         hi = min(X.shape[0], lo + batch)
         n = hi - lo
         net.forward(X[lo:hi], O[:n], G[:n])
         torch.cuda.synchronize()
-        logp = torch.log_softmax(O[:n, :1536], dim=1)
+        logp = torch.log_softmax(O[:n, :P], dim=1)
         t = T[lo:hi]
         kl = (t * (torch.log(t.clamp_min(1e-30)) - logp)).sum(1)
         kls.append(kl)
-        ge = (G[:n] - TG[lo:hi]).abs().sum(1) / TG[lo:hi].abs().sum(1).clamp_min(1e-12)
+        ge = (G[:n, :P] - TG[lo:hi]).abs().sum(1) / TG[lo:hi].abs().sum(1).clamp_min(1e-12)
         g_err.append(ge)
     kl = torch.cat(kls)
     ge = torch.cat(g_err)
@@ -153,7 +153,8 @@ def save(net, path: Path, meta: dict):
 
 def load(path: Path = DEFAULT_CKPT, ctx=None) -> "engine.Net":
     d = np.load(path)
-    net = engine.Net(seed=0, ctx=ctx)
+    N = int(d["N"]) if "N" in d else 16
+    net = engine.Net(seed=0, ctx=ctx, N=N)
     net.set_params(d["params"])
     return net
 
@@ -166,18 +167,19 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", type=str, default=str(DEFAULT_CKPT))
+    ap.add_argument("--N", type=int, default=16, choices=[16, 21, 23])
     a = ap.parse_args()
     import torch
     ctx = engine.default_context(0)
-    X, T, TG = build_dataset(ctx, a.samples, seed=a.seed)
+    X, T, TG = build_dataset(ctx, a.samples, seed=a.seed, N=a.N)
     Xt, Tt, TGt, Xv, Tv, TGv = split(X, T, TG, seed=a.seed)
-    net = engine.Net(seed=a.seed + 1, ctx=ctx)
+    net = engine.Net(seed=a.seed + 1, ctx=ctx, N=a.N)
     before = evaluate(net, Xv, Tv, TGv)
     print("before:", before)
     secs = train(net, Xt, Tt, TGt, epochs=a.epochs, batch=a.batch, lr=a.lr, seed=a.seed)
     after = evaluate(net, Xv, Tv, TGv)
     print("after:", after)
-    save(net, Path(a.out), {"samples": X.shape[0], "epochs": a.epochs, "train_seconds": secs,
+    save(net, Path(a.out), {"N": a.N, "samples": X.shape[0], "epochs": a.epochs, "train_seconds": secs,
                             "val_kl_mean": after["kl_mean"], "val_kl_p95": after["kl_p95"],
                             "val_grad_rel_l1": after["grad_rel_l1"]})
     print("saved", a.out)

@@ -202,21 +202,28 @@ DRWC_API int drwc_gemm_bf16(drwc_ctx* ctx, int M, int N, int K, const void* A, i
  * FP32 master weights. Architecture family of training_pytorch/src/
  * architecture.py; trained here on FDM data the engine generates. */
 typedef struct drwc_net drwc_net;
-#define DRWC_NET_N 16
-#define DRWC_NET_OUT 1552      /* Poisson logits (1536) + confidence + padding */
-#define DRWC_NET_PANELS 1536
+#define DRWC_NET_N 16          /* the learned walker's resolution */
+#define DRWC_NET_OUT 1552      /* N = 16: Poisson logits (1536) + confidence + padding */
+#define DRWC_NET_PANELS 1536   /* N = 16: 6 N^2 */
+/* N: 16, 21 or 23 (the cube resolution the network reads and predicts). */
 DRWC_API int drwc_net_create(drwc_ctx* ctx, int N, uint64_t seed, drwc_net** out);
 DRWC_API int drwc_net_destroy(drwc_net* net);
+/* Sizes (host, each nullable): N, panels = 6 N^2, out_row = floats per row of
+ * O (panels + confidence, padded to 16), grad_row = floats per row of G
+ * (panels padded to 16), features = encoder outputs per cube. */
+DRWC_API int drwc_net_dims(drwc_net* net, int32_t* N, int32_t* panels, int32_t* out_row,
+                           int32_t* grad_row, int32_t* features);
 DRWC_API int drwc_net_param_count(drwc_net* net, int64_t* count);
 DRWC_API int drwc_net_get_params(drwc_net* net, float* host);
 DRWC_API int drwc_net_set_params(drwc_net* net, const float* host);
 DRWC_API int drwc_net_gradients(drwc_net* net, float* host);
-/* Device buffers: X [B, 4096] BF16 -> O [B, 1552] FP32, G [B, 1536] FP32
- * (nullable). Async on the context stream. */
+/* Device buffers: X [B, N^3] BF16 -> O [B, out_row] FP32, G [B, grad_row]
+ * FP32 (nullable). Async on the context stream. */
 DRWC_API int drwc_net_forward(drwc_net* net, int B, const void* X, float* O, float* G);
-/* One optimisation step (device buffers X, T = target Green's functions
- * [B, 1536] rows summing to 1, TG = scaled gradient targets [B, 1536] or
- * NULL); apply = 0 computes losses and gradients without updating.
+/* One optimisation step (device buffers X [B, N^3], T = target Green's
+ * functions [B, panels] rows summing to 1, TG = scaled gradient targets
+ * [B, panels] or NULL); apply = 0 computes losses and gradients without
+ * updating.
  * loss_out (host, 3): cross entropy, confidence MSE, gradient MSE. */
 DRWC_API int drwc_net_train_step(drwc_net* net, int B, const void* X, const float* T,
                                  const float* TG, float lr, float weight_decay, float clip,
@@ -304,16 +311,18 @@ DRWC_API int drwc_job_h2d_bytes(drwc_job* job, int64_t* bytes);
 DRWC_API int drwc_frw_harvest(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
                               int64_t walk0, int64_t nwalks, int32_t cap, double* rec,
                               int32_t* code, int32_t* count);
-/* Logged cubes -> network inputs X (BF16 [n, 4096], eps / max eps) and FP64
- * permittivity (nullable), N = 16. First-hop cubes are voxelised in the frame
- * where their gradient axis is z, so their gradient target is WVTZ. */
-DRWC_API int drwc_records_voxelise(drwc_ctx* ctx, const drwc_structure* s, int n,
+/* Logged cubes -> network inputs X (BF16 [n, N^3], eps / max eps) and FP64
+ * permittivity (nullable) at resolution N (16, 21, 23). First-hop cubes are
+ * voxelised in the frame where their gradient axis is z, so their gradient
+ * target is WVTZ. */
+DRWC_API int drwc_records_voxelise(drwc_ctx* ctx, const drwc_structure* s, int N, int n,
                                    const double* rec, const int32_t* code, void* X,
                                    double* eps64);
 /* Random transition cubes (1-4 layers along a random axis, 0-2 boxes, eps in
- * [2, 8], noise_frac of them with voxel noise), N = 16: X BF16 and FP64. */
-DRWC_API int drwc_cubes_random(drwc_ctx* ctx, int n, uint64_t seed, float noise_frac, void* X,
-                               double* eps64);
+ * [2, 8], noise_frac of them with voxel noise) at resolution N (16, 21, 23):
+ * X BF16 [n, N^3] and FP64. */
+DRWC_API int drwc_cubes_random(drwc_ctx* ctx, int N, int n, uint64_t seed, float noise_frac,
+                               void* X, double* eps64);
 
 typedef struct drwc_learned_opts {
     int32_t slots;          /* walks in flight (default 65536) */
@@ -343,10 +352,10 @@ DRWC_API int drwc_frw_walks_learned(drwc_ctx* ctx, const drwc_structure* s,
  * two batches of walk records) fits the HBM arena and a job-table entry is
  * free, and their walks then share the slots with every other running job.
  * Each replay of a captured CUDA graph advances every slot by
- * steps_per_graph hops: the geometry step of all slots, then (with a
- * network) one batched network pass over the N = 16 cubes of all jobs, and
- * the FDM solves bucketed by cube resolution, buckets on parallel graph
- * branches. A job's walks are reduced batch by batch in walk-id order, so its
+ * steps_per_graph hops: the geometry step of all slots, then one batched
+ * network pass per resolution that has a network over the cubes of all its
+ * jobs, and the FDM solves bucketed by cube resolution, buckets on parallel
+ * graph branches. A job's walks are reduced batch by batch in walk-id order, so its
  * result is bit-identical to drwc_frw_run (plain form) whatever else runs. */
 typedef struct drwc_server drwc_server;
 #define DRWC_SERVER_MAX_SIZES 4
@@ -372,11 +381,13 @@ typedef struct drwc_server_opts {
     int32_t reserved_;
 } drwc_server_opts;
 DRWC_API void drwc_server_opts_default(drwc_server_opts* o);
-/* net (nullable): with a network, hops of N = 16 jobs go through it
- * (confidence routing + audits as drwc_frw_walks_learned); without one every
- * hop is an FDM solve. The server uses the context's stream and lock. */
-DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts, drwc_net* net,
-                                drwc_server** out);
+/* nets (n_nets of them, each of a different served resolution; none: every
+ * hop is an FDM solve): the hops of a job whose N has a network go through it
+ * (confidence routing + audits as drwc_frw_walks_learned), the others through
+ * the FDM solve. The server uses the context's stream and lock and holds the
+ * networks (destroy it before them). */
+DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts,
+                                drwc_net* const* nets, int32_t n_nets, drwc_server** out);
 /* Stops the request thread; queued and running jobs end as failed
  * (DRWC_ERR_SHUTDOWN). */
 DRWC_API int drwc_server_destroy(drwc_server* srv);

@@ -71,7 +71,7 @@ def test_server_defaults_and_argument_checks_without_device():
     o2 = engine.server_opts(sizes=(16, 23), slots=1024)
     assert o2.n_sizes == 2 and list(o2.sizes[:2]) == [16, 23] and o2.slots == 1024
     h = C.c_void_p()
-    assert L.drwc_server_create(None, C.byref(o), None, C.byref(h)) == 1
+    assert L.drwc_server_create(None, C.byref(o), None, 0, C.byref(h)) == 1
     assert L.drwc_server_destroy(None) == 1
     st = abi.ServerStats()
     assert L.drwc_server_stats_get(None, C.byref(st)) == 1

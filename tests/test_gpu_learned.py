@@ -98,22 +98,22 @@ def _eps_cpu(s, pts):
     return eps
 
 
-def test_separable_voxelisation_matches_fill_rule(ctx):
+@pytest.mark.parametrize("N", [16, 23])
+def test_separable_voxelisation_matches_fill_rule(ctx, N):
     """Network inputs of logged walk cubes (dense stack: 5 layers, 10 blocks;
     first-hop cubes in their rotated frames) equal the fill rule evaluated at
-    every cell centre, bit for bit."""
+    every cell centre, bit for bit, at N = 16 and 23."""
     import torch
     s = W.dense_stack(seed=3)
     p = W.job_params_plain(N=16, seed=77)
     rec, code = engine.harvest(s, p, 0, 256, 6000, ctx=ctx)
     n = int(rec.shape[0])
     dev = rec.device
-    X = torch.empty(n, 4096, dtype=torch.bfloat16, device=dev)
-    eps = torch.empty(n, 4096, dtype=torch.float64, device=dev)
-    engine.records_voxelise(s, rec, code, X, eps, ctx=ctx)
+    X = torch.empty(n, N ** 3, dtype=torch.bfloat16, device=dev)
+    eps = torch.empty(n, N ** 3, dtype=torch.float64, device=dev)
+    engine.records_voxelise(s, rec, code, X, eps, ctx=ctx, N=N)
     torch.cuda.synchronize()
     rec, code, eps = rec.cpu().numpy(), code.cpu().numpy(), eps.cpu().numpy()
-    N = 16
     t = np.array([(2.0 * i + 1.0) / N - 1.0 for i in range(N)])
     k, j, i = np.meshgrid(np.arange(N), np.arange(N), np.arange(N), indexing="ij")
     i, j, k = i.ravel(), j.ravel(), k.ravel()

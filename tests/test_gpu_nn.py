@@ -19,18 +19,19 @@ def _bf(t):
     return t.to(torch.bfloat16).float()
 
 
-def _unpack(p):
+def _unpack(p, N=16):
     import torch
-    lay, _ = engine._param_layout()
+    lay, _ = engine._param_layout(N)
     P = {k: torch.from_numpy(p[o:o + n].copy()) for k, (o, n) in lay.items()}
     return P
 
 
 def ref_forward(P, X, round_act=True):
-    """X [B, 16, 16, 16] (z, y, x) float; returns O [B, 1552], G [B, 1536]."""
+    """X [B, N, N, N] (z, y, x) float; returns O [B, out_row], G [B, panels]."""
     import torch
     import torch.nn.functional as F
-    B = X.shape[0]
+    B, N = X.shape[0], X.shape[1]
+    dm = engine.net_dims(N)
     w1 = _bf(P["w1"]).view(16, 1, 3, 3, 3)
     w2 = _bf(P["w2"]).view(32, 27, 16).permute(0, 2, 1).reshape(32, 16, 3, 3, 3)
     w3 = _bf(P["w3"]).view(64, 27, 32).permute(0, 2, 1).reshape(64, 32, 3, 3, 3)
@@ -38,68 +39,73 @@ def ref_forward(P, X, round_act=True):
     h = rb(F.relu(F.conv3d(X[:, None], w1, P["b1"], stride=2, padding=1)))
     h = rb(F.relu(F.conv3d(h, w2, P["b2"], stride=2, padding=1)))
     h = rb(F.relu(F.conv3d(h, w3, P["b3"], stride=2, padding=1)))
-    feat = h.permute(0, 2, 3, 4, 1).reshape(B, 512)
-    O = feat @ _bf(P["wd"]).view(1552, 512).T + P["bd"]
-    G = feat @ _bf(P["wg"]).view(1536, 512).T + P["bg"]
+    F_ = dm["features"]
+    feat = h.permute(0, 2, 3, 4, 1).reshape(B, F_)
+    O = feat @ _bf(P["wd"]).view(dm["out_row"], F_).T + P["bd"]
+    G = feat @ _bf(P["wg"]).view(dm["panels"], F_).T + P["bg"]
     return O, G
 
 
-def _inputs(B, seed):
+def _inputs(B, seed, N=16):
     import torch
-    eps, _ = W.fdm_cubes(B, 16, seed=seed, noise_frac=0.3)
+    eps, _ = W.fdm_cubes(B, N, seed=seed, noise_frac=0.3)
     x = eps / eps.reshape(B, -1).max(axis=1)[:, None, None, None]
     return torch.from_numpy(x.astype(np.float32)).to(torch.bfloat16)
 
 
-def test_forward_matches_reference(ctx):
+@pytest.mark.parametrize("N", [16, 21, 23])
+def test_forward_matches_reference(ctx, N):
     import torch
-    net = engine.Net(seed=3, ctx=ctx)
+    net = engine.Net(seed=3, ctx=ctx, N=N)
+    assert (net.N, net.panels, net.out_row, net.grad_row, net.features) == tuple(
+        engine.net_dims(N)[k] for k in ("N", "panels", "out_row", "grad_row", "features"))
     B = 37
-    X = _inputs(B, 1)
+    X = _inputs(B, 1, N)
     dev = torch.device("cuda", 0)
-    O = torch.zeros(B, 1552, device=dev)
-    G = torch.zeros(B, 1536, device=dev)
+    O = torch.zeros(B, net.out_row, device=dev)
+    G = torch.zeros(B, net.grad_row, device=dev)
     net.forward(X.view(B, -1).to(dev), O, G)
     ctx.synchronize()
-    P = _unpack(net.get_params())
+    P = _unpack(net.get_params(), N)
     Or, Gr = ref_forward(P, X.float())
-    for got, ref in ((O.cpu(), Or), (G.cpu(), Gr)):
+    for got, ref in ((O.cpu(), Or), (G.cpu()[:, :net.panels], Gr)):
         scale = ref.abs().max().item()
         assert (got - ref).abs().max().item() <= 2e-2 * scale
 
 
-@pytest.mark.parametrize("B", [64, 512])
-def test_backward_matches_autograd(ctx, B):
+@pytest.mark.parametrize("B,N", [(64, 16), (512, 16), (96, 21), (96, 23)])
+def test_backward_matches_autograd(ctx, B, N):
     import torch
-    net = engine.Net(seed=5, ctx=ctx)
-    X = _inputs(B, 2)
+    net = engine.Net(seed=5, ctx=ctx, N=N)
+    NP = net.panels
+    X = _inputs(B, 2, N)
     g = torch.Generator().manual_seed(0)
-    T = torch.rand(B, 1536, generator=g) ** 4
+    T = torch.rand(B, NP, generator=g) ** 4
     T = T / T.sum(1, keepdim=True)
-    TG = torch.randn(B, 1536, generator=g) * 0.1
+    TG = torch.randn(B, NP, generator=g) * 0.1
     dev = torch.device("cuda", 0)
     loss = net.train_step(X.view(B, -1).to(dev), T.to(dev), TG.to(dev), lr=0.0, apply=False,
                           w_conf=0.1, w_grad=1.0)
     grads = net.gradients()
-    P = _unpack(net.get_params())
+    P = _unpack(net.get_params(), N)
     Pt = {k: v.clone().requires_grad_(True) for k, v in P.items()}
     O, G = ref_forward(Pt, X.float(), round_act=False)
-    logs = torch.log_softmax(O[:, :1536], dim=1)
+    logs = torch.log_softmax(O[:, :NP], dim=1)
     ce = -(T * logs).sum(1).mean()
     kl = (T * (torch.log(T.clamp_min(1e-30)) - logs)).sum(1)
     cstar = torch.log10(kl.detach().clamp_min(0) + 1e-8)
-    conf = ((O[:, 1536] - cstar) ** 2).mean()
+    conf = ((O[:, NP] - cstar) ** 2).mean()
     gm = ((G - TG) ** 2).mean()
     total = ce + 0.1 * conf + 1.0 * gm
     total.backward()
     assert abs(loss[0] - ce.item()) <= 1e-2 * abs(ce.item())
-    lay, _ = engine._param_layout()
+    lay, _ = engine._param_layout(N)
     for k in ("w1", "b1", "w2", "b2", "w3", "b3", "wd", "bd", "wg", "bg"):
         o, n = lay[k]
         gd = torch.from_numpy(grads[o:o + n])
         gr = Pt[k].grad.reshape(-1)
         if k in ("wd", "bd"):  # rows past the confidence output carry no gradient
-            m = 1537 * (512 if k == "wd" else 1)
+            m = (NP + 1) * (net.features if k == "wd" else 1)
             gd, gr = gd[:m], gr[:m]
         rel = (gd - gr).norm().item() / max(gr.norm().item(), 1e-12)
         assert rel < 5e-2, (k, rel)

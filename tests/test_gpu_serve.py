@@ -84,17 +84,22 @@ def small_net(ctx):
 
 
 def test_learned_mix_equals_alone(ctx, small_net):
+    """Networks for N = 16 and 21 (the 21 one untrained: the equality does not
+    depend on the weights) and an N = 23 job on the FDM path, alone and mixed."""
+    net21 = engine.Net(seed=11, ctx=ctx, N=21)
+    nets = [small_net, net21]
     jobs = [
         (W.two_layer_crossing(), _params(16, 21, 20000, 8192)),
         (W.wire_stack(3, 5, seed=6), _params(16, 22, 15000, 8192)),
         (W.wire_stack(2, 6, seed=7), _params(21, 23, 10000, 8192)),
+        (W.wire_stack(2, 4, seed=8), _params(23, 24, 8000, 8192)),
     ]
     opts = dict(slots=8192, audit_frac=0.05, conf_threshold=-1.0)
     alone = []
     for s, p in jobs:
-        with engine.Server(ctx, net=small_net, **opts) as srv:
+        with engine.Server(ctx, net=nets, **opts) as srv:
             alone.append(srv.wait(srv.submit(s, p), timeout=600))
-    with engine.Server(ctx, net=small_net, **opts) as srv:
+    with engine.Server(ctx, net=nets, **opts) as srv:
         ids = [srv.submit(s, p) for s, p in jobs]
         res = [srv.wait(i, timeout=600) for i in ids]
         st = srv.stats()
@@ -102,6 +107,9 @@ def test_learned_mix_equals_alone(ctx, small_net):
         _same(r, a)
     assert st["net_hops"] > 0 and st["audits"] > 0 and st["fdm_hops"] > 0
     assert st["audit_kl_mean"] > 0.0
+    # the untrained N = 21 network cannot be in the same place as a trained one,
+    # but its walks finish and are counted
+    assert res[2].walks == 10000
 
 
 def test_rejected_requests(ctx):
@@ -152,3 +160,24 @@ def test_learned_server_agrees_with_learned_walker(ctx, small_net):
     assert st["net_hops"] == st["hops"] and r.walks == nw
     assert abs(r.hops - int(h1.sum())) <= 0.01 * h1.sum()
     assert np.all(np.abs(r.cap - c1) <= 1.0 * r.stderr + 1e-12), (r.cap, c1, r.stderr)
+
+
+@pytest.mark.parametrize("N", [21, 23])
+def test_learned_server_at_larger_resolutions(ctx, N):
+    """A network trained here at N = 21 / 23 (2^16 engine-generated samples,
+    3 epochs) drives the hops of a job at that resolution: the walks finish,
+    nearly every hop goes through the network, and the self-capacitance
+    lands near the FDM walk's (a loose bar for a network trained this
+    briefly; the benchmark measures the full-size training)."""
+    X, T, TG = train.build_dataset(ctx, 1 << 16, seed=3, log=lambda *a: None, N=N)
+    net = engine.Net(seed=4, ctx=ctx, N=N)
+    train.train(net, X, T, TG, epochs=3, batch=512, lr=1e-3, log=lambda *a: None)
+    s = W.two_layer_crossing()
+    p = _params(N, 51, 60000, 16384)
+    ref = engine.extract(s, p, ctx)
+    with engine.Server(ctx, net=net, slots=16384, audit_frac=0.01, conf_threshold=1e9) as srv:
+        r = srv.wait(srv.submit(s, p), timeout=900)
+        st = srv.stats()
+    assert r.walks == 60000 and st["net_hops"] >= 0.95 * st["hops"]
+    assert abs(r.cap[0] - ref.cap[0]) <= 0.05 * abs(ref.cap[0]), (r.cap[0], ref.cap[0])
+
