@@ -260,8 +260,9 @@ def serving_section(ctx, args, net):
     through three arms on the same seeded jobs: drwc_frw_run one job at a
     time in arrival order (the FDM-per-hop engine without serving), the
     server with an FDM solve on every hop, and the server with the learned
-    network (N = 16 jobs) and the uniform-permittivity table for cubes of a
-    single permittivity. Latency = submission to result."""
+    networks (one per resolution, N = 16 from the learned section, 21 and 23
+    trained here the same way) and the uniform-permittivity table for cubes
+    of a single permittivity. Latency = submission to result."""
     from deeprwcap_b200 import engine
     from deeprwcap_b200 import workloads as W
     stream = W.serving_stream(n_jobs=args.serve_jobs, rate=50.0, seed=1,
@@ -318,11 +319,33 @@ def serving_section(ctx, args, net):
            "total_walks": int(sum(j.walks for j in stream)),
            "sequential_frw_run": seq, "served_fdm": plain}
     if net is not None:
-        learned, res_l = served(net=net, uniform_table=1)
+        # networks for the other served resolutions, trained here like the N = 16 one
+        from deeprwcap_b200 import train
+        nets, train_info = [net], {}
+        for N in (21, 23):
+            t0 = time.perf_counter()
+            X, T, TG = train.build_dataset(ctx, args.serve_train_samples, seed=N, N=N,
+                                           log=lambda *a: None)
+            Xt, Tt, TGt, Xv, Tv, TGv = train.split(X, T, TG, seed=N)
+            nN = engine.Net(seed=N, ctx=ctx, N=N)
+            train.train(nN, Xt, Tt, TGt, epochs=args.train_epochs, batch=512, lr=1e-3,
+                        log=lambda *a: None)
+            train_info[str(N)] = {"samples": int(X.shape[0]), "epochs": args.train_epochs,
+                                  "seconds": time.perf_counter() - t0,
+                                  **train.evaluate(nN, Xv, Tv, TGv)}
+            del X, T, TG, Xt, Tt, TGt, Xv, Tv, TGv
+            nets.append(nN)
+        out["train_21_23"] = train_info
+        learned, res_l = served(net=nets, uniform_table=1)
         # capacitance agreement of the learned+served form with the FDM walk, per job
         self_diff = [abs(a.cap[0] - b.cap[0]) / abs(b.cap[0]) for a, b in zip(res_l, res_p)]
         learned["self_cap_rel_diff_vs_fdm"] = {"max": float(max(self_diff)),
                                                "mean": float(np.mean(self_diff))}
+        # the two estimates are independent runs: difference over combined 1-sigma
+        zs = [abs(a.cap[0] - b.cap[0]) / float(np.hypot(a.stderr[0], b.stderr[0]))
+              for a, b in zip(res_l, res_p)]
+        learned["self_cap_diff_over_combined_sigma"] = {"max": float(max(zs)),
+                                                        "mean": float(np.mean(zs))}
         learned["self_cap_rel_stderr_fdm_mean"] = float(np.mean(
             [b.stderr[0] / abs(b.cap[0]) for b in res_p]))
         out["served_learned_table"] = learned
@@ -620,6 +643,7 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--serve-jobs", type=int, default=10)
     ap.add_argument("--serve-walks-max", type=float, default=1e6)
+    ap.add_argument("--serve-train-samples", type=int, default=1 << 18)
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.workload == "fdm_batch":
