@@ -207,11 +207,18 @@ def learned_section(ctx, args):
     for name, kw in (("served_learned", {}), ("served_learned_table", {"uniform_table": 1})):
         pj = W.job_params_plain(N=16, seed=4242, tol=FDM_TOL, min_walks=nw, max_walks=nw,
                                 batch_walks=1 << 16)
-        with engine.Server(ctx, net=net, **kw) as srv:
+        with engine.Server(ctx, net=net, timing=1 if not kw else 0, **kw) as srv:
             t2 = time.perf_counter()
             r = srv.wait(srv.submit(s, pj), timeout=3600)
             dt = time.perf_counter() - t2
             sst = srv.stats()
+        if not kw:
+            # network stage of the served step (voxeliser + conv1, conv2, conv3, heads,
+            # sampler) timed by graph event nodes; one gradient-head row per walk
+            flop = sst["net_rows"] * 2.0 * (512 * 16 * 27 + 64 * 32 * 432 + 8 * 64 * 864 +
+                                             512 * net.out_row) + nw * 2.0 * 512 * net.grad_row
+            served_nn = {"rows": sst["net_rows"], "seconds": sst["net_seconds"],
+                         "tflops": flop / max(sst["net_seconds"], 1e-12) / 1e12}
         served[name] = {"seconds": dt, "hops": int(r.hops), "hops_per_s": r.hops / dt,
                         "net_hops": sst["net_hops"], "fdm_hops": sst["fdm_hops"],
                         "table_hops": sst["table_hops"], "fallbacks": sst["fallbacks"],
@@ -251,7 +258,10 @@ def learned_section(ctx, args):
             "self_rel_diff": abs(c1[0] - c0[0]) / abs(c0[0]),
             "nn_forward": {"cubes": B, "seconds": t_nn, "tflops": flop / t_nn / 1e12,
                            "peak_tflops": bf16, "frac": flop / t_nn / 1e12 / bf16,
-                           "peak_source": src}}
+                           "peak_source": src, "path": "drwc_net_forward (conv1 as a GEMM)"},
+            "nn_served_stage": {**served_nn, "peak_tflops": bf16,
+                                "frac": served_nn["tflops"] / bf16, "peak_source": src,
+                                "note": "server network stage incl. voxelisation and sampling"}}
 
 
 def serving_section(ctx, args, net):

@@ -385,32 +385,38 @@ __global__ void __launch_bounds__(256, 4) sv_voxelise_kernel(SvArgs A, int bucke
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.stats + SV_NET_ROWS, (unsigned long long)na);
 }
 
-// One CTA (256 threads) per network row: draw from the prediction, or route
-// the hop to the FDM bucket of its job.
+// Weight of panel q of a network row: the softmax numerator exp(o_q - max)
+// of the Poisson head, or |g_q| (scale removed) of the gradient head.
+DRWC_DEV double sv_weight(const float* r, int q, bool first, float mx) {
+    return first ? fabs((double)r[q] / (double)kGradScale) : (double)__expf(r[q] - mx);
+}
+
+// One warp per network row: draw from the prediction (FP64 running sums over
+// per-lane chunks of the 6N^2 panels, scanned across the warp; the lane whose
+// chunk holds the target walks it), or route the hop to the FDM bucket.
 template <int N>
 __global__ void __launch_bounds__(256) sv_sample_kernel(SvArgs A, int bucket) {
-    constexpr int M = 6 * N * N, NT = 256;
+    constexpr int M = 6 * N * N, CH = (M + 31) / 32;
     const int ldo = A.out_row[bucket], ldg = A.grad_row[bucket];
     const float* __restrict__ Ob = A.O[bucket];
     const float* __restrict__ Gb = A.Gh[bucket];
-    __shared__ double wv[M];
-    __shared__ double red[2 * (NT / 32) + 16];
-    __shared__ int route;
+    const int lane = threadIdx.x & 31;
+    const int warps = (int)(blockDim.x >> 5) * (int)gridDim.x;
     const int na = (int)A.cnt[4 * bucket];
     unsigned long long my_net = 0;
-    for (int row = blockIdx.x; row < na; row += gridDim.x) {
+    for (int row = blockIdx.x * (int)(blockDim.x >> 5) + (threadIdx.x >> 5); row < na;
+         row += warps) {
         const int slot = A.alist[bucket][row];
         const SvJob& J = A.jobs[A.st.job[slot]];
         const long long w = A.st.walk[slot];
         const int h = A.st.hops[slot];
         const bool first = h == 0;
-        if (threadIdx.x == 0) {
+        int route = 0;
+        if (lane == 0) {
             const float conf = Ob[(size_t)row * ldo + M];
             const bool audit =
                 philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 2).x < (double)A.audit_frac;
-            const bool fallback = conf > A.conf_thresh;
-            route = 0;
-            if (audit || fallback) {
+            if (audit || conf > A.conf_thresh) {
                 const unsigned idx = atomicAdd(&A.cnt[4 * bucket + 2], 1u);
                 A.blist[bucket][idx] = slot;
                 A.bkind[bucket][idx] = (audit ? 1 : 0) | (row << 1);
@@ -418,42 +424,59 @@ __global__ void __launch_bounds__(256) sv_sample_kernel(SvArgs A, int bucket) {
                 atomicAdd(A.stats + (audit ? SV_AUDITS : SV_FALLBACKS), 1ull);
             }
         }
-        __syncthreads();
-        if (route) { __syncthreads(); continue; }
-        double tot = 0.0;
-        int b;
-        if (first) {
-            const float* g = Gb + (size_t)A.st.grow[slot] * ldg;
-            for (int q = threadIdx.x; q < M; q += NT) wv[q] = (double)g[q] / (double)kGradScale;
-            __syncthreads();
-            const double u = philox_uniform2(J.W.seed, (uint64_t)w, 0, 1).y;
-            b = cta_sample<NT>(wv, M, true, u, red, &tot);
-        } else {
-            const float* o = Ob + (size_t)row * ldo;
-            float mx = -1e30f;
-            for (int q = threadIdx.x; q < M; q += NT) mx = fmaxf(mx, o[q]);
-            for (int s = 16; s > 0; s >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, s));
-            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-            __syncthreads();
-            float m = (float)red[0];
-            for (int q = 1; q < NT / 32; ++q) m = fmaxf(m, (float)red[q]);
-            __syncthreads();
-            for (int q = threadIdx.x; q < M; q += NT) wv[q] = (double)__expf(o[q] - m);
-            __syncthreads();
-            const double u = philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 0).x;
-            b = cta_sample<NT>(wv, M, false, u, red, &tot);
+        if (__shfl_sync(0xffffffffu, route, 0)) continue;
+        const float* r = first ? Gb + (size_t)A.st.grow[slot] * ldg : Ob + (size_t)row * ldo;
+        float mx = 0.f;
+        if (!first) {
+            mx = -1e30f;
+            for (int q = lane; q < M; q += 32) mx = fmaxf(mx, r[q]);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         }
-        if (threadIdx.x == 0) {
-            if (b < 0) {
+        const int q0 = min(lane * CH, M), q1 = min(q0 + CH, M);
+        double sum = 0.0;
+        int last = -1;
+        for (int q = q0; q < q1; ++q) {
+            const double v = sv_weight(r, q, first, mx);
+            sum += v;
+            if (v > 0.0) last = q;
+        }
+        double incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double n = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += n;
+        }
+        const double tot = __shfl_sync(0xffffffffu, incl, 31);
+        int lastall = last;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lastall = max(lastall, __shfl_xor_sync(0xffffffffu, lastall, o));
+        const double u = first ? philox_uniform2(J.W.seed, (uint64_t)w, 0, 1).y
+                               : philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 0).x;
+        const double target = u * tot;
+        int pick = 0x7fffffff;
+        if (sum > 0.0 && incl > target) {
+            double run = incl - sum;
+            for (int q = q0; q < q1; ++q) {
+                const double v = sv_weight(r, q, first, mx);
+                run += v;
+                if (run > target && v > 0.0) { pick = q; break; }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) pick = min(pick, __shfl_xor_sync(0xffffffffu, pick, o));
+        const int bsel = pick == 0x7fffffff ? lastall : pick;
+        if (lane == 0) {
+            if (bsel < 0) {
                 sv_finish(A, slot, -1);  // no transition possible: the walk is lost
             } else {
                 const double a = A.st.a[slot];
                 double loc[3], mv[3];
-                locate_f64(N, b, loc);
+                locate_f64(N, bsel, loc);
                 if (first) {
                     unrotate(rot_of_code(A.st.code[slot]), loc, mv);
-                    A.st.omega[slot] =
-                        first_hop_weight(J.G, A.st.sgn[slot], A.st.epsw[slot], tot, wv[b], a);
+                    A.st.omega[slot] = first_hop_weight(J.G, A.st.sgn[slot], A.st.epsw[slot], tot,
+                                                        (double)r[bsel] / (double)kGradScale, a);
                 } else {
                     mv[0] = loc[0]; mv[1] = loc[1]; mv[2] = loc[2];
                 }
@@ -464,9 +487,9 @@ __global__ void __launch_bounds__(256) sv_sample_kernel(SvArgs A, int bucket) {
             }
             my_net += 1;
         }
-        __syncthreads();
     }
-    if (threadIdx.x == 0 && my_net) {
+    // per-warp counts
+    if (lane == 0 && my_net) {
         atomicAdd(A.stats + SV_NET_HOPS, my_net);
         atomicAdd(A.stats + SV_HOPS, my_net);
     }

@@ -28,8 +28,7 @@ namespace drwc {
 constexpr int kUmmaM = 128;
 constexpr int kUmmaThreads = 128;                // threads of a GEMM-tile CTA
 constexpr int kUmmaBK = 64;                      // K per shared-memory stage (4 MMAs)
-constexpr uint32_t kWaitTicks = 1000000;         // try_wait suspend hint (ns)
-constexpr int kWaitRounds = 20000;               // => bounded wait of about 20 s
+constexpr long long kWaitCycles = 4000000000LL;  // bounded wait: about 2 s of SM clock
 
 DRWC_DEV uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -60,21 +59,25 @@ DRWC_DEV void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
 
-// Bounded wait on phase `parity`; returns false on timeout.
+// Bounded wait on phase `parity`; returns false on timeout. try_wait without
+// a suspend-time hint returns as soon as the phase completes (or after a
+// short system-defined slice), so the loop reacts at once; the cycle count
+// bounds the total.
 DRWC_DEV bool mbar_wait(uint64_t* bar, uint32_t parity) {
     const uint32_t a = smem_u32(bar);
-    for (int round = 0; round < kWaitRounds; ++round) {
+    const long long t0 = clock64();
+    for (;;) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
             "selp.u32 %0, 1, 0, p;\n\t}"
             : "=r"(done)
-            : "r"(a), "r"(parity), "r"(kWaitTicks)
+            : "r"(a), "r"(parity)
             : "memory");
         if (done) return true;
+        if (clock64() - t0 > kWaitCycles) return false;
     }
-    return false;
 }
 
 DRWC_DEV void umma_fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
