@@ -36,6 +36,7 @@
 #include "host.cuh"
 #include "nn.cuh"
 #include "umma_launch.cuh"
+#include "umma_tma.cuh"
 
 namespace drwc {
 
@@ -568,10 +569,16 @@ static int net_heads(drwc_net* n, int rows, const int* rowmap, float* O, float* 
     const int kNP = n->np, kDecRows = n->dec, kFeat = n->feat;
     int rc = DRWC_OK;
     if (O) {
-        rc = launch_umma<128>(ctx, rows, kDecRows, kFeat,
-                              RowsBf16{n->a3, rows, kFeat, kFeat, rowmap},
-                              RowsBf16{n->pb + n->L.wd, kDecRows, kFeat, kFeat, nullptr},
-                              EpiF32{O, n->p + n->L.bd, kDecRows, kDecRows, rowmap}, n->err);
+        rc = rowmap ? DRWC_ERR_INVALID
+                    : launch_umma_tma<128>(ctx, rows, nullptr, 1, kDecRows, kFeat, n->a3, kFeat,
+                                           n->pb + n->L.wd, kFeat,
+                                           EpiF32{O, n->p + n->L.bd, kDecRows, kDecRows, nullptr},
+                                           n->err);
+        if (rc == DRWC_ERR_INVALID)
+            rc = launch_umma<128>(ctx, rows, kDecRows, kFeat,
+                                  RowsBf16{n->a3, rows, kFeat, kFeat, rowmap},
+                                  RowsBf16{n->pb + n->L.wd, kDecRows, kFeat, kFeat, nullptr},
+                                  EpiF32{O, n->p + n->L.bd, kDecRows, kDecRows, rowmap}, n->err);
         if (rc) return rc;
     }
     if (G && rows_g > 0) {
@@ -624,10 +631,14 @@ static int net_forward_dyn_t(drwc_net* n, int Bmax, const unsigned* nrows, const
                              RowsBf16{pb + n->L.w3, 64, 27 * 32, 27 * 32, nullptr},
                              EpiReluBf16{n->a3, n->p + n->L.b3, 64}, n->err);
     if (rc) return rc;
-    rc = launch_umma_dyn<128>(ctx, Bmax, nrows, 1, S::DEC, S::FEAT,
-                              RowsBf16{n->a3, Bmax, S::FEAT, S::FEAT, nullptr},
-                              RowsBf16{n->pb + n->L.wd, S::DEC, S::FEAT, S::FEAT, nullptr},
+    rc = launch_umma_tma<128>(ctx, Bmax, nrows, 1, S::DEC, S::FEAT, n->a3, S::FEAT,
+                              n->pb + n->L.wd, S::FEAT,
                               EpiF32{O, n->p + n->L.bd, S::DEC, S::DEC, nullptr}, n->err);
+    if (rc == DRWC_ERR_INVALID)
+        rc = launch_umma_dyn<128>(ctx, Bmax, nrows, 1, S::DEC, S::FEAT,
+                                  RowsBf16{n->a3, Bmax, S::FEAT, S::FEAT, nullptr},
+                                  RowsBf16{n->pb + n->L.wd, S::DEC, S::FEAT, S::FEAT, nullptr},
+                                  EpiF32{O, n->p + n->L.bd, S::DEC, S::DEC, nullptr}, n->err);
     if (rc) return rc;
     return launch_umma_dyn<128>(ctx, Bmax, nrows_g, 1, S::NP, S::FEAT,
                                 RowsBf16{n->a3, Bmax, S::FEAT, S::FEAT, gmap},

@@ -6,6 +6,7 @@
 
 #include "host.cuh"
 #include "umma.cuh"
+#include "umma_tma.cuh"
 
 namespace drwc {
 
@@ -80,6 +81,10 @@ DRWC_API int drwc_gemm_bf16(drwc_ctx* ctx, int M, int N, int K, const void* A, i
     RowLoader lb{(const __nv_bfloat16*)B, N, K, ldb};
     StoreF32 st{C, bias, N, ldc, act};
     constexpr int BN = 128;
+    // TMA-fed, warp-specialised tiles when the operands allow it
+    const int rt = launch_umma_tma<BN>(ctx, M, nullptr, 1, N, K, (const __nv_bfloat16*)A, lda,
+                                       (const __nv_bfloat16*)B, ldb, st, err_flag);
+    if (rt != DRWC_ERR_INVALID) return rt;
     static bool attr = false;
     if (!attr) {
         DRWC_CUDA_TRY(cudaFuncSetAttribute(gemm_bf16_kernel<BN>,
