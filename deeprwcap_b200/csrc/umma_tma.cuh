@@ -5,13 +5,13 @@
 // A CTA of 192 threads walks output tiles (128 x BN) blockIdx.x, +gridDim.x,
 // ... in m-fastest order:
 //   warp 0 (one thread)  producer: for every K stage of 64, arms the stage's
-//                        "full" mbarrier with the byte count and issues
-//                        2D TMA loads (cp.async.bulk.tensor, no multicast) of
-//                        8-column boxes of A (128 rows) and B (BN rows), which
-//                        land in the canonical no-swizzle K-major layout
-//                        (8-row core matrices 128 B apart, K halves rows x 16 B
-//                        apart); it waits on the stage's "empty" mbarrier
-//                        before reusing it;
+//                        "full" mbarrier with the byte count and issues one
+//                        2D TMA load (cp.async.bulk.tensor, no multicast) per
+//                        operand: a box of 64 columns (128 B) x 128 rows of A
+//                        and x BN rows of B with the 128-byte swizzle, i.e.
+//                        the K-major SWIZZLE_128B layout the tensor cores read
+//                        (8-row atoms of 1024 B); it waits on the stage's
+//                        "empty" mbarrier before reusing it;
 //   warp 1 (one thread)  MMA issuer: waits "full", issues four
 //                        tcgen05.mma.kind::f16 (K = 16 each) into one of two
 //                        TMEM accumulators, commits to "empty" (the stage is
@@ -58,6 +58,19 @@ DRWC_DEV void mbar_arrive_expect(uint64_t* bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
                  "r"(bytes)
                  : "memory");
+}
+
+// Shared-memory descriptor of a K-major SWIZZLE_128B operand: 8-row atoms
+// 1024 B apart (stride byte offset), layout type 2 in bits 61-63; a K step
+// of 16 BF16 advances the start address by 32 B inside the 128-byte rows.
+DRWC_DEV uint64_t umma_smem_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);      // start address >> 4
+    d |= (uint64_t)1u << 16;                       // leading byte offset (unused here) = 16 B
+    d |= (uint64_t)((1024u >> 4) & 0x3FFFu) << 32; // stride byte offset: 1024 B between atoms
+    d |= (uint64_t)1u << 46;                       // descriptor version 1
+    d |= (uint64_t)2u << 61;                       // layout: SWIZZLE_128B
+    return d;
 }
 
 DRWC_DEV void mbar_arrive(uint64_t* bar) {
@@ -135,14 +148,8 @@ __global__ void __launch_bounds__(kTmaThreads) umma_tma_kernel(const __grid_cons
                     if (r > 0 && !mbar_wait(&empty[s], (r - 1) & 1)) { fail(); break; }
                     mbar_arrive_expect(&full[s], SA + SB);
                     const uint32_t fb = smem_u32(&full[s]);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        tma_load_2d(smem_u32(sA + s * SA + j * kUmmaM * 16), &ta, kt * kUmmaBK + 8 * j,
-                                    m0, fb);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                        tma_load_2d(smem_u32(sB + s * SB + j * BN * 16), &tb, kt * kUmmaBK + 8 * j,
-                                    n0, fb);
+                    tma_load_2d(smem_u32(sA + s * SA), &ta, kt * kUmmaBK, m0, fb);
+                    tma_load_2d(smem_u32(sB + s * SB), &tb, kt * kUmmaBK, n0, fb);
                     *issued = g + 1;
                 }
             }
@@ -164,10 +171,8 @@ __global__ void __launch_bounds__(kTmaThreads) umma_tma_kernel(const __grid_cons
                     const int k0 = kt * kUmmaBK;
                     const int ksteps = min(kUmmaBK, K - k0 + 15) / 16;
                     for (int ks = 0; ks < ksteps && ks < kUmmaBK / 16; ++ks) {
-                        const uint64_t da = umma_smem_desc(smem_u32(sA + s * SA + 2 * ks * kUmmaM * 16),
-                                                           kUmmaM * 16, 128);
-                        const uint64_t db = umma_smem_desc(smem_u32(sB + s * SB + 2 * ks * BN * 16),
-                                                           BN * 16, 128);
+                        const uint64_t da = umma_smem_desc_sw128(smem_u32(sA + s * SA + 32 * ks));
+                        const uint64_t db = umma_smem_desc_sw128(smem_u32(sB + s * SB + 32 * ks));
                         umma_bf16(d, da, db, umma_idesc_bf16<BN>(), (kt > 0 || ks > 0) ? 1u : 0u);
                     }
                     umma_commit(&empty[s]);
@@ -232,7 +237,8 @@ inline TensorMapEncodeFn tensor_map_encoder() {
 }
 
 // 2D map of a row-major BF16 matrix [rows, cols] (leading dimension ld
-// elements): boxes of 8 columns x box_rows rows, zero fill outside.
+// elements): boxes of 64 columns (128 B) x box_rows rows with the 128-byte
+// swizzle, zero fill outside.
 inline bool tensor_map_rows(CUtensorMap* map, const void* base, int64_t rows, int64_t cols,
                             int64_t ld, int box_rows) {
     TensorMapEncodeFn enc = tensor_map_encoder();
@@ -240,10 +246,10 @@ inline bool tensor_map_rows(CUtensorMap* map, const void* base, int64_t rows, in
         return false;
     const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
-    const cuuint32_t box[2] = {8, (cuuint32_t)box_rows};
+    const cuuint32_t box[2] = {(cuuint32_t)kUmmaBK, (cuuint32_t)box_rows};
     const cuuint32_t estr[2] = {1, 1};
     return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
-               box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
            CUDA_SUCCESS;
 }
