@@ -1,6 +1,11 @@
 """Train the learned transition network on FDM data the engine generates.
 
     python -m deeprwcap_b200.train [--N 16|21|23] [--samples 1048576] [--epochs 3] [--out PATH]
+        [--data poisson.bin gradient.bin]
+
+With --data the training cubes come from ggft training-data files (the
+reference generator's, or ones deeprwcap_b200.ggft_dataset wrote); the target
+a file does not hold is solved by the engine. Otherwise:
 
 Training data (all on the device):
   * transition cubes logged from real walks (drwc_frw_harvest) on the
@@ -168,10 +173,16 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", type=str, default=str(DEFAULT_CKPT))
     ap.add_argument("--N", type=int, default=16, choices=[16, 21, 23])
+    ap.add_argument("--data", nargs="*", default=None,
+                    help="ggft .bin files (poisson.bin / gradient.bin) instead of engine-generated cubes")
     a = ap.parse_args()
     import torch
     ctx = engine.default_context(0)
-    X, T, TG = build_dataset(ctx, a.samples, seed=a.seed, N=a.N)
+    if a.data:
+        from . import ggft_dataset
+        X, T, TG = ggft_dataset.training_arrays(ctx, a.data, a.N)
+    else:
+        X, T, TG = build_dataset(ctx, a.samples, seed=a.seed, N=a.N)
     Xt, Tt, TGt, Xv, Tv, TGv = split(X, T, TG, seed=a.seed)
     net = engine.Net(seed=a.seed + 1, ctx=ctx, N=a.N)
     before = evaluate(net, Xv, Tv, TGv)
