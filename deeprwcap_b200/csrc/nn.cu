@@ -21,7 +21,11 @@
 // (tap, input channel) with the channel fastest, so an 8-wide K chunk of a
 // conv is one 16-byte load of 8 channels at one tap. The backward pass uses
 // the same tile: weight gradients as split-K GEMMs over (batch x position),
-// input gradients as transposed-convolution gathers.
+// input gradients as transposed-convolution gathers. Inference (the forward
+// entry points, the learned walker, the server) runs conv1 and conv2 fused
+// in one CTA per group of cubes (stem.cuh), so A1 never reaches global
+// memory; training runs every layer as a GEMM and keeps A1 for the backward
+// pass.
 //
 // The architecture follows the learned-transition design of DeepRWCap
 // (training_pytorch/src/architecture.py: small 3-D conv encoders on the
@@ -35,6 +39,7 @@
 
 #include "host.cuh"
 #include "nn.cuh"
+#include "stem.cuh"
 #include "umma_launch.cuh"
 #include "umma_tma.cuh"
 
@@ -590,10 +595,68 @@ static int net_heads(drwc_net* n, int rows, const int* rowmap, float* O, float* 
     return rc;
 }
 
+// Inference stem: the cubes of X (BF16 [B][N^3]) through conv1 and conv2 on
+// the tensor cores inside one CTA per group of cubes (stem.cuh), conv2's
+// activations to a2. Training keeps the per-layer GEMMs: its backward pass
+// needs conv1's activations.
+template <int N>
+__global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
+    stem_cubes_kernel(const bf16* __restrict__ X, int B, NetStem W) {
+    using D = StemDims<N>;
+    extern __shared__ __align__(1024) unsigned char stem_smem[];
+    if ((int)blockIdx.x * D::CUBES >= B) return;
+    Stem<N> st{stem_smem};
+    st.begin(W);
+    bool ok = true;
+    for (int grp = blockIdx.x; ok && grp * D::CUBES < B; grp += gridDim.x) {
+        const int g0 = grp * D::CUBES, nc = min(D::CUBES, B - g0);
+        for (int cb = 0; ok && cb < nc; ++cb) {
+            const bf16* src = X + (size_t)(g0 + cb) * (N * N * N);
+            bf16* xs = st.xs();
+            for (int v = threadIdx.x; v < N * N * N; v += blockDim.x) xs[v] = src[v];
+            __syncthreads();
+            ok = st.conv1(cb, W.err);
+        }
+        if (ok) ok = st.conv2(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err);
+    }
+    st.end();
+}
+
+// Encoder for inference: fused stem, then conv3 as a tile GEMM.
+template <int N>
+static int net_infer_encode_t(drwc_net* n, int B, const bf16* X) {
+    using S = NetDims<N>;
+    using D = StemDims<N>;
+    drwc_ctx* ctx = n->ctx;
+    static int per_sm = 0;  // resident stem CTAs per SM (one instantiation per N)
+    if (!per_sm) {
+        DRWC_CUDA_TRY(cudaFuncSetAttribute(stem_cubes_kernel<N>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, D::BYTES));
+        DRWC_CUDA_TRY(cudaFuncSetAttribute(stem_cubes_kernel<N>,
+                                           cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+        DRWC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, stem_cubes_kernel<N>,
+                                                                    D::NT, D::BYTES));
+        if (per_sm < 1) { per_sm = 0; return DRWC_ERR_INVALID; }
+    }
+    const int groups = (B + D::CUBES - 1) / D::CUBES;
+    const int resident = std::max(per_sm, D::CTAS) * ctx->sm_count;
+    stem_cubes_kernel<N><<<std::min(groups, resident), D::NT, D::BYTES, ctx->stream>>>(
+        X, B, net_stem_operands(n));
+    int rc = launch_check(ctx);
+    if (rc) return rc;
+    return launch_umma<64>(ctx, B * S::P4, 64, 27 * 32, ConvGather<S::D3, 32>{n->a2, B * S::P4},
+                           RowsBf16{n->pb + n->L.w3, 64, 27 * 32, 27 * 32, nullptr},
+                           EpiReluBf16{n->a3, n->p + n->L.b3, 64}, n->err);
+}
+
+static int net_infer_encode(drwc_net* n, int B, const bf16* X) {
+    return net_dispatch(n->N, [&](auto nc) { return net_infer_encode_t<decltype(nc)::value>(n, B, X); });
+}
+
 int net_forward_locked(drwc_net* n, int B, const bf16* X, float* O, float* G) {
     int rc = net_reserve(n, B);
     if (rc) return rc;
-    rc = net_encode(n, B, X);
+    rc = net_infer_encode(n, B, X);
     if (rc) return rc;
     return net_heads(n, B, nullptr, O, G, nullptr, B);
 }
@@ -602,7 +665,7 @@ int net_forward_mapped(drwc_net* n, int B, const bf16* X, float* O, float* G, co
                        int rows_g) {
     int rc = net_reserve(n, B);
     if (rc) return rc;
-    rc = net_encode(n, B, X);
+    rc = net_infer_encode(n, B, X);
     if (rc) return rc;
     return net_heads(n, B, nullptr, O, G, gmap, rows_g);
 }
@@ -614,18 +677,18 @@ static int net_forward_dyn_t(drwc_net* n, int Bmax, const unsigned* nrows, const
     drwc_ctx* ctx = n->ctx;
     const bf16* pb = n->pb;
     int rc = DRWC_OK;
-    if (X) {  // else conv1's activations are already in a1 (net_conv1_operands)
+    if (X) {  // else conv2's activations are already in a2 (net_stem_operands)
         rc = launch_umma_dyn<16>(ctx, Bmax * S::P2, nrows, S::P2, 16, 27,
                                  ConvGather<S::D1, 1>{X, Bmax * S::P2},
                                  RowsBf16{pb + n->L.w1, 16, 27, 27, nullptr},
                                  EpiReluBf16{n->a1, n->p + n->L.b1, 16}, n->err);
         if (rc) return rc;
+        rc = launch_umma_dyn<32>(ctx, Bmax * S::P3, nrows, S::P3, 32, 27 * 16,
+                                 ConvGather<S::D2, 16>{n->a1, Bmax * S::P3},
+                                 RowsBf16{pb + n->L.w2, 32, 27 * 16, 27 * 16, nullptr},
+                                 EpiReluBf16{n->a2, n->p + n->L.b2, 32}, n->err);
+        if (rc) return rc;
     }
-    rc = launch_umma_dyn<32>(ctx, Bmax * S::P3, nrows, S::P3, 32, 27 * 16,
-                             ConvGather<S::D2, 16>{n->a1, Bmax * S::P3},
-                             RowsBf16{pb + n->L.w2, 32, 27 * 16, 27 * 16, nullptr},
-                             EpiReluBf16{n->a2, n->p + n->L.b2, 32}, n->err);
-    if (rc) return rc;
     rc = launch_umma_dyn<64>(ctx, Bmax * S::P4, nrows, S::P4, 64, 27 * 32,
                              ConvGather<S::D3, 32>{n->a2, Bmax * S::P4},
                              RowsBf16{pb + n->L.w3, 64, 27 * 32, 27 * 32, nullptr},
@@ -656,8 +719,9 @@ int net_forward_dyn(drwc_net* n, int Bmax, const unsigned* nrows, const bf16* X,
 
 int net_reserve_rows(drwc_net* n, int B) { return net_reserve(n, B); }
 
-NetConv1 net_conv1_operands(drwc_net* n) {
-    return NetConv1{n->pb + n->L.w1, n->p + n->L.b1, n->a1};
+NetStem net_stem_operands(drwc_net* n) {
+    return NetStem{n->pb + n->L.w1, n->p + n->L.b1, n->pb + n->L.w2, n->p + n->L.b2, n->a2,
+                   n->err};
 }
 
 void net_hold(drwc_net* n, int delta) { n->holders += delta; }

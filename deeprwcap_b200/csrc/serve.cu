@@ -41,6 +41,7 @@
 
 #include "geom.cuh"
 #include "nn.cuh"
+#include "stem.cuh"
 
 namespace drwc {
 
@@ -113,7 +114,7 @@ struct SvArgs {
     float* Gh[DRWC_SERVER_MAX_SIZES];
     int out_row[DRWC_SERVER_MAX_SIZES];
     int grad_row[DRWC_SERVER_MAX_SIZES];
-    NetConv1 c1[DRWC_SERVER_MAX_SIZES];  // conv1 runs inside the voxeliser
+    NetStem stem[DRWC_SERVER_MAX_SIZES];  // conv1 and conv2 run inside the voxeliser
     unsigned long long* stats;
     double* audit_kl;                   // [0] sum, [1] count
     double* bsum;
@@ -338,51 +339,53 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
     }
 }
 
-// One CTA (256 threads) per network row: the cube voxelised in shared
-// memory (eps / max eps, BF16) and the network's first layer applied to it,
-// so only conv1's activations reach global memory.
+// Network rows in groups (two cubes at N = 16, one at 21 and 23), one group
+// at a time per CTA: each cube voxelised in shared memory (eps / max eps,
+// BF16) and the network's stem (conv1, conv2) applied to it on the tensor
+// cores there, so only conv2's activations reach global memory.
 template <int N>
-__global__ void __launch_bounds__(256, 4) sv_voxelise_kernel(SvArgs A, int bucket) {
-    constexpr int Do = (N - 1) / 2 + 1;
+__global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
+    sv_stem_kernel(SvArgs A, int bucket) {
+    using D = StemDims<N>;
+    extern __shared__ __align__(1024) unsigned char sv_stem_smem[];
     __shared__ double tco[N];
     __shared__ double pal[kMaxMaterials];
-    __shared__ uint8_t mat[N * N * N];
-    __shared__ __align__(16) __nv_bfloat16 xs[N * N * N];
-    __shared__ float4 w4[27 * 4];
-    __shared__ float b1[16];
     __shared__ VoxScratch<N> vs;
     __shared__ float red[32];
-    centre_offsets<N>(tco);
-    // weights [co][tap] -> tap-major float4 groups of 4 output channels
-    for (int q = threadIdx.x; q < 16 * 27; q += blockDim.x) {
-        const int co = q / 27, tap = q % 27;
-        reinterpret_cast<float*>(w4)[tap * 16 + co] = __bfloat162float(A.c1[bucket].w1[q]);
-    }
-    if (threadIdx.x < 16) b1[threadIdx.x] = A.c1[bucket].b1[threadIdx.x];
     const int na = (int)A.cnt[4 * bucket];
-    int loaded = -1;
-    for (int row = blockIdx.x; row < na; row += gridDim.x) {
-        const int slot = A.alist[bucket][row];
-        const int j = A.st.job[slot];
-        const SvJob& J = A.jobs[j];
-        if (j != loaded) {
-            __syncthreads();
-            for (int v = threadIdx.x; v < J.g.n_mat; v += blockDim.x) pal[v] = J.g.pal[v];
-            loaded = j;
-        }
-        __syncthreads();
-        const bool first = A.st.hops[slot] == 0;
-        const int rot = first ? rot_of_code(A.st.code[slot]) : 0;
-        const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
-        voxelise_net<N>(J.g, c, A.st.a[slot], rot, tco, pal, mat, xs, nullptr, red, vs);
-        if (first && threadIdx.x == 0) {
-            const EpsPalette E{mat, pal, nullptr, nullptr, nullptr, 0};
-            A.st.epsw[slot] = center_diel<N>(E, DRWC_WVTZ);
-        }
-        conv1_cube<N>(xs, w4, b1, A.c1[bucket].a1 + (size_t)row * (Do * Do * Do) * 16);
-        __syncthreads();
-    }
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.stats + SV_NET_ROWS, (unsigned long long)na);
+    if ((int)blockIdx.x * D::CUBES >= na) return;
+    const NetStem& W = A.stem[bucket];
+    centre_offsets<N>(tco);
+    Stem<N> st{sv_stem_smem};
+    st.begin(W);
+    int loaded = -1;
+    bool ok = true;
+    for (int grp = blockIdx.x; ok && grp * D::CUBES < na; grp += gridDim.x) {
+        const int g0 = grp * D::CUBES, nc = min(D::CUBES, na - g0);
+        for (int cb = 0; ok && cb < nc; ++cb) {
+            const int slot = A.alist[bucket][g0 + cb];
+            const int j = A.st.job[slot];
+            const SvJob& J = A.jobs[j];
+            if (j != loaded) {
+                __syncthreads();
+                for (int v = threadIdx.x; v < J.g.n_mat; v += blockDim.x) pal[v] = J.g.pal[v];
+                loaded = j;
+            }
+            __syncthreads();
+            const bool first = A.st.hops[slot] == 0;
+            const int rot = first ? rot_of_code(A.st.code[slot]) : 0;
+            const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
+            voxelise_net<N>(J.g, c, A.st.a[slot], rot, tco, pal, st.mat(), st.xs(), nullptr, red, vs);
+            if (first && threadIdx.x == 0) {
+                const EpsPalette E{st.mat(), pal, nullptr, nullptr, nullptr, 0};
+                A.st.epsw[slot] = center_diel<N>(E, DRWC_WVTZ);
+            }
+            ok = st.conv1(cb, W.err);
+        }
+        if (ok) ok = st.conv2(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err);
+    }
+    st.end();
 }
 
 // Weight of panel q of a network row: the softmax numerator exp(o_q - max)
@@ -739,6 +742,7 @@ struct drwc_server {
     double* d_akl = nullptr;
     SvArgs A{};
     int fdm_grid[DRWC_SERVER_MAX_SIZES] = {};
+    int stem_grid[DRWC_SERVER_MAX_SIZES] = {};
     size_t fdm_smem[DRWC_SERVER_MAX_SIZES] = {};
     double* fdm_sy[DRWC_SERVER_MAX_SIZES] = {};
     float* fdm_ss[DRWC_SERVER_MAX_SIZES] = {};
@@ -787,6 +791,25 @@ static int sv_fdm_setup(drwc_server* v, int b) {
     if (per_sm < 1) return DRWC_ERR_INVALID;
     v->fdm_grid[b] = per_sm * v->ctx->sm_count;
     v->fdm_smem[b] = smem;
+    return DRWC_OK;
+}
+
+// The stem kernel's shared memory and a persistent grid of its resident CTAs.
+template <int N>
+static int sv_stem_setup(drwc_server* v, int b) {
+    using D = StemDims<N>;
+    DRWC_CUDA_TRY(cudaFuncSetAttribute(sv_stem_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       D::BYTES));
+    // all of the unified L1 as shared memory, or the SM holds one CTA fewer
+    DRWC_CUDA_TRY(cudaFuncSetAttribute(sv_stem_kernel<N>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       100));
+    int per_sm = 0;
+    DRWC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sv_stem_kernel<N>, D::NT,
+                                                                D::BYTES));
+    if (per_sm < 1) return DRWC_ERR_INVALID;
+    // at least the CTAs per SM the kernel is built for (the grid loops over
+    // groups, so an estimate on the low side costs nothing)
+    v->stem_grid[b] = std::max(per_sm, D::CTAS) * v->ctx->sm_count;
     return DRWC_OK;
 }
 
@@ -883,7 +906,7 @@ static int sv_step(drwc_server* v, int k) {
         rc = dispatch_N(v->o.sizes[b], [&](auto nc) -> int {
             constexpr int NC = decltype(nc)::value;
             if constexpr (NC == 16 || NC == 21 || NC == 23) {
-                sv_voxelise_kernel<NC><<<g2, 256, 0, s>>>(A, b);
+                sv_stem_kernel<NC><<<v->stem_grid[b], StemDims<NC>::NT, StemDims<NC>::BYTES, s>>>(A, b);
                 int r = launch_check(ctx);
                 if (r) return r;
                 r = net_forward_dyn(v->bnet[b], A.S, A.cnt + 4 * b, nullptr, A.O[b], A.Gh[b],
@@ -1448,17 +1471,16 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts,
         }
         for (int b = 0; !rc && b < o.n_sizes; ++b) {
             if (!v->bnet[b]) continue;
-            // room for four voxeliser CTAs per SM
-            cudaError_t e = cudaSuccess;
-            if (o.sizes[b] == 16)
-                e = cudaFuncSetAttribute(sv_voxelise_kernel<16>, cudaFuncAttributePreferredSharedMemoryCarveout, 50);
-            else if (o.sizes[b] == 21)
-                e = cudaFuncSetAttribute(sv_voxelise_kernel<21>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-            else if (o.sizes[b] == 23)
-                e = cudaFuncSetAttribute(sv_voxelise_kernel<23>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-            if (e != cudaSuccess) rc = DRWC_ERR_CUDA;
+            rc = dispatch_N(o.sizes[b], [&](auto nc) -> int {
+                constexpr int NC = decltype(nc)::value;
+                if constexpr (NC == 16 || NC == 21 || NC == 23) {
+                    return sv_stem_setup<NC>(v.get(), b);
+                } else {
+                    return DRWC_ERR_INVALID;
+                }
+            });
             if (!rc) rc = net_reserve_rows(v->bnet[b], o.slots);
-            if (!rc) v->A.c1[b] = net_conv1_operands(v->bnet[b]);  // a1 as reserved for `slots` rows
+            if (!rc) v->A.stem[b] = net_stem_operands(v->bnet[b]);  // a2 as reserved for `slots` rows
         }
         if (!rc) rc = sv_alloc(v.get());
         if (!rc) rc = sv_tables(v.get());

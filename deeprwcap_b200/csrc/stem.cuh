@@ -1,0 +1,281 @@
+// Stem of the learned transition network (conv1 and conv2) on the tensor
+// cores, inside the CTA that voxelised the cube, so neither the voxel grid
+// nor conv1's activations leave shared memory.
+//
+// A group is the set of cubes whose conv2 rows fill one 128-row MMA tile
+// (two cubes at N = 16: 4^3 = 64 rows each) or a single cube (N = 21, 23:
+// 6^3 = 216 rows over two tiles). Per cube, conv1 (1 -> 16 channels, 3^3,
+// stride 2, zero padding) is an implicit GEMM [D2^3 x 32] x [32 x 16]: the
+// threads write the im2col rows of up to four 128-row M tiles (taps 27..31
+// zero) into a staging area in the canonical K-major no-swizzle layout, one
+// thread issues two tcgen05.mma (K = 16) per tile into its own 16 TMEM
+// columns, and the epilogue (tcgen05.ld, bias, ReLU, BF16) writes the rows
+// into the group's conv1 activations [cube][D2^3][16] in shared memory.
+// conv2 (16 -> 32 channels) then gathers its im2col rows from there, nine
+// taps (K steps) per staging fill, accumulates each 128-row tile in 32 TMEM
+// columns and writes its activations [row][32] (BF16, channels last) to
+// global memory, where the tile GEMMs of conv3 and the heads read them.
+//
+// Operands are the BF16 values the stand-alone convolution GEMMs read and
+// each MMA sums in FP32, so a row's result does not depend on the other rows
+// of its tile or on how rows are grouped. Phases are serialised inside the
+// CTA (fill, barrier, MMA, bounded mbarrier wait, epilogue); co-resident CTAs
+// overlap one another's phases. A wait that runs out raises the error flag,
+// every thread leaves at the next barrier, and the CTA still waits (bounded)
+// for its MMAs before it frees its tensor memory.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "nn.cuh"
+#include "umma.cuh"
+
+namespace drwc {
+
+template <int N>
+struct StemDims {
+    static constexpr int D2 = (N - 1) / 2 + 1, P2 = D2 * D2 * D2;  // conv1 output
+    static constexpr int D3 = (D2 - 1) / 2 + 1, P3 = D3 * D3 * D3;  // conv2 output
+    static constexpr int CUBES = P3 <= 64 ? kUmmaM / P3 : 1;        // cubes per group
+    static_assert(CUBES == 1 || CUBES * P3 == kUmmaM, "a group's conv2 rows fill whole tiles");
+    static constexpr int ROWS2 = CUBES * P3;                         // conv2 rows per group
+    static constexpr int MT2 = (ROWS2 + kUmmaM - 1) / kUmmaM;       // conv2 M tiles
+    static constexpr int MT1 = (P2 + kUmmaM - 1) / kUmmaM;          // conv1 M tiles per cube
+    static constexpr int R1 = 4;     // conv1 M tiles per MMA batch (16 TMEM columns each)
+    static constexpr int TAPS = 9;   // conv2 taps (K steps of 16) per MMA batch
+    static constexpr int NT = N <= 16 ? 256 : 512;
+    static constexpr int CTAS = N <= 16 ? 2 : 1;
+    static_assert(MT2 <= 2, "conv2 accumulators: columns 64..127");
+    // dynamic shared memory (bytes); every operand block is 1024-aligned
+    static constexpr int OPA = R1 * 8192 > TAPS * 4096 ? R1 * 8192 : TAPS * 4096;
+    static constexpr int W2B = 27 * 32 * 32;  // conv2 weights: 27 K steps x 32 rows x 32 B
+    static constexpr int W1B = 2 * 16 * 32;   // conv1 weights: 2 K steps x 16 rows x 32 B
+    static constexpr int A1B = CUBES * P2 * 32;
+    static constexpr int XSB = (N * N * N * 2 + 15) / 16 * 16;
+    static constexpr int MATB = (N * N * N + 15) / 16 * 16;
+    static constexpr int O_W2 = OPA, O_W1 = O_W2 + W2B, O_A1 = O_W1 + W1B, O_XS = O_A1 + A1B,
+                         O_MAT = O_XS + XSB, O_B1 = O_MAT + MATB, O_B2 = O_B1 + 16 * 4,
+                         O_BAR = O_B2 + 32 * 4, O_TSLOT = O_BAR + 8, O_ABORT = O_TSLOT + 4,
+                         BYTES = (O_ABORT + 4 + 15) / 16 * 16;
+    static constexpr uint32_t TCOLS = 128;  // conv1: 4 x 16 columns; conv2: from column 64
+};
+
+// 16 columns of the warp's 32 TMEM lanes.
+DRWC_DEV void tmem_ld16(uint32_t taddr, float* v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ReLU(v + b) of 16 channels as BF16, two 16-byte stores.
+DRWC_DEV void stem_store16(const float* v, const float* b, __nv_bfloat16* dst) {
+    __align__(16) __nv_bfloat162 o[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        o[q] = __floats2bfloat162_rn(fmaxf(v[2 * q] + b[2 * q], 0.f),
+                                     fmaxf(v[2 * q + 1] + b[2 * q + 1], 0.f));
+    uint4* d = reinterpret_cast<uint4*>(dst);
+    d[0] = reinterpret_cast<const uint4*>(o)[0];
+    d[1] = reinterpret_cast<const uint4*>(o)[1];
+}
+
+template <int N>
+struct Stem {
+    using S = StemDims<N>;
+    unsigned char* sm;
+    uint32_t tmem = 0;
+    uint32_t phase = 0;
+    bool pending = false;  // MMAs committed and not yet seen complete
+
+    DRWC_DEV unsigned char* opa() const { return sm; }
+    DRWC_DEV __nv_bfloat16* xs() const { return reinterpret_cast<__nv_bfloat16*>(sm + S::O_XS); }
+    DRWC_DEV uint8_t* mat() const { return sm + S::O_MAT; }
+    DRWC_DEV __nv_bfloat16* a1(int cube) const {
+        return reinterpret_cast<__nv_bfloat16*>(sm + S::O_A1) + (size_t)cube * S::P2 * 16;
+    }
+    DRWC_DEV const float* b1() const { return reinterpret_cast<const float*>(sm + S::O_B1); }
+    DRWC_DEV const float* b2() const { return reinterpret_cast<const float*>(sm + S::O_B2); }
+    DRWC_DEV uint64_t* bar() const { return reinterpret_cast<uint64_t*>(sm + S::O_BAR); }
+    DRWC_DEV volatile int* abort_flag() const {
+        return reinterpret_cast<volatile int*>(sm + S::O_ABORT);
+    }
+    DRWC_DEV bool aborted() const { return *abort_flag() != 0; }
+
+    // Weights in the canonical K-major layout, biases, barrier, TMEM.
+    DRWC_DEV void begin(const NetStem& w) {
+        const int t = threadIdx.x;
+        for (int e = t; e < 16 * 32; e += blockDim.x) {
+            const int co = e >> 5, k = e & 31;
+            *reinterpret_cast<__nv_bfloat16*>(sm + S::O_W1 + umma_tile_off(co, k, 16)) =
+                k < 27 ? w.w1[co * 27 + k] : __float2bfloat16(0.f);
+        }
+        for (int e = t; e < 32 * 432; e += blockDim.x) {
+            const int co = e / 432, k = e % 432;
+            *reinterpret_cast<__nv_bfloat16*>(sm + S::O_W2 + umma_tile_off(co, k, 32)) =
+                w.w2[co * 432 + k];
+        }
+        if (t < 16) reinterpret_cast<float*>(sm + S::O_B1)[t] = w.b1[t];
+        if (t < 32) reinterpret_cast<float*>(sm + S::O_B2)[t] = w.b2[t];
+        if (t == 0) {
+            mbar_init(bar(), 1);
+            *abort_flag() = 0;
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + S::O_TSLOT);
+        if ((t >> 5) == 0) {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                         ::"r"(smem_u32(tslot)), "r"(S::TCOLS));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        tmem = *tslot;
+    }
+
+    // The staging area is written: make it visible to the tensor cores and
+    // meet at a barrier; false when a wait has run out (every thread agrees).
+    DRWC_DEV bool staged() {
+        umma_fence_proxy_async();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        return !aborted();
+    }
+
+    // After thread 0 committed: wait for the MMAs (bounded).
+    DRWC_DEV void complete(int* err) {
+        pending = true;
+        if (!mbar_wait(bar(), phase)) {
+            *abort_flag() = 1;
+            if (err) atomicExch(err, 1);
+        } else {
+            pending = false;
+        }
+        phase ^= 1;
+        tc_fence_after();
+    }
+
+    // conv1 of the cube in xs() into a1(cube), up to R1 M tiles per batch.
+    DRWC_DEV bool conv1(int cube, int* err) {
+        const __nv_bfloat16* x = xs();
+        const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
+        for (int m0 = 0; m0 < S::MT1; m0 += S::R1) {
+            const int nb = min(S::R1, S::MT1 - m0);
+            for (int it = t; it < nb * kUmmaM; it += S::NT) {
+                const int j = it >> 7, r = it & 127, p = (m0 + j) * kUmmaM + r;
+                uint32_t pk[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) pk[i] = 0u;
+                if (p < S::P2) {
+                    const int pz = p / (S::D2 * S::D2), py = (p / S::D2) % S::D2, px = p % S::D2;
+                    const int z0 = 2 * pz - 1, y0 = 2 * py - 1, x0 = 2 * px - 1;
+#pragma unroll
+                    for (int tap = 0; tap < 27; ++tap) {
+                        const int z = z0 + tap / 9, y = y0 + (tap / 3) % 3, xx = x0 + tap % 3;
+                        const bool in = (unsigned)z < (unsigned)N && (unsigned)y < (unsigned)N &&
+                                        (unsigned)xx < (unsigned)N;
+                        const uint32_t v =
+                            in ? (uint32_t)__bfloat16_as_ushort(x[(z * N + y) * N + xx]) : 0u;
+                        pk[tap >> 1] |= v << (16 * (tap & 1));
+                    }
+                }
+                unsigned char* base = opa() + j * 8192 + (r >> 3) * 256 + (r & 7) * 16;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)  // taps 8c .. 8c + 7: K step c / 2, half c % 2
+                    *reinterpret_cast<uint4*>(base + (c >> 1) * 4096 + (c & 1) * 128) =
+                        make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+            }
+            if (!staged()) return false;
+            if (t == 0) {
+                for (int j = 0; j < nb; ++j)
+                    for (int s = 0; s < 2; ++s)
+                        umma_bf16(tmem + 16 * j,
+                                  umma_smem_desc(smem_u32(opa() + j * 8192 + s * 4096), 128, 256),
+                                  umma_smem_desc(smem_u32(sm + S::O_W1 + s * 512), 128, 256),
+                                  umma_idesc_bf16<16>(), (uint32_t)s);
+                umma_commit(bar());
+            }
+            complete(err);
+            __nv_bfloat16* dst = a1(cube);
+            for (int j = sub; j < nb; j += S::NT / 128) {
+                float v[16];
+                tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 16 * j, v);
+                const int p = (m0 + j) * kUmmaM + 32 * q + lane;
+                if (p < S::P2) stem_store16(v, b1(), dst + (size_t)p * 16);
+            }
+            tc_fence_before();  // the next batch's MMAs overwrite these columns
+        }
+        __syncthreads();  // a1 complete; every thread sees the same abort flag
+        return !aborted();
+    }
+
+    // conv2 of the group's nc cubes (a1(0 .. nc-1)) -> a2 rows [g0 * P3, ..).
+    DRWC_DEV bool conv2(int nc, __nv_bfloat16* __restrict__ a2, int* err) {
+        const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
+        for (int mt = 0; mt < S::MT2; ++mt) {
+            for (int cc = 0; cc < 27 / S::TAPS; ++cc) {
+                for (int it = t; it < 256 * S::TAPS; it += S::NT) {
+                    const int pr = it & 255, ti = it >> 8, r = pr >> 1, h = pr & 1;
+                    const int R = mt * kUmmaM + r, tap = cc * S::TAPS + ti;
+                    uint4 val = make_uint4(0u, 0u, 0u, 0u);
+                    if (R < S::ROWS2) {
+                        const int cube = R / S::P3, p = R % S::P3;
+                        const int pz = p / (S::D3 * S::D3), py = (p / S::D3) % S::D3, px = p % S::D3;
+                        const int z = 2 * pz - 1 + tap / 9, y = 2 * py - 1 + (tap / 3) % 3,
+                                  xx = 2 * px - 1 + tap % 3;
+                        if (cube < nc && (unsigned)z < (unsigned)S::D2 &&
+                            (unsigned)y < (unsigned)S::D2 && (unsigned)xx < (unsigned)S::D2)
+                            val = *reinterpret_cast<const uint4*>(
+                                a1(cube) + (size_t)((z * S::D2 + y) * S::D2 + xx) * 16 + 8 * h);
+                    }
+                    *reinterpret_cast<uint4*>(opa() + ti * 4096 + (r >> 3) * 256 + h * 128 +
+                                              (r & 7) * 16) = val;
+                }
+                if (!staged()) return false;
+                if (t == 0) {
+                    for (int ti = 0; ti < S::TAPS; ++ti)
+                        umma_bf16(tmem + 64 + 32 * mt,
+                                  umma_smem_desc(smem_u32(opa() + ti * 4096), 128, 256),
+                                  umma_smem_desc(smem_u32(sm + S::O_W2 + (cc * S::TAPS + ti) * 1024),
+                                                 128, 256),
+                                  umma_idesc_bf16<32>(), (cc | ti) ? 1u : 0u);
+                    umma_commit(bar());
+                }
+                complete(err);
+            }
+        }
+        // epilogue: (tile, 16-column half) tasks over the warp quarters
+        for (int task = sub; task < 2 * S::MT2; task += S::NT / 128) {
+            const int mt = task >> 1, half = task & 1;
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 64 + 32 * mt + 16 * half, v);
+            const int R = mt * kUmmaM + 32 * q + lane;
+            if (R < S::ROWS2 && R / S::P3 < nc)
+                stem_store16(v, b2() + 16 * half, a2 + (size_t)R * 32 + 16 * half);
+        }
+        tc_fence_before();
+        __syncthreads();
+        return !aborted();
+    }
+
+    // Wait (bounded) for MMAs still in flight after a timeout, free TMEM.
+    DRWC_DEV void end() {
+        if (threadIdx.x == 0 && pending) mbar_wait(bar(), phase ^ 1);
+        tc_fence_before();
+        __syncthreads();
+        if ((threadIdx.x >> 5) == 0)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                         "r"(S::TCOLS));
+    }
+};
+
+}  // namespace drwc

@@ -53,13 +53,15 @@ def _inputs(B, seed, N=16):
     return torch.from_numpy(x.astype(np.float32)).to(torch.bfloat16)
 
 
-@pytest.mark.parametrize("N", [16, 21, 23])
-def test_forward_matches_reference(ctx, N):
+@pytest.mark.parametrize("N,B", [(16, 37), (16, 701), (21, 37), (23, 37), (23, 203)])
+def test_forward_matches_reference(ctx, N, B):
+    """Inference runs conv1 and conv2 fused per group of cubes (two cubes per
+    CTA pass at N = 16, one at 21 / 23; odd B leaves a half group, the larger
+    B give CTAs several groups), conv3 and the heads as tile GEMMs."""
     import torch
     net = engine.Net(seed=3, ctx=ctx, N=N)
     assert (net.N, net.panels, net.out_row, net.grad_row, net.features) == tuple(
         engine.net_dims(N)[k] for k in ("N", "panels", "out_row", "grad_row", "features"))
-    B = 37
     X = _inputs(B, 1, N)
     dev = torch.device("cuda", 0)
     O = torch.zeros(B, net.out_row, device=dev)

@@ -144,10 +144,10 @@ def test_uniform_table_hops_follow_the_fdm_walk(ctx):
 
 
 def test_learned_server_agrees_with_learned_walker(ctx, small_net):
-    """The server runs conv1 on the CUDA cores inside its voxeliser (same BF16
-    operands, FP32 sums in another order); the learned walker runs it as a
-    tensor-core GEMM. Same walks, same network: the capacitance rows agree
-    well inside the statistical error."""
+    """The server runs conv1 and conv2 on the tensor cores inside its
+    voxeliser; the learned walker voxelises to global memory first. Same BF16
+    operands, same walks, same network: the capacitance rows agree well
+    inside the statistical error."""
     s = W.two_layer_crossing()
     nw = 40000
     p = _params(16, 31, nw, 8192)
