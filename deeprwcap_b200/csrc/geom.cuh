@@ -89,8 +89,8 @@ DRWC_DEV double encl_dist(const DevGeom& g, const double r[3]) {
     return best;
 }
 
-// Nearest conductor (L-infinity) for warp 0: the enclosure wins ties, then
-// the lowest box index. Result in lane 0 (and broadcast to the warp).
+// Nearest conductor (L-infinity), called by a whole warp: the enclosure wins
+// ties, then the lowest box index. Every lane gets the result.
 DRWC_DEV void nearest(const DevGeom& g, const double r[3], double* d_out, int* net_out) {
     const int lane = threadIdx.x & 31;
     double best = CUDART_INF;
@@ -100,7 +100,11 @@ DRWC_DEV void nearest(const DevGeom& g, const double r[3], double* d_out, int* n
             const double d = box_dist(g.box + 6 * b, r);
             if (d < best || (d == best && b < bidx)) { best = d; bidx = b; }
         }
-    } else if (lane == 0) {
+    } else {
+        // rings of grid cells at Chebyshev distance `ring` from the point's
+        // cell, the ring's cells spread over the lanes; the warp agrees on
+        // the best box after each ring, so it stops at the same ring as a
+        // scan in ring order would
         int ci[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -113,22 +117,40 @@ DRWC_DEV void nearest(const DevGeom& g, const double r[3], double* d_out, int* n
             // boxes not met in rings < ring lie at least (ring-1) cells away
             const double reach = (double)(ring - 1) * g.gmin_cell * (1.0 - 1e-12);
             if (ring > 1 && (best < reach || dwall < reach)) break;
-            for (int z = ci[2] - ring; z <= ci[2] + ring; ++z) {
-                if (z < 0 || z >= g.gdim[2]) continue;
-                for (int y = ci[1] - ring; y <= ci[1] + ring; ++y) {
-                    if (y < 0 || y >= g.gdim[1]) continue;
-                    for (int x = ci[0] - ring; x <= ci[0] + ring; ++x) {
-                        if (x < 0 || x >= g.gdim[0]) continue;
-                        const int cheb = max(abs(x - ci[0]), max(abs(y - ci[1]), abs(z - ci[2])));
-                        if (cheb != ring) continue;
-                        const int cell = x + g.gdim[0] * (y + g.gdim[1] * z);
-                        for (int it = g.gstart[cell]; it < g.gstart[cell + 1]; ++it) {
-                            const int b = g.gitems[it];
-                            const double d = box_dist(g.box + 6 * b, r);
-                            if (d < best || (d == best && b < bidx)) { best = d; bidx = b; }
-                        }
-                    }
+            const int side = 2 * ring + 1, per = 4 * (side - 1);
+            const int cells = ring == 0 ? 1 : 2 * side * side + (side - 2) * per;
+            for (int t = lane; t < cells; t += 32) {
+                int dx, dy, dz;
+                if (ring == 0) {
+                    dx = dy = dz = 0;
+                } else if (t < 2 * side * side) {  // the two full faces z = -ring, +ring
+                    const int u = t % (side * side);
+                    dz = t < side * side ? -ring : ring;
+                    dx = u % side - ring;
+                    dy = u / side - ring;
+                } else {  // the square border of each layer in between
+                    const int u = t - 2 * side * side, k = u % per, e = side - 1;
+                    dz = -ring + 1 + u / per;
+                    if (k < e) { dx = -ring + k; dy = -ring; }
+                    else if (k < 2 * e) { dx = ring; dy = -ring + (k - e); }
+                    else if (k < 3 * e) { dx = ring - (k - 2 * e); dy = ring; }
+                    else { dx = -ring; dy = ring - (k - 3 * e); }
                 }
+                const int x = ci[0] + dx, y = ci[1] + dy, z = ci[2] + dz;
+                if (x < 0 || x >= g.gdim[0] || y < 0 || y >= g.gdim[1] || z < 0 || z >= g.gdim[2])
+                    continue;
+                const int cell = x + g.gdim[0] * (y + g.gdim[1] * z);
+                for (int it = g.gstart[cell]; it < g.gstart[cell + 1]; ++it) {
+                    const int b = g.gitems[it];
+                    const double d = box_dist(g.box + 6 * b, r);
+                    if (d < best || (d == best && b < bidx)) { best = d; bidx = b; }
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bidx, o);
+                if (ob < best || (ob == best && oi < bidx)) { best = ob; bidx = oi; }
             }
         }
     }
@@ -189,10 +211,18 @@ DRWC_DEV void voxelise(const DevGeom& g, const double c[3], double a, const doub
 // Shared memory beyond the solver's: material ids, cell-centre offsets, the
 // palette and its pair-conductance tables.
 template <int N>
+struct VoxScratch;
+
+template <int N>
 struct WalkSmem {
-    static size_t bytes(int P) {
+    static size_t base(int P) {
         return Cube<N>::kSmemBytes + ((size_t)N * N * N + 15) / 16 * 16 + 8 * N + 16 * P +
                8 * (size_t)P * P + 4 * (size_t)P * P + 16;
+    }
+    // vox: room for the separable voxeliser's scratch after the rest (walks
+    // in structures with dielectric blocks)
+    static size_t bytes(int P, bool vox = false) {
+        return vox ? (base(P) + 15) / 16 * 16 + (sizeof(VoxScratch<N>) + 15) / 16 * 16 : base(P);
     }
 };
 
@@ -295,13 +325,15 @@ DRWC_DEV int rot_of_code(int code) { return code == DRWC_WVTX ? 1 : code == DRWC
 // ranges of the blocks that reach the cube (in block order: the first
 // containing block wins, as in mat_at); per voxel a few integer tests. The
 // result is mat_at's at every cell centre.
-constexpr int kVoxMaxBlocks = 32;  // blocks reaching one cube; beyond: mat_at per voxel
+constexpr int kVoxMaxBlocks = 64;  // blocks reaching one cube; beyond: mat_at per voxel
+constexpr int kVoxMaskFrom = 4;    // more blocks than this: per-axis block masks
 
 template <int N>
 struct VoxScratch {
     double crd[3][N];
     int lm[N];
     int rel[kVoxMaxBlocks][7];  // i0, i1, j0, j1, k0, k1 (original axes), material
+    uint64_t msk[3][N];         // bit q: block q's range holds this index (axis, index)
     int nrel;
 };
 
@@ -330,11 +362,26 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
                 hit = true;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    int i0 = N, i1 = -1;
-                    for (int i = 0; i < N; ++i) {
-                        const double x = vs.crd[d][i];
-                        if (x >= D[d] && x <= D[3 + d]) { i0 = min(i0, i); i1 = i; }
+                    // the centres are non-decreasing along an axis, so the
+                    // ones inside [lo, hi] form the range [first >= lo,
+                    // last <= hi]: two binary searches
+                    const double* x = vs.crd[d];
+                    const double lo = D[d], hi = D[3 + d];
+                    int i0 = 0, n = N;
+                    while (n > 0) {  // first index with x >= lo
+                        const int h = n >> 1;
+                        if (x[i0 + h] < lo) { i0 += h + 1; n -= h + 1; }
+                        else n = h;
                     }
+                    int i1 = 0;
+                    n = N;
+                    while (n > 0) {  // first index with x > hi
+                        const int h = n >> 1;
+                        if (x[i1 + h] <= hi) { i1 += h + 1; n -= h + 1; }
+                        else n = h;
+                    }
+                    i1 -= 1;
+                    if (i0 > i1) { i0 = N; i1 = -1; }
                     r[2 * d] = i0;
                     r[2 * d + 1] = i1;
                     hit &= i0 <= i1;
@@ -356,6 +403,19 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
         }
     }
     __syncthreads();
+    // many blocks: one mask per axis index, so a voxel's first block is the
+    // lowest bit of three ANDed masks (block order kept)
+    const int nrel = vs.nrel;
+    if (nrel > kVoxMaskFrom && nrel <= kVoxMaxBlocks) {
+        if (t < 3 * N) {
+            const int d = t / N, i = t % N;
+            uint64_t m = 0;
+            for (int q = 0; q < nrel; ++q)
+                if (i >= vs.rel[q][2 * d] && i <= vs.rel[q][2 * d + 1]) m |= 1ull << q;
+            vs.msk[d][i] = m;
+        }
+        __syncthreads();
+    }
 }
 
 // Material of voxel (i, j, k) of the (possibly rotated) cube.
@@ -370,6 +430,10 @@ DRWC_DEV int vox_material(const DevGeom& g, const VoxScratch<N>& vs, const doubl
         double p[3];
         rotated_point(c, a, tco, i, j, k, rot, p);
         return mat_at(g, p);
+    }
+    if (vs.nrel > kVoxMaskFrom) {
+        const uint64_t m = vs.msk[0][ox] & vs.msk[1][oy] & vs.msk[2][oz];
+        return m ? vs.rel[__ffsll((long long)m) - 1][6] : vs.lm[oz];
     }
     for (int q = 0; q < vs.nrel; ++q) {
         const int* r = vs.rel[q];

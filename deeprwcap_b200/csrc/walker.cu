@@ -125,7 +125,16 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
                     W.log_code[li] = code;
                 }
             }
-            voxelise<N>(g, c, a, tco, mat);
+            if (g.n_diel > 0) {  // separable: per-axis index ranges of the blocks
+                VoxScratch<N>& vs = *reinterpret_cast<VoxScratch<N>*>(
+                    smem + (WalkSmem<N>::base(P) + 15) / 16 * 16);
+                vox_prepare<N>(g, c, a, tco, vs);
+                for (int v = t; v < D::NNN; v += blockDim.x)
+                    mat[v] = (uint8_t)vox_material<N>(g, vs, c, a, tco, v % N, (v / N) % N,
+                                                      v / D::NN, 0);
+            } else {
+                voxelise<N>(g, c, a, tco, mat);
+            }
             __syncthreads();
             FdmStats st;
             cube_solve<N>(E, ys, ss, code, W.prm, &st);
@@ -194,22 +203,22 @@ __global__ void hop_sum_kernel(long long nw, const int32_t* __restrict__ hops,
 // Resident CTAs per SM for a given palette size (the shared-memory request
 // grows with it); the attribute is set once for the largest palette.
 template <int N>
-static int walk_shape(int P, int* per_sm) {
+static int walk_shape(int P, bool vox, int* per_sm) {
     static bool attr = false;
-    static int cache[kMaxMaterials + 1] = {0};
+    static int cache[2][kMaxMaterials + 1] = {{0}};
     if (!attr) {
         DRWC_CUDA_TRY(cudaFuncSetAttribute(walk_kernel<N>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)WalkSmem<N>::bytes(kMaxMaterials)));
+                                           (int)WalkSmem<N>::bytes(kMaxMaterials, true)));
         attr = true;
     }
-    if (!cache[P]) {
+    if (!cache[vox][P]) {
         int nb = 0;
         DRWC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &nb, walk_kernel<N>, Cube<N>::NT, WalkSmem<N>::bytes(P)));
-        cache[P] = nb < 1 ? 1 : nb;
+            &nb, walk_kernel<N>, Cube<N>::NT, WalkSmem<N>::bytes(P, vox)));
+        cache[vox][P] = nb < 1 ? 1 : nb;
     }
-    *per_sm = cache[P];
+    *per_sm = cache[vox][P];
     return DRWC_OK;
 }
 
@@ -229,7 +238,8 @@ static int launch_walks(drwc_ctx* ctx, const HostGeom& hg, const Gauss& G, const
         using D = Cube<NC>;
         const int nmat = hg.dev.n_mat;
         int per_sm = 0;
-        int rc = walk_shape<NC>(nmat, &per_sm);
+        const bool vox = hg.dev.n_diel > 0;
+        int rc = walk_shape<NC>(nmat, vox, &per_sm);
         if (rc) return rc;
         const int grid = (int)std::min<long long>(nw, (long long)per_sm * ctx->sm_count);
         void* scratch = nullptr;
@@ -238,7 +248,7 @@ static int launch_walks(drwc_ctx* ctx, const HostGeom& hg, const Gauss& G, const
         double* sy = (double*)scratch;
         float* sf = (float*)(sy + (size_t)grid * D::NNN);
         DRWC_CUDA_TRY(cudaMemsetAsync(wb.counter, 0, 8 * sizeof(unsigned long long), ctx->stream));
-        walk_kernel<NC><<<grid, D::NT, WalkSmem<NC>::bytes(nmat), ctx->stream>>>(
+        walk_kernel<NC><<<grid, D::NT, WalkSmem<NC>::bytes(nmat, vox), ctx->stream>>>(
             hg.dev, G, P, walk0, nw, wb.counter, wb.counter + 2, wb.end, wb.hops, wb.w, sy, sf);
         return launch_check(ctx);
     });
@@ -1058,7 +1068,7 @@ DRWC_API int drwc_frw_walks_learned(drwc_ctx* ctx, const drwc_structure* s,
     using D = Cube<N>;
     const int nmat = j->hg.dev.n_mat;
     int per_sm = 0;
-    rc = walk_shape<N>(nmat, &per_sm);  // same shared memory as the FDM walk
+    rc = walk_shape<N>(nmat, false, &per_sm);  // same shared memory as the FDM walk
     if (rc) return rc;
     static bool lw_attr = false;
     if (!lw_attr) {
