@@ -208,6 +208,26 @@ DRWC_DEV void voxelise(const DevGeom& g, const double c[3], double a, const doub
     }
 }
 
+// Structures without dielectric blocks: a cell's material is the layer of
+// its z index (mat_at's layer rule at that index's centre z), decided once
+// per index into lm (shared, N ints).
+template <int N>
+DRWC_DEV void voxelise_planes(const DevGeom& g, const double c[3], double a, const double* tco,
+                              uint8_t* mat, int* lm) {
+    const int t = threadIdx.x;
+    if (t < N) {
+        const double z = dadd(c[2], dmul(a, tco[t]));
+        int li = 0;
+        for (int l = 0; l < g.n_layers; ++l) {
+            if (z >= g.zlo[l]) li = l;
+            else break;
+        }
+        lm[t] = g.n_layers > 0 ? g.lmat[li] : 0;
+    }
+    __syncthreads();
+    for (int v = t; v < N * N * N; v += blockDim.x) mat[v] = (uint8_t)lm[v / (N * N)];
+}
+
 // Shared memory beyond the solver's: material ids, cell-centre offsets, the
 // palette and its pair-conductance tables.
 template <int N>
@@ -215,13 +235,13 @@ struct VoxScratch;
 
 template <int N>
 struct WalkSmem {
-    static size_t base(int P) {
+    __host__ __device__ static size_t base(int P) {
         return Cube<N>::kSmemBytes + ((size_t)N * N * N + 15) / 16 * 16 + 8 * N + 16 * P +
                8 * (size_t)P * P + 4 * (size_t)P * P + 16;
     }
     // vox: room for the separable voxeliser's scratch after the rest (walks
     // in structures with dielectric blocks)
-    static size_t bytes(int P, bool vox = false) {
+    __host__ __device__ static size_t bytes(int P, bool vox = false) {
         return vox ? (base(P) + 15) / 16 * 16 + (sizeof(VoxScratch<N>) + 15) / 16 * 16 : base(P);
     }
 };
@@ -335,6 +355,7 @@ struct VoxScratch {
     int rel[kVoxMaxBlocks][7];  // i0, i1, j0, j1, k0, k1 (original axes), material
     uint64_t msk[3][N];         // bit q: block q's range holds this index (axis, index)
     int nrel;
+    float lmax;                 // largest layer permittivity over the z indices (FP32)
 };
 
 template <int N>
@@ -351,6 +372,11 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
             else break;
         }
         vs.lm[t] = g.n_layers > 0 ? g.lmat[li] : 0;
+    }
+    if (t < 32) {
+        float pm = t < N ? (float)g.pal[vs.lm[t]] : 0.f;
+        for (int o = 16; o > 0; o >>= 1) pm = fmaxf(pm, __shfl_xor_sync(0xffffffffu, pm, o));
+        if (t == 0) vs.lmax = pm;
     }
     if (t < 32) {  // warp 0 keeps the blocks that reach the cube, in block order
         for (int b0 = 0; b0 < g.n_diel; b0 += 32) {
@@ -451,6 +477,22 @@ DRWC_DEV void voxelise_net(const DevGeom& g, const double c[3], double a, int ro
                            __nv_bfloat16* X, double* eps64, float* red, VoxScratch<N>& vs) {
     constexpr int NNN = N * N * N;
     vox_prepare<N>(g, c, a, tco, vs);
+    if (vs.nrel == 0) {
+        // no block reaches the cube: a cell's material is its layer, one per
+        // index along the original z axis, and the largest permittivity is
+        // the largest of those layers'
+        const float inv = 1.f / vs.lmax;
+        for (int v = threadIdx.x; v < NNN; v += blockDim.x) {
+            const int i = v % N, j = (v / N) % N, k = v / (N * N);
+            const int m = vs.lm[rot == 1 ? j : rot == 2 ? i : k];
+            matsm[v] = (uint8_t)m;
+            const double e = palsm[m];
+            X[v] = __float2bfloat16((float)e * inv);
+            if (eps64) eps64[v] = e;
+        }
+        __syncthreads();
+        return;
+    }
     float mx = 0.f;
     for (int v = threadIdx.x; v < NNN; v += blockDim.x) {
         const int i = v % N, j = (v / N) % N, k = v / (N * N);

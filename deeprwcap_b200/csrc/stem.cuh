@@ -151,17 +151,22 @@ struct Stem {
         return !aborted();
     }
 
-    // After thread 0 committed: wait for the MMAs (bounded).
+    // After thread 0 committed: warp 0 waits for the MMAs (bounded), the
+    // other warps at the CTA barrier, which leaves their issue slots to the
+    // co-resident CTA; the barrier orders the accumulator reads after the
+    // MMAs' completion.
     DRWC_DEV void complete(int* err) {
-        pending = true;
-        if (!mbar_wait(bar(), phase)) {
-            *abort_flag() = 1;
-            if (err) atomicExch(err, 1);
-        } else {
-            pending = false;
+        if (threadIdx.x < 32) {
+            const bool done = mbar_wait(bar(), phase);
+            if (!done && threadIdx.x == 0) {
+                *abort_flag() = 1;
+                if (err) atomicExch(err, 1);
+            }
         }
         phase ^= 1;
+        __syncthreads();
         tc_fence_after();
+        pending = aborted();  // after a timeout the MMAs may still be in flight
     }
 
     // conv1 of the cube in xs() into a1(cube), up to R1 M tiles per batch.
@@ -221,24 +226,33 @@ struct Stem {
     // conv2 of the group's nc cubes (a1(0 .. nc-1)) -> a2 rows [g0 * P3, ..).
     DRWC_DEV bool conv2(int nc, __nv_bfloat16* __restrict__ a2, int* err) {
         const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
+        static_assert(S::TAPS == 9 && S::NT % 256 == 0, "a fill is one dz plane of taps");
+        // every thread keeps one (row, channel half) of the tile and walks
+        // the taps of each fill: the row's position is decoded once
+        const int pr = t & 255, r = pr >> 1, h = pr & 1;
+        unsigned char* dst = opa() + (r >> 3) * 256 + h * 128 + (r & 7) * 16;
         for (int mt = 0; mt < S::MT2; ++mt) {
-            for (int cc = 0; cc < 27 / S::TAPS; ++cc) {
-                for (int it = t; it < 256 * S::TAPS; it += S::NT) {
-                    const int pr = it & 255, ti = it >> 8, r = pr >> 1, h = pr & 1;
-                    const int R = mt * kUmmaM + r, tap = cc * S::TAPS + ti;
+            const int R = mt * kUmmaM + r;
+            const int cube = R / S::P3, p = R % S::P3;
+            const bool row_ok = R < S::ROWS2 && cube < nc;
+            const int z0 = 2 * (p / (S::D3 * S::D3)) - 1, y0 = 2 * ((p / S::D3) % S::D3) - 1,
+                      x0 = 2 * (p % S::D3) - 1;
+            unsigned yx_ok = 0;  // bit dy * 3 + dx: that tap's (y, x) lies inside the grid
+#pragma unroll
+            for (int k = 0; k < 9; ++k)
+                if ((unsigned)(y0 + k / 3) < (unsigned)S::D2 && (unsigned)(x0 + k % 3) < (unsigned)S::D2)
+                    yx_ok |= 1u << k;
+            const __nv_bfloat16* src0 = a1(row_ok ? cube : 0) + 8 * h;
+            for (int cc = 0; cc < 3; ++cc) {  // fill cc holds the taps with dz = cc
+                const int z = z0 + cc;
+                const bool z_ok = row_ok && (unsigned)z < (unsigned)S::D2;
+#pragma unroll
+                for (int ti = S::NT == 256 ? 0 : t >> 8; ti < 9; ti += S::NT / 256) {
                     uint4 val = make_uint4(0u, 0u, 0u, 0u);
-                    if (R < S::ROWS2) {
-                        const int cube = R / S::P3, p = R % S::P3;
-                        const int pz = p / (S::D3 * S::D3), py = (p / S::D3) % S::D3, px = p % S::D3;
-                        const int z = 2 * pz - 1 + tap / 9, y = 2 * py - 1 + (tap / 3) % 3,
-                                  xx = 2 * px - 1 + tap % 3;
-                        if (cube < nc && (unsigned)z < (unsigned)S::D2 &&
-                            (unsigned)y < (unsigned)S::D2 && (unsigned)xx < (unsigned)S::D2)
-                            val = *reinterpret_cast<const uint4*>(
-                                a1(cube) + (size_t)((z * S::D2 + y) * S::D2 + xx) * 16 + 8 * h);
-                    }
-                    *reinterpret_cast<uint4*>(opa() + ti * 4096 + (r >> 3) * 256 + h * 128 +
-                                              (r & 7) * 16) = val;
+                    if (z_ok && ((yx_ok >> ti) & 1u))
+                        val = *reinterpret_cast<const uint4*>(
+                            src0 + (size_t)((z * S::D2 + y0 + ti / 3) * S::D2 + x0 + ti % 3) * 16);
+                    *reinterpret_cast<uint4*>(dst + ti * 4096) = val;
                 }
                 if (!staged()) return false;
                 if (t == 0) {

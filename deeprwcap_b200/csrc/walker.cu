@@ -43,6 +43,7 @@ struct WalkState {
     int done;
     long long walk;
     double sgn_out;
+    int lm[DRWC_N_MAX];  // layer material per z index (structures without blocks)
 };
 
 template <int N>
@@ -133,7 +134,7 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
                     mat[v] = (uint8_t)vox_material<N>(g, vs, c, a, tco, v % N, (v / N) % N,
                                                       v / D::NN, 0);
             } else {
-                voxelise<N>(g, c, a, tco, mat);
+                voxelise_planes<N>(g, c, a, tco, mat, S.lm);
             }
             __syncthreads();
             FdmStats st;
