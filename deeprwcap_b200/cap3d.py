@@ -11,7 +11,9 @@ testcases/cap3d/*.cap3d); lengths in um:
     <window> v1(x,y,z) v2(x,y,z)        the simulation box: the grounded enclosure
     <plate_medium> diel, z_top           stratified dielectric, stacked by z_top
     <medium> <block>...</block> diel     dielectric blocks (first listed wins)
-    <conductor> name <block>...</block>  one net per conductor, in file order
+    <conductor> name <block>...</block>  conductors; a "<k>__" name prefix numbers
+                                         the pieces of one net, and conductors
+                                         of the same name are one net
     <block> basepoint(..) v1(..) v2(..) hvector(..)
                                          an axis-aligned box spanned by three
                                          edge vectors from its base point
@@ -60,7 +62,21 @@ class Cap3d:
 
     @property
     def net_names(self) -> list:
-        return [c[0] for c in self.conductors]
+        """Nets in order of first appearance (conductors of one net merged)."""
+        out = []
+        for name, _ in self.conductors:
+            n = net_of(name)
+            if n not in out:
+                out.append(n)
+        return out
+
+
+def net_of(conductor: str) -> str:
+    """Net of a conductor: a ``<digits>__`` prefix numbers the pieces of one
+    net (``9__signalGND`` is a piece of ``signalGND``), and conductors of the
+    same name are one net."""
+    m = re.match(r"^\d+__(.+)$", conductor)
+    return m.group(1) if m else conductor
 
 
 def _box(b: dict, where: str) -> list:
@@ -157,14 +173,16 @@ def parse(source) -> Cap3d:
 
 
 def to_structure(c: Cap3d) -> W.StructureSpec:
-    """The engine structure: conductor boxes with net ids in file order,
+    """The engine structure: conductor boxes with net ids in order of the
+    nets' first appearance (pieces of one net merged, see ``net_of``),
     plate media as layers (layer l from the previous z_top, the first from
     the window bottom), media blocks as dielectric blocks, the window as the
     grounded enclosure."""
     boxes, nets = [], []
-    for i, (_, bl) in enumerate(c.conductors):
+    ids = {n: i for i, n in enumerate(c.net_names)}
+    for name, bl in c.conductors:
         boxes.extend(bl)
-        nets.extend([i] * len(bl))
+        nets.extend([ids[net_of(name)]] * len(bl))
     plates = sorted(c.plates, key=lambda p: p[2])
     if plates:
         zlo = [float(c.window_lo[2])] + [p[2] for p in plates[:-1]]
@@ -173,7 +191,7 @@ def to_structure(c: Cap3d) -> W.StructureSpec:
         zlo, eps = [float(c.window_lo[2])], [1.0]
     diel = [[*b, e] for _, e, bl in c.media for b in bl]
     return W.StructureSpec(np.asarray(boxes, dtype=np.float64).reshape(-1, 6),
-                           np.asarray(nets, dtype=np.int32), len(c.conductors),
+                           np.asarray(nets, dtype=np.int32), len(ids),
                            np.asarray(zlo, dtype=np.float64), np.asarray(eps, dtype=np.float64),
                            np.asarray(diel, dtype=np.float64).reshape(-1, 7),
                            c.window_lo.astype(np.float64), c.window_hi.astype(np.float64))
@@ -213,7 +231,7 @@ def extract(c: Cap3d, master: str | None = None, ctx=None, **kw) -> dict:
     ``WINDOW``), plus the engine's raw row and run statistics."""
     from . import engine
     s = to_structure(c)
-    name = master or (c.masters[0] if c.masters else c.net_names[0])
+    name = net_of(master) if master else (net_of(c.masters[0]) if c.masters else c.net_names[0])
     if name not in c.net_names:
         raise ValueError(f"master {name!r} is not a conductor")
     mi = c.net_names.index(name)
@@ -341,7 +359,7 @@ def main() -> None:
     if a.c_ratio is not None:
         kw["c_ratio"] = a.c_ratio
     res = [extract(c, m, **kw) for m in (c.masters or c.net_names[:1])]
-    out = {"case": Path(a.case).name, "nets": len(c.conductors),
+    out = {"case": Path(a.case).name, "conductors": len(c.conductors), "nets": len(c.net_names),
            "boxes": sum(len(b) for _, b in c.conductors),
            "media_blocks": sum(len(b) for _, _, b in c.media), "plates": len(c.plates),
            "results": res}

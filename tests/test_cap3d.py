@@ -112,6 +112,20 @@ def test_structure():
     np.testing.assert_array_equal(s.encl_lo, [-2, -2, 0])
 
 
+def test_pieces_of_a_net_are_merged():
+    text = CASE.replace("\tname B\n", "\tname 12__B\n").replace(
+        "<layer>", "<conductor>\n\tname 3__B\n\t<block>\n\t\tbasepoint(3.0,2.0,1.2)\n"
+        "\t\tv1(0.5,0,0)\n\t\tv2(0,0.3,0)\n\t\thvector(0,0,0.3)\n\t</block>\n"
+        "</conductor>\n<conductor>\n\tname A\n\t<block>\n\t\tbasepoint(-1.0,-1.0,3.0)\n"
+        "\t\tv1(0.2,0,0)\n\t\tv2(0,0.2,0)\n\t\thvector(0,0,0.2)\n\t</block>\n"
+        "</conductor>\n<layer>", 1)
+    c = C.parse(text)
+    assert len(c.conductors) == 5 and c.net_names == ["GROUND", "A", "B"]
+    s = C.to_structure(c)
+    assert s.n_nets == 3 and list(s.nets) == [0, 1, 1, 2, 2, 1]
+    assert C.net_of("9__signalGND") == "signalGND" and C.net_of("ln_14") == "ln_14"
+
+
 def test_clearance_and_job_params():
     c = C.parse(CASE)
     s = C.to_structure(c)
