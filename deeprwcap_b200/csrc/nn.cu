@@ -254,6 +254,17 @@ struct EpiF32 {
             if (c < N) dst[c] = v[i] + (bias ? bias[c] : 0.f);
         }
     }
+    // 4 consecutive columns (col a multiple of 4) of one row.
+    DRWC_DEV void store4(int row, int col, float4 v) const {
+        float* dst = out + (int64_t)(rowmap ? rowmap[row] : row) * ld + col;
+        if (col + 4 <= N && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+            if (bias) { v.x += bias[col]; v.y += bias[col + 1]; v.z += bias[col + 2]; v.w += bias[col + 3]; }
+            *reinterpret_cast<float4*>(dst) = v;
+            return;
+        }
+        const float e[4] = {v.x, v.y, v.z, v.w};
+        for (int i = 0; i < 4 && col + i < N; ++i) dst[i] = e[i] + (bias ? bias[col + i] : 0.f);
+    }
 };
 
 // Accumulate into FP32 [rows, N] with atomics (split-K weight gradients).
@@ -575,7 +586,7 @@ static int net_heads(drwc_net* n, int rows, const int* rowmap, float* O, float* 
     int rc = DRWC_OK;
     if (O) {
         rc = rowmap ? DRWC_ERR_INVALID
-                    : launch_umma_tma<128>(ctx, rows, nullptr, 1, kDecRows, kFeat, n->a3, kFeat,
+                    : launch_umma_tma<DRWC_TMA_BN>(ctx, rows, nullptr, 1, kDecRows, kFeat, n->a3, kFeat,
                                            n->pb + n->L.wd, kFeat,
                                            EpiF32{O, n->p + n->L.bd, kDecRows, kDecRows, nullptr},
                                            n->err);
@@ -694,7 +705,7 @@ static int net_forward_dyn_t(drwc_net* n, int Bmax, const unsigned* nrows, const
                              RowsBf16{pb + n->L.w3, 64, 27 * 32, 27 * 32, nullptr},
                              EpiReluBf16{n->a3, n->p + n->L.b3, 64}, n->err);
     if (rc) return rc;
-    rc = launch_umma_tma<128>(ctx, Bmax, nrows, 1, S::DEC, S::FEAT, n->a3, S::FEAT,
+    rc = launch_umma_tma<DRWC_TMA_BN>(ctx, Bmax, nrows, 1, S::DEC, S::FEAT, n->a3, S::FEAT,
                               n->pb + n->L.wd, S::FEAT,
                               EpiF32{O, n->p + n->L.bd, S::DEC, S::DEC, nullptr}, n->err);
     if (rc == DRWC_ERR_INVALID)

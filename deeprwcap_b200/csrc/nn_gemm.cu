@@ -54,6 +54,23 @@ struct StoreF32 {
             }
         }
     }
+    // 4 consecutive columns (col a multiple of 4) of one row.
+    DRWC_DEV void store4(int row, int col, float4 v) const {
+        float* dst = c + (int64_t)row * ldc + col;
+        float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (col + i < N) {
+                e[i] += bias ? bias[col + i] : 0.f;
+                if (act == 1) e[i] = fmaxf(e[i], 0.f);
+            }
+        }
+        if (col + 4 <= N && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+            *reinterpret_cast<float4*>(dst) = make_float4(e[0], e[1], e[2], e[3]);
+            return;
+        }
+        for (int i = 0; i < 4 && col + i < N; ++i) dst[i] = e[i];
+    }
 };
 
 template <int BN>
@@ -82,7 +99,7 @@ DRWC_API int drwc_gemm_bf16(drwc_ctx* ctx, int M, int N, int K, const void* A, i
     StoreF32 st{C, bias, N, ldc, act};
     constexpr int BN = 128;
     // TMA-fed, warp-specialised tiles when the operands allow it
-    const int rt = launch_umma_tma<BN>(ctx, M, nullptr, 1, N, K, (const __nv_bfloat16*)A, lda,
+    const int rt = launch_umma_tma<DRWC_TMA_BN>(ctx, M, nullptr, 1, N, K, (const __nv_bfloat16*)A, lda,
                                        (const __nv_bfloat16*)B, ldb, st, err_flag);
     if (rt != DRWC_ERR_INVALID) return rt;
     static bool attr = false;
