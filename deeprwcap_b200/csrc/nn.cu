@@ -225,6 +225,20 @@ struct EpiReluBf16 {
             if (c < N) dst[c] = __float2bfloat16(fmaxf(v[i] + bias[c], 0.f));
         }
     }
+    // 4 consecutive columns (col a multiple of 4) of one row.
+    DRWC_DEV void store4(int row, int col, float4 v) const {
+        bf16* dst = out + (int64_t)row * N + col;
+        if (col + 4 <= N && (reinterpret_cast<uintptr_t>(dst) & 7) == 0) {
+            __align__(8) __nv_bfloat162 h[2];
+            h[0] = __floats2bfloat162_rn(fmaxf(v.x + bias[col], 0.f), fmaxf(v.y + bias[col + 1], 0.f));
+            h[1] = __floats2bfloat162_rn(fmaxf(v.z + bias[col + 2], 0.f), fmaxf(v.w + bias[col + 3], 0.f));
+            *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(h);
+            return;
+        }
+        const float e[4] = {v.x, v.y, v.z, v.w};
+        for (int i = 0; i < 4 && col + i < N; ++i)
+            dst[i] = __float2bfloat16(fmaxf(e[i] + bias[col + i], 0.f));
+    }
 };
 
 // bias -> FP32 rows [rows, ld].

@@ -21,6 +21,8 @@
 
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace drwc {
@@ -123,6 +125,38 @@ DRWC_DEV void tmem_ld32(uint32_t taddr, float* v) {
 DRWC_DEV uint32_t umma_tile_off(int row, int k, int rows) {
     return (uint32_t)((k >> 4) * rows * 32 + (row >> 3) * 256 + ((k >> 3) & 1) * 128 +
                       (row & 7) * 16 + (k & 7) * 2);
+}
+
+// Epilogue functors that can store 4 consecutive columns of one row
+// (store4) get coalesced stores: each warp writes its 32 x 32 accumulator
+// block back through shared memory, four rows per store instruction (eight
+// lanes per row), instead of one row segment per lane.
+template <class EPI, class = void>
+struct EpiHasStore4 : std::false_type {};
+template <class EPI>
+struct EpiHasStore4<EPI, std::void_t<decltype(&EPI::store4)>> : std::true_type {};
+
+// The block's floats per warp in shared memory: rows padded to 33 floats,
+// so the row-per-lane writes and the column reads are free of bank conflicts.
+constexpr int kEpiStageFloats = 32 * 33;
+
+// Rows row0 .. row0+31 (lane = row) x columns col0 .. col0+31 of a warp's
+// accumulator values v, through the warp's staging block stg.
+template <class EPI>
+DRWC_DEV void epi_block_store(const EPI& epi, float* stg, const float* v, int row0, int col0,
+                              int M, int N) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int e = 0; e < 32; ++e) stg[lane * 33 + e] = v[e];
+    __syncwarp();
+#pragma unroll
+    for (int it = 0; it < 8; ++it) {
+        const int rr = it * 4 + (lane >> 3), cc = (lane & 7) * 4;
+        const float* src = stg + rr * 33 + cc;
+        if (row0 + rr < M && col0 + cc < N)
+            epi.store4(row0 + rr, col0 + cc, make_float4(src[0], src[1], src[2], src[3]));
+    }
+    __syncwarp();
 }
 
 // Shared-memory stages of a tile: enough K stages in flight to cover the
@@ -341,12 +375,19 @@ DRWC_DEV void umma_gemm_tile(int M, int N, int K, int m0, int n0, const LA& la, 
         if (uses[q] > 0) ok &= mbar_wait(&bar[q], (uses[q] - 1) & 1);
     tc_fence_after();
     if (!ok && err) atomicExch(err, 1);
-    // epilogue: warp w reads accumulator lanes (rows) 32w .. 32w+31
+    // epilogue: warp w reads accumulator lanes (rows) 32w .. 32w+31; the
+    // stages are idle now and stage the coalesced stores
     const int row = m0 + warp * 32 + lane;
     for (int c = 0; c < BN; c += 32) {
         float v[32];
         tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-        if (ok && row < M && n0 + c < N) epi(row, n0 + c, v);
+        if constexpr (EpiHasStore4<EPI>::value) {
+            if (ok && n0 + c < N)
+                epi_block_store(epi, reinterpret_cast<float*>(smem) + warp * kEpiStageFloats, v,
+                                m0 + warp * 32, n0 + c, M, N);
+        } else {
+            if (ok && row < M && n0 + c < N) epi(row, n0 + c, v);
+        }
     }
     if (own) umma_tmem_free<BN>(tmem);
     else {

@@ -50,24 +50,15 @@ constexpr int tma_stages() {
 #define DRWC_TMA_BN 256
 #endif
 
-// Per epilogue warp, a 32 x 32 FP32 block staged with rows padded to 33
-// floats, so that both the row-per-lane writes and the column reads are free
-// of bank conflicts.
-constexpr int kTmaStageFloats = 32 * 33;
+// Per epilogue warp, one staged 32 x 32 block (epi_block_store).
+constexpr int kTmaStageFloats = kEpiStageFloats;
 
 template <int BN>
 constexpr size_t tma_smem_bytes() {
     return (size_t)tma_stages<BN>() * (kUmmaM + BN) * kUmmaBK * 2 + 256 + 4 * kTmaStageFloats * 4;
 }
 
-// Epilogue functors that can store 4 consecutive columns of one row
-// (store4) get coalesced stores: each warp writes its 32 x 32 block back
-// through shared memory, four rows of 128 B per store instruction, instead
-// of one 128-byte row segment per lane.
-template <class EPI, class = void>
-struct EpiHasStore4 : std::false_type {};
-template <class EPI>
-struct EpiHasStore4<EPI, std::void_t<decltype(&EPI::store4)>> : std::true_type {};
+
 
 DRWC_DEV void tma_load_2d(uint32_t dst, const CUtensorMap* map, int c0, int c1, uint32_t bar) {
     asm volatile(
@@ -222,19 +213,7 @@ __global__ void __launch_bounds__(kTmaThreads) umma_tma_kernel(const __grid_cons
                 float v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(ab * BN + c), v);
                 if constexpr (EpiHasStore4<EPI>::value) {
-                    if (n0 + c >= N) continue;  // warp-uniform
-#pragma unroll
-                    for (int e = 0; e < 32; ++e) stg[lane * 33 + e] = v[e];
-                    __syncwarp();
-#pragma unroll
-                    for (int it = 0; it < 8; ++it) {
-                        const int rr = it * 4 + (lane >> 3), cc = (lane & 7) * 4;
-                        const float* src = stg + rr * 33 + cc;
-                        const int grow = m0 + q * 32 + rr, gcol = n0 + c + cc;
-                        if (grow < M && gcol < N)
-                            epi.store4(grow, gcol, make_float4(src[0], src[1], src[2], src[3]));
-                    }
-                    __syncwarp();
+                    if (n0 + c < N) epi_block_store(epi, stg, v, m0 + q * 32, n0 + c, M, N);
                 } else {
                     if (row < M && n0 + c < N) epi(row, n0 + c, v);
                 }
