@@ -2,14 +2,15 @@
 
     python -m deeprwcap_b200.serve [--structure dense_stack|two_layer_crossing]
         [--walks 65536] [--N 16] [--net none|random|PATH] [--uniform-table 0|1]
-        [--stream JOBS] [--walks-max 1e6]
+        [--stream JOBS] [--walks-max 1e6] [--net-sizes 16,21,23]
 
 One job of --walks walks on the named structure (or, with --stream, a
 seeded Poisson stream of that many jobs, 50 jobs/s, as in the serving
 benchmark) is submitted to a server created with the given options; the job
 results and the server's counters are printed as one JSON line. --net random
-uses an untrained network (the cost of the learned path does not depend on
-its weights); PATH loads a network saved by deeprwcap_b200.train.
+uses untrained networks, one per size in --net-sizes (the cost of the
+learned path does not depend on the weights); PATH loads a network saved by
+deeprwcap_b200.train.
 """
 from __future__ import annotations
 
@@ -28,6 +29,8 @@ def main() -> None:
     ap.add_argument("--walks", type=int, default=65536)
     ap.add_argument("--N", type=int, default=16)
     ap.add_argument("--net", default="none")
+    ap.add_argument("--net-sizes", default="16",
+                    help="with --net random: the cube resolutions to build networks for, e.g. 16,21,23")
     ap.add_argument("--uniform-table", type=int, default=0)
     ap.add_argument("--slots", type=int, default=65536)
     ap.add_argument("--stream", type=int, default=0)
@@ -36,7 +39,7 @@ def main() -> None:
     ctx = engine.default_context(0)
     net = None
     if a.net == "random":
-        net = engine.Net(seed=1, ctx=ctx)
+        net = [engine.Net(seed=1, ctx=ctx, N=int(n)) for n in a.net_sizes.split(",")]
     elif a.net != "none":
         from . import train
         net = train.load(a.net, ctx=ctx)
