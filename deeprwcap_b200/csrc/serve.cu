@@ -523,6 +523,9 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
     const unsigned count = A.cnt[4 * bucket + 2];
     unsigned* next_item = A.cnt + 4 * bucket + 3;
     __shared__ unsigned s_idx;
+    __shared__ int lm[N];  // layer material per z index (structures without blocks)
+    VoxScratch<N>& vs =   // separable voxeliser (structures with blocks)
+        *reinterpret_cast<VoxScratch<N>*>(smem + (WalkSmem<N>::base(maxP) + 15) / 16 * 16);
     int loaded = -1, P = 0;
     unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0;
     for (;;) {
@@ -556,7 +559,14 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
         const int code = first ? A.st.code[slot] : DRWC_GFT;
         const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
         const double a = A.st.a[slot];
-        voxelise<N>(J.g, c, a, tco, mat);
+        if (J.g.n_diel > 0) {
+            vox_prepare<N>(J.g, c, a, tco, vs);
+            for (int v = threadIdx.x; v < D::NNN; v += blockDim.x)
+                mat[v] = (uint8_t)vox_material<N>(J.g, vs, c, a, tco, v % N, (v / N) % N,
+                                                  v / D::NN, 0);
+        } else {
+            voxelise_planes<N>(J.g, c, a, tco, mat, lm);
+        }
         __syncthreads();
         FdmStats st;
         cube_solve<N>(E, ys, ss, code, J.W.prm, &st);
@@ -783,7 +793,7 @@ namespace drwc {
 template <int N>
 static int sv_fdm_setup(drwc_server* v, int b) {
     using D = Cube<N>;
-    const size_t smem = WalkSmem<N>::bytes(v->o.max_materials);
+    const size_t smem = WalkSmem<N>::bytes(v->o.max_materials, true);
     DRWC_CUDA_TRY(cudaFuncSetAttribute(sv_fdm_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
     int per_sm = 0;
