@@ -976,6 +976,9 @@ lw_fdm_kernel(LwArgs A, double* __restrict__ scratch_y, float* __restrict__ scra
     float* ss = scratch_s + (size_t)blockIdx.x * D::NNN;
     __syncthreads();
     const unsigned int count = *A.fdm_count;
+    __shared__ int lm[N];  // layer material per z index (structures without blocks)
+    VoxScratch<N>& vs =   // separable voxeliser (structures with blocks)
+        *reinterpret_cast<VoxScratch<N>*>(smem + (WalkSmem<N>::base(P) + 15) / 16 * 16);
     for (unsigned int idx = blockIdx.x; idx < count; idx += gridDim.x) {
         const int slot = A.fdm_list[idx];
         const int audit = A.fdm_kind[idx] & 1;
@@ -986,7 +989,14 @@ lw_fdm_kernel(LwArgs A, double* __restrict__ scratch_y, float* __restrict__ scra
         const int code = first ? A.st.code[slot] : DRWC_GFT;
         const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
         const double a = A.st.a[slot];
-        voxelise<N>(g, c, a, tco, mat);
+        if (g.n_diel > 0) {
+            vox_prepare<N>(g, c, a, tco, vs);
+            for (int v = threadIdx.x; v < D::NNN; v += blockDim.x)
+                mat[v] = (uint8_t)vox_material<N>(g, vs, c, a, tco, v % N, (v / N) % N,
+                                                  v / D::NN, 0);
+        } else {
+            voxelise_planes<N>(g, c, a, tco, mat, lm);
+        }
         __syncthreads();
         FdmStats st;
         cube_solve<N>(E, ys, ss, code, A.W.prm, &st);
@@ -1069,13 +1079,14 @@ DRWC_API int drwc_frw_walks_learned(drwc_ctx* ctx, const drwc_structure* s,
     using D = Cube<N>;
     const int nmat = j->hg.dev.n_mat;
     int per_sm = 0;
-    rc = walk_shape<N>(nmat, false, &per_sm);  // same shared memory as the FDM walk
+    const bool vox = j->hg.dev.n_diel > 0;
+    rc = walk_shape<N>(nmat, vox, &per_sm);  // same shared memory as the FDM walk
     if (rc) return rc;
     static bool lw_attr = false;
     if (!lw_attr) {
         DRWC_CUDA_TRY(cudaFuncSetAttribute(lw_fdm_kernel<N>,
                                            cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)WalkSmem<N>::bytes(kMaxMaterials)));
+                                           (int)WalkSmem<N>::bytes(kMaxMaterials, true)));
         lw_attr = true;
     }
     const int fdm_grid = per_sm * ctx->sm_count;
@@ -1150,7 +1161,7 @@ DRWC_API int drwc_frw_walks_learned(drwc_ctx* ctx, const drwc_structure* s,
         if (r) return r;
         lw_sample_kernel<<<g2, 256, 0, ctx->stream>>>(A);
         if ((r = launch_check(ctx))) return r;
-        lw_fdm_kernel<N><<<fdm_grid, D::NT, WalkSmem<N>::bytes(nmat), ctx->stream>>>(A, sy, ss);
+        lw_fdm_kernel<N><<<fdm_grid, D::NT, WalkSmem<N>::bytes(nmat, vox), ctx->stream>>>(A, sy, ss);
         return launch_check(ctx);
     };
     const auto t0 = std::chrono::steady_clock::now();
