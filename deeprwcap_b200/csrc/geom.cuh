@@ -172,6 +172,30 @@ DRWC_DEV void nearest(const DevGeom& g, const double r[3], double* d_out, int* n
 
 // Material id at a point: first containing dielectric block, else the last
 // stratified layer with zlo <= z (layer 0 below all of them).
+// Layer index of height z: the last layer l with zlo[l] <= z among the
+// first layers that all satisfy it (scan in order, stop at the first layer
+// above z; layer 0 below all of them). The bounds are read eight at a time,
+// so a cube's layer search waits for one memory round trip per eight layers
+// instead of one per layer.
+DRWC_DEV int layer_index(const DevGeom& g, double z) {
+    int li = 0;
+    for (int l0 = 0; l0 < g.n_layers; l0 += 8) {
+        double zz[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) zz[e] = l0 + e < g.n_layers ? g.zlo[l0 + e] : 0.0;
+        bool stop = false;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            if (!stop && l0 + e < g.n_layers) {
+                if (z >= zz[e]) li = l0 + e;
+                else stop = true;
+            }
+        }
+        if (stop) break;
+    }
+    return li;
+}
+
 DRWC_DEV int mat_at(const DevGeom& g, const double p[3]) {
     for (int b = 0; b < g.n_diel; ++b) {
         const double* D = g.diel + 7 * b;
@@ -180,12 +204,7 @@ DRWC_DEV int mat_at(const DevGeom& g, const double p[3]) {
             return g.dmat[b];
     }
     if (g.n_layers <= 0) return 0;
-    int li = 0;
-    for (int l = 0; l < g.n_layers; ++l) {
-        if (p[2] >= g.zlo[l]) li = l;
-        else break;
-    }
-    return g.lmat[li];
+    return g.lmat[layer_index(g, p[2])];
 }
 
 // Cell-centre offsets (2i+1)/N - 1, rounded exactly as the CPU walk computes them.
@@ -217,12 +236,7 @@ DRWC_DEV void voxelise_planes(const DevGeom& g, const double c[3], double a, con
     const int t = threadIdx.x;
     if (t < N) {
         const double z = dadd(c[2], dmul(a, tco[t]));
-        int li = 0;
-        for (int l = 0; l < g.n_layers; ++l) {
-            if (z >= g.zlo[l]) li = l;
-            else break;
-        }
-        lm[t] = g.n_layers > 0 ? g.lmat[li] : 0;
+        lm[t] = g.n_layers > 0 ? g.lmat[layer_index(g, z)] : 0;
     }
     __syncthreads();
     for (int v = t; v < N * N * N; v += blockDim.x) mat[v] = (uint8_t)lm[v / (N * N)];
@@ -360,21 +374,25 @@ struct VoxScratch {
 
 template <int N>
 DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const double* tco,
-                          VoxScratch<N>& vs) {
+                          VoxScratch<N>& vs, const double* palsm = nullptr) {
     const int t = threadIdx.x;
+    // warp 0 fetches its lanes' first dielectric blocks now: they do not
+    // depend on the cube, so their latency overlaps the rest of the set-up
+    double Dv[6];
+    int dm = 0;
+    if (t < 32 && t < g.n_diel) {
+        const double* D = g.diel + 7 * t;
+#pragma unroll
+        for (int e = 0; e < 6; ++e) Dv[e] = D[e];
+        dm = g.dmat[t];
+    }
     if (t < 3 * N) vs.crd[t / N][t % N] = dadd(c[t / N], dmul(a, tco[t % N]));
     if (t == 0) vs.nrel = 0;
     __syncthreads();
-    if (t < N) {
-        int li = 0;
-        for (int l = 0; l < g.n_layers; ++l) {
-            if (vs.crd[2][t] >= g.zlo[l]) li = l;
-            else break;
-        }
-        vs.lm[t] = g.n_layers > 0 ? g.lmat[li] : 0;
-    }
+    if (t < N) vs.lm[t] = g.n_layers > 0 ? g.lmat[layer_index(g, vs.crd[2][t])] : 0;
     if (t < 32) {
-        float pm = t < N ? (float)g.pal[vs.lm[t]] : 0.f;
+        const double* pal = palsm ? palsm : g.pal;
+        float pm = t < N ? (float)pal[vs.lm[t]] : 0.f;
         for (int o = 16; o > 0; o >>= 1) pm = fmaxf(pm, __shfl_xor_sync(0xffffffffu, pm, o));
         if (t == 0) vs.lmax = pm;
     }
@@ -384,7 +402,12 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
             int r[6] = {0, -1, 0, -1, 0, -1};
             bool hit = false;
             if (b < g.n_diel) {
-                const double* D = g.diel + 7 * b;
+                if (b0 > 0) {
+                    const double* D = g.diel + 7 * b;
+#pragma unroll
+                    for (int e = 0; e < 6; ++e) Dv[e] = D[e];
+                    dm = g.dmat[b];
+                }
                 hit = true;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
@@ -392,7 +415,7 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
                     // ones inside [lo, hi] form the range [first >= lo,
                     // last <= hi]: two binary searches
                     const double* x = vs.crd[d];
-                    const double lo = D[d], hi = D[3 + d];
+                    const double lo = Dv[d], hi = Dv[3 + d];
                     int i0 = 0, n = N;
                     while (n > 0) {  // first index with x >= lo
                         const int h = n >> 1;
@@ -420,7 +443,7 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
                 if (q < kVoxMaxBlocks) {
 #pragma unroll
                     for (int e = 0; e < 6; ++e) vs.rel[q][e] = r[e];
-                    vs.rel[q][6] = g.dmat[b];
+                    vs.rel[q][6] = dm;
                 }
             }
             __syncwarp();
@@ -476,7 +499,7 @@ DRWC_DEV void voxelise_net(const DevGeom& g, const double c[3], double a, int ro
                            const double* tco, const double* palsm, uint8_t* matsm,
                            __nv_bfloat16* X, double* eps64, float* red, VoxScratch<N>& vs) {
     constexpr int NNN = N * N * N;
-    vox_prepare<N>(g, c, a, tco, vs);
+    vox_prepare<N>(g, c, a, tco, vs, palsm);
     if (vs.nrel == 0) {
         // no block reaches the cube: a cell's material is its layer, one per
         // index along the original z axis, and the largest permittivity is
