@@ -376,16 +376,6 @@ template <int N>
 DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const double* tco,
                           VoxScratch<N>& vs, const double* palsm = nullptr) {
     const int t = threadIdx.x;
-    // warp 0 fetches its lanes' first dielectric blocks now: they do not
-    // depend on the cube, so their latency overlaps the rest of the set-up
-    double Dv[6];
-    int dm = 0;
-    if (t < 32 && t < g.n_diel) {
-        const double* D = g.diel + 7 * t;
-#pragma unroll
-        for (int e = 0; e < 6; ++e) Dv[e] = D[e];
-        dm = g.dmat[t];
-    }
     if (t < 3 * N) vs.crd[t / N][t % N] = dadd(c[t / N], dmul(a, tco[t % N]));
     if (t == 0) vs.nrel = 0;
     __syncthreads();
@@ -401,13 +391,13 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
             const int b = b0 + t;
             int r[6] = {0, -1, 0, -1, 0, -1};
             bool hit = false;
+            double Dv[6];
+            int dm = 0;
             if (b < g.n_diel) {
-                if (b0 > 0) {
-                    const double* D = g.diel + 7 * b;
+                const double* D = g.diel + 7 * b;
 #pragma unroll
-                    for (int e = 0; e < 6; ++e) Dv[e] = D[e];
-                    dm = g.dmat[b];
-                }
+                for (int e = 0; e < 6; ++e) Dv[e] = D[e];
+                dm = g.dmat[b];
                 hit = true;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
