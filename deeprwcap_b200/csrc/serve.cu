@@ -352,6 +352,7 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
     __shared__ double pal[kMaxMaterials];
     __shared__ VoxScratch<N> vs;
     __shared__ float red[32];
+    __shared__ DevGeom gs;  // the current job's geometry header: its fields are read per voxel pass
     const int na = (int)A.cnt[4 * bucket];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.stats + SV_NET_ROWS, (unsigned long long)na);
     if ((int)blockIdx.x * D::CUBES >= na) return;
@@ -370,13 +371,14 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
             if (j != loaded) {
                 __syncthreads();
                 for (int v = threadIdx.x; v < J.g.n_mat; v += blockDim.x) pal[v] = J.g.pal[v];
+                if (threadIdx.x == 0) gs = J.g;
                 loaded = j;
             }
             __syncthreads();
             const bool first = A.st.hops[slot] == 0;
             const int rot = first ? rot_of_code(A.st.code[slot]) : 0;
             const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
-            voxelise_net<N>(J.g, c, A.st.a[slot], rot, tco, pal, st.mat(), st.xs(), nullptr, red, vs);
+            voxelise_net<N>(gs, c, A.st.a[slot], rot, tco, pal, st.mat(), st.xs(), nullptr, red, vs);
             if (first && threadIdx.x == 0) {
                 const EpsPalette E{st.mat(), pal, nullptr, nullptr, nullptr, 0};
                 A.st.epsw[slot] = center_diel<N>(E, DRWC_WVTZ);
@@ -524,6 +526,7 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
     unsigned* next_item = A.cnt + 4 * bucket + 3;
     __shared__ unsigned s_idx;
     __shared__ int lm[N];  // layer material per z index (structures without blocks)
+    __shared__ DevGeom gs;  // the current job's geometry header
     VoxScratch<N>& vs =   // separable voxeliser (structures with blocks)
         *reinterpret_cast<VoxScratch<N>*>(smem + (WalkSmem<N>::base(maxP) + 15) / 16 * 16);
     int loaded = -1, P = 0;
@@ -549,6 +552,7 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
                 pair64[v] = J.g.pair64[v];
                 pair32[v] = J.g.pair32[v];
             }
+            if (threadIdx.x == 0) gs = J.g;
             loaded = j;
         }
         __syncthreads();
@@ -559,13 +563,13 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
         const int code = first ? A.st.code[slot] : DRWC_GFT;
         const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
         const double a = A.st.a[slot];
-        if (J.g.n_diel > 0) {
-            vox_prepare<N>(J.g, c, a, tco, vs);
+        if (gs.n_diel > 0) {
+            vox_prepare<N>(gs, c, a, tco, vs);
             for (int v = threadIdx.x; v < D::NNN; v += blockDim.x)
-                mat[v] = (uint8_t)vox_material<N>(J.g, vs, c, a, tco, v % N, (v / N) % N,
+                mat[v] = (uint8_t)vox_material<N>(gs, vs, c, a, tco, v % N, (v / N) % N,
                                                   v / D::NN, 0);
         } else {
-            voxelise_planes<N>(J.g, c, a, tco, mat, lm);
+            voxelise_planes<N>(gs, c, a, tco, mat, lm);
         }
         __syncthreads();
         FdmStats st;
