@@ -386,9 +386,13 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
         for (int o = 16; o > 0; o >>= 1) pm = fmaxf(pm, __shfl_xor_sync(0xffffffffu, pm, o));
         if (t == 0) vs.lmax = pm;
     }
-    if (t < 32) {  // warp 0 keeps the blocks that reach the cube, in block order
+    // warp 1 (warp 0 in CTAs of one warp) keeps the blocks that reach the
+    // cube, in block order, while warp 0 decides the layers
+    const int scan_warp = blockDim.x >= 64 ? 1 : 0;
+    if ((t >> 5) == scan_warp) {
+        const int lane = t & 31;
         for (int b0 = 0; b0 < g.n_diel; b0 += 32) {
-            const int b = b0 + t;
+            const int b = b0 + lane;
             int r[6] = {0, -1, 0, -1, 0, -1};
             bool hit = false;
             double Dv[6];
@@ -429,7 +433,7 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
             const unsigned m = __ballot_sync(0xffffffffu, hit);
             const int base = vs.nrel;
             if (hit) {
-                const int q = base + __popc(m & ((1u << t) - 1));
+                const int q = base + __popc(m & ((1u << lane) - 1));
                 if (q < kVoxMaxBlocks) {
 #pragma unroll
                     for (int e = 0; e < 6; ++e) vs.rel[q][e] = r[e];
@@ -437,7 +441,7 @@ DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const d
                 }
             }
             __syncwarp();
-            if (t == 0) vs.nrel = base + __popc(m);
+            if (lane == 0) vs.nrel = base + __popc(m);
             __syncwarp();
         }
     }
