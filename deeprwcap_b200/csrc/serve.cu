@@ -339,6 +339,25 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
     }
 }
 
+// The slot fields a network row's cube is built from.
+struct SvCubeHdr {
+    int slot, job, hops, code;
+    double px, py, pz, a;
+};
+
+DRWC_DEV SvCubeHdr sv_cube_hdr(const SvArgs& A, int bucket, int row) {
+    SvCubeHdr h;
+    h.slot = A.alist[bucket][row];
+    h.job = A.st.job[h.slot];
+    h.hops = A.st.hops[h.slot];
+    h.code = A.st.code[h.slot];
+    h.px = A.st.px[h.slot];
+    h.py = A.st.py[h.slot];
+    h.pz = A.st.pz[h.slot];
+    h.a = A.st.a[h.slot];
+    return h;
+}
+
 // Network rows in groups (two cubes at N = 16, one at 21 and 23), one group
 // at a time per CTA: each cube voxelised in shared memory (eps / max eps,
 // BF16) and the network's stem (conv1, conv2) applied to it on the tensor
@@ -353,11 +372,14 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
     __shared__ VoxScratch<N> vs;
     __shared__ float red[32];
     __shared__ DevGeom gs;  // the current job's geometry header: its fields are read per voxel pass
+    __shared__ SvCubeHdr hdr[D::CUBES];  // the group's cubes, fetched a group ahead
     const int na = (int)A.cnt[4 * bucket];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.stats + SV_NET_ROWS, (unsigned long long)na);
     if ((int)blockIdx.x * D::CUBES >= na) return;
     const NetStem& W = A.stem[bucket];
     centre_offsets<N>(tco);
+    if ((int)threadIdx.x < D::CUBES && (int)(blockIdx.x * D::CUBES + threadIdx.x) < na)
+        hdr[threadIdx.x] = sv_cube_hdr(A, bucket, blockIdx.x * D::CUBES + threadIdx.x);
     Stem<N> st{sv_stem_smem};
     st.begin(W);
     int loaded = -1;
@@ -365,27 +387,33 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
     for (int grp = blockIdx.x; ok && grp * D::CUBES < na; grp += gridDim.x) {
         const int g0 = grp * D::CUBES, nc = min(D::CUBES, na - g0);
         for (int cb = 0; ok && cb < nc; ++cb) {
-            const int slot = A.alist[bucket][g0 + cb];
-            const int j = A.st.job[slot];
-            const SvJob& J = A.jobs[j];
+            __syncthreads();  // hdr written; the previous cube's readers of pal and gs done
+            const SvCubeHdr h = hdr[cb];
+            const int j = h.job;  // the same in every thread: the branch below is uniform
             if (j != loaded) {
-                __syncthreads();
+                const SvJob& J = A.jobs[j];
                 for (int v = threadIdx.x; v < J.g.n_mat; v += blockDim.x) pal[v] = J.g.pal[v];
                 if (threadIdx.x == 0) gs = J.g;
                 loaded = j;
+                __syncthreads();
             }
-            __syncthreads();
-            const bool first = A.st.hops[slot] == 0;
-            const int rot = first ? rot_of_code(A.st.code[slot]) : 0;
-            const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
-            voxelise_net<N>(gs, c, A.st.a[slot], rot, tco, pal, st.mat(), st.xs(), nullptr, red, vs);
+            const bool first = h.hops == 0;
+            const int rot = first ? rot_of_code(h.code) : 0;
+            const double c[3] = {h.px, h.py, h.pz};
+            voxelise_net<N>(gs, c, h.a, rot, tco, pal, st.mat(), st.xs(), nullptr, red, vs);
             if (first && threadIdx.x == 0) {
                 const EpsPalette E{st.mat(), pal, nullptr, nullptr, nullptr, 0};
-                A.st.epsw[slot] = center_diel<N>(E, DRWC_WVTZ);
+                A.st.epsw[h.slot] = center_diel<N>(E, DRWC_WVTZ);
             }
             ok = st.conv1(cb, W.err);
         }
+        // the next group's cubes are fetched while conv2 runs
+        const int gn = (grp + (int)gridDim.x) * D::CUBES + (int)threadIdx.x;
+        const bool fetch = (int)threadIdx.x < D::CUBES && gn < na;
+        SvCubeHdr nh;
+        if (fetch) nh = sv_cube_hdr(A, bucket, gn);
         if (ok) ok = st.conv2(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err);
+        if (fetch) hdr[threadIdx.x] = nh;  // conv2 ended with a barrier: no cube reads hdr now
     }
     st.end();
 }
