@@ -486,14 +486,12 @@ DRWC_DEV int vox_material(const DevGeom& g, const VoxScratch<N>& vs, const doubl
     return vs.lm[oz];
 }
 
-// CTA-wide: voxelise one cube (rotated frame) into BF16 eps / max eps and,
-// optionally, FP64 eps. vs: shared scratch (separable voxelisation).
+// The cells of a cube whose vox_prepare has run (see voxelise_net).
 template <int N>
-DRWC_DEV void voxelise_net(const DevGeom& g, const double c[3], double a, int rot,
-                           const double* tco, const double* palsm, uint8_t* matsm,
-                           __nv_bfloat16* X, double* eps64, float* red, VoxScratch<N>& vs) {
+DRWC_DEV void voxelise_cells(const DevGeom& g, const double c[3], double a, int rot,
+                             const double* tco, const double* palsm, uint8_t* matsm,
+                             __nv_bfloat16* X, double* eps64, float* red, VoxScratch<N>& vs) {
     constexpr int NNN = N * N * N;
-    vox_prepare<N>(g, c, a, tco, vs, palsm);
     if (vs.nrel == 0) {
         // no block reaches the cube: a cell's material is its layer, one per
         // index along the original z axis, and the largest permittivity is
@@ -529,6 +527,16 @@ DRWC_DEV void voxelise_net(const DevGeom& g, const double c[3], double a, int ro
         if (eps64) eps64[v] = e;
     }
     __syncthreads();
+}
+
+// CTA-wide: voxelise one cube (rotated frame) into BF16 eps / max eps and,
+// optionally, FP64 eps. vs: shared scratch (separable voxelisation).
+template <int N>
+DRWC_DEV void voxelise_net(const DevGeom& g, const double c[3], double a, int rot,
+                           const double* tco, const double* palsm, uint8_t* matsm,
+                           __nv_bfloat16* X, double* eps64, float* red, VoxScratch<N>& vs) {
+    vox_prepare<N>(g, c, a, tco, vs, palsm);
+    voxelise_cells<N>(g, c, a, rot, tco, palsm, matsm, X, eps64, red, vs);
 }
 
 // log-sum-exp of M FP32 values over the CTA (all threads get it).

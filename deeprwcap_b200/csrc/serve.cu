@@ -373,6 +373,7 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
     __shared__ float red[32];
     __shared__ DevGeom gs;  // the current job's geometry header: its fields are read per voxel pass
     __shared__ SvCubeHdr hdr[D::CUBES];  // the group's cubes, fetched a group ahead
+    __shared__ __nv_bfloat16 pvs[N];     // per-index values of a cube no block reaches
     const int na = (int)A.cnt[4 * bucket];
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(A.stats + SV_NET_ROWS, (unsigned long long)na);
     if ((int)blockIdx.x * D::CUBES >= na) return;
@@ -400,12 +401,36 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
             const bool first = h.hops == 0;
             const int rot = first ? rot_of_code(h.code) : 0;
             const double c[3] = {h.px, h.py, h.pz};
-            voxelise_net<N>(gs, c, h.a, rot, tco, pal, st.mat(), st.xs(), nullptr, red, vs);
-            if (first && threadIdx.x == 0) {
-                const EpsPalette E{st.mat(), pal, nullptr, nullptr, nullptr, 0};
-                A.st.epsw[h.slot] = center_diel<N>(E, DRWC_WVTZ);
+            vox_prepare<N>(gs, c, h.a, tco, vs, pal);
+            int uaxis = -1;
+            if (vs.nrel == 0) {
+                // no block reaches the cube: its values vary along one index
+                // (the original z axis in the rotated frame), pvs holds them;
+                // the voxels themselves are not written
+                uaxis = rot == 1 ? 1 : rot == 2 ? 0 : 2;
+                const float inv = 1.f / vs.lmax;
+                if (threadIdx.x < N)
+                    pvs[threadIdx.x] = __float2bfloat16((float)pal[vs.lm[threadIdx.x]] * inv);
+                if (first && threadIdx.x == 0) {
+                    // the centre cells the permittivity at the centre is read from
+                    constexpr int cc = N / 2;
+                    for (int k = cc - 1; k <= cc; ++k)
+                        for (int jj = cc - 1; jj <= cc; ++jj)
+                            for (int i = cc - 1; i <= cc; ++i)
+                                st.mat()[(k * N + jj) * N + i] =
+                                    (uint8_t)vs.lm[rot == 1 ? jj : rot == 2 ? i : k];
+                    const EpsPalette E{st.mat(), pal, nullptr, nullptr, nullptr, 0};
+                    A.st.epsw[h.slot] = center_diel<N>(E, DRWC_WVTZ);
+                }
+                __syncthreads();
+            } else {
+                voxelise_cells<N>(gs, c, h.a, rot, tco, pal, st.mat(), st.xs(), nullptr, red, vs);
+                if (first && threadIdx.x == 0) {
+                    const EpsPalette E{st.mat(), pal, nullptr, nullptr, nullptr, 0};
+                    A.st.epsw[h.slot] = center_diel<N>(E, DRWC_WVTZ);
+                }
             }
-            ok = st.conv1(cb, W.err);
+            ok = st.conv1(cb, W.err, uaxis, pvs);
         }
         // the next group's cubes are fetched while conv2 runs
         const int gn = (grp + (int)gridDim.x) * D::CUBES + (int)threadIdx.x;

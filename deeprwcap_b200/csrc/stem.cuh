@@ -169,8 +169,13 @@ struct Stem {
         pending = aborted();  // after a timeout the MMAs may still be in flight
     }
 
-    // conv1 of the cube in xs() into a1(cube), up to R1 M tiles per batch.
-    DRWC_DEV bool conv1(int cube, int* err) {
+    // conv1 of the cube into a1(cube), up to R1 M tiles per batch, from the
+    // voxels in xs() or, with uaxis >= 0, from pv: the cube's values then
+    // vary along that index alone (0 = x, 1 = y, 2 = z; pv[t] is the value
+    // at index t), so a row's 27 taps come from three values and the grid
+    // bounds (the same values xs would hold).
+    DRWC_DEV bool conv1(int cube, int* err, int uaxis = -1,
+                        const __nv_bfloat16* __restrict__ pv = nullptr) {
         const __nv_bfloat16* x = xs();
         const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
         for (int m0 = 0; m0 < S::MT1; m0 += S::R1) {
@@ -183,14 +188,34 @@ struct Stem {
                 if (p < S::P2) {
                     const int pz = p / (S::D2 * S::D2), py = (p / S::D2) % S::D2, px = p % S::D2;
                     const int z0 = 2 * pz - 1, y0 = 2 * py - 1, x0 = 2 * px - 1;
+                    if (uaxis >= 0) {
+                        const int u0 = uaxis == 2 ? z0 : uaxis == 1 ? y0 : x0;
+                        uint32_t uv[3], ok[3];  // values along the axis; in-grid bits per axis
 #pragma unroll
-                    for (int tap = 0; tap < 27; ++tap) {
-                        const int z = z0 + tap / 9, y = y0 + (tap / 3) % 3, xx = x0 + tap % 3;
-                        const bool in = (unsigned)z < (unsigned)N && (unsigned)y < (unsigned)N &&
-                                        (unsigned)xx < (unsigned)N;
-                        const uint32_t v =
-                            in ? (uint32_t)__bfloat16_as_ushort(x[(z * N + y) * N + xx]) : 0u;
-                        pk[tap >> 1] |= v << (16 * (tap & 1));
+                        for (int d = 0; d < 3; ++d) {
+                            uv[d] = (unsigned)(u0 + d) < (unsigned)N
+                                        ? (uint32_t)__bfloat16_as_ushort(pv[u0 + d]) : 0u;
+                            ok[d] = ((unsigned)(x0 + d) < (unsigned)N ? 1u : 0u) |
+                                    ((unsigned)(y0 + d) < (unsigned)N ? 2u : 0u) |
+                                    ((unsigned)(z0 + d) < (unsigned)N ? 4u : 0u);
+                        }
+#pragma unroll
+                        for (int tap = 0; tap < 27; ++tap) {
+                            const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+                            const bool in = (ok[dx] & 1u) && (ok[dy] & 2u) && (ok[dz] & 4u);
+                            const uint32_t v = uaxis == 2 ? uv[dz] : uaxis == 1 ? uv[dy] : uv[dx];
+                            pk[tap >> 1] |= (in ? v : 0u) << (16 * (tap & 1));
+                        }
+                    } else {
+#pragma unroll
+                        for (int tap = 0; tap < 27; ++tap) {
+                            const int z = z0 + tap / 9, y = y0 + (tap / 3) % 3, xx = x0 + tap % 3;
+                            const bool in = (unsigned)z < (unsigned)N &&
+                                            (unsigned)y < (unsigned)N && (unsigned)xx < (unsigned)N;
+                            const uint32_t v =
+                                in ? (uint32_t)__bfloat16_as_ushort(x[(z * N + y) * N + xx]) : 0u;
+                            pk[tap >> 1] |= v << (16 * (tap & 1));
+                        }
                     }
                 }
                 unsigned char* base = opa() + j * 8192 + (r >> 3) * 256 + (r & 7) * 16;
