@@ -374,23 +374,36 @@ struct VoxScratch {
 
 template <int N>
 DRWC_DEV void vox_prepare(const DevGeom& g, const double c[3], double a, const double* tco,
-                          VoxScratch<N>& vs, const double* palsm = nullptr) {
+                          VoxScratch<N>& vs, const double* palsm = nullptr,
+                          __nv_bfloat16* pv = nullptr) {
     const int t = threadIdx.x;
-    if (t < 3 * N) vs.crd[t / N][t % N] = dadd(c[t / N], dmul(a, tco[t % N]));
-    if (t == 0) vs.nrel = 0;
-    __syncthreads();
-    if (t < N) vs.lm[t] = g.n_layers > 0 ? g.lmat[layer_index(g, vs.crd[2][t])] : 0;
+    // warp 0: the layer of each z index, from the lane's own coordinate, and
+    // the largest layer permittivity; with pv set, pv[t] = the BF16 value
+    // (eps / largest) of z index t, which is the cube's value at every cell
+    // of that index when no block reaches the cube
     if (t < 32) {
         const double* pal = palsm ? palsm : g.pal;
-        float pm = t < N ? (float)pal[vs.lm[t]] : 0.f;
+        float pm = 0.f;
+        int m = 0;
+        if (t < N) {
+            const double z = dadd(c[2], dmul(a, tco[t]));
+            m = g.n_layers > 0 ? g.lmat[layer_index(g, z)] : 0;
+            vs.lm[t] = m;
+            pm = (float)pal[m];
+        }
         for (int o = 16; o > 0; o >>= 1) pm = fmaxf(pm, __shfl_xor_sync(0xffffffffu, pm, o));
         if (t == 0) vs.lmax = pm;
+        if (pv && t < N) pv[t] = __float2bfloat16((float)pal[m] * (1.f / pm));
     }
-    // warp 1 (warp 0 in CTAs of one warp) keeps the blocks that reach the
-    // cube, in block order, while warp 0 decides the layers
+    // warp 1 (warp 0 in CTAs of one warp): the cell-centre coordinates, then
+    // the blocks that reach the cube, in block order, while warp 0 decides
+    // the layers
     const int scan_warp = blockDim.x >= 64 ? 1 : 0;
     if ((t >> 5) == scan_warp) {
         const int lane = t & 31;
+        for (int q = lane; q < 3 * N; q += 32) vs.crd[q / N][q % N] = dadd(c[q / N], dmul(a, tco[q % N]));
+        if (lane == 0) vs.nrel = 0;
+        __syncwarp();
         for (int b0 = 0; b0 < g.n_diel; b0 += 32) {
             const int b = b0 + lane;
             int r[6] = {0, -1, 0, -1, 0, -1};

@@ -401,16 +401,13 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
             const bool first = h.hops == 0;
             const int rot = first ? rot_of_code(h.code) : 0;
             const double c[3] = {h.px, h.py, h.pz};
-            vox_prepare<N>(gs, c, h.a, tco, vs, pal);
+            vox_prepare<N>(gs, c, h.a, tco, vs, pal, pvs);
             int uaxis = -1;
             if (vs.nrel == 0) {
                 // no block reaches the cube: its values vary along one index
                 // (the original z axis in the rotated frame), pvs holds them;
                 // the voxels themselves are not written
                 uaxis = rot == 1 ? 1 : rot == 2 ? 0 : 2;
-                const float inv = 1.f / vs.lmax;
-                if (threadIdx.x < N)
-                    pvs[threadIdx.x] = __float2bfloat16((float)pal[vs.lm[threadIdx.x]] * inv);
                 if (first && threadIdx.x == 0) {
                     // the centre cells the permittivity at the centre is read from
                     constexpr int cc = N / 2;
@@ -422,7 +419,6 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
                     const EpsPalette E{st.mat(), pal, nullptr, nullptr, nullptr, 0};
                     A.st.epsw[h.slot] = center_diel<N>(E, DRWC_WVTZ);
                 }
-                __syncthreads();
             } else {
                 voxelise_cells<N>(gs, c, h.a, rot, tco, pal, st.mat(), st.xs(), nullptr, red, vs);
                 if (first && threadIdx.x == 0) {
