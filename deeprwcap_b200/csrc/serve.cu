@@ -388,7 +388,10 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
     for (int grp = blockIdx.x; ok && grp * D::CUBES < na; grp += gridDim.x) {
         const int g0 = grp * D::CUBES, nc = min(D::CUBES, na - g0);
         for (int cb = 0; ok && cb < nc; ++cb) {
-            __syncthreads();  // hdr written; the previous cube's readers of pal and gs done
+            // the group's headers were written after the previous group's last
+            // barrier; later cubes follow conv1's closing barrier, which the
+            // readers of pal and gs have passed
+            if (cb == 0) __syncthreads();
             const SvCubeHdr h = hdr[cb];
             const int j = h.job;  // the same in every thread: the branch below is uniform
             if (j != loaded) {
