@@ -6,14 +6,16 @@
 // (two cubes at N = 16: 4^3 = 64 rows each) or a single cube (N = 21, 23:
 // 6^3 = 216 rows over two tiles). Per cube, conv1 (1 -> 16 channels, 3^3,
 // stride 2, zero padding) is an implicit GEMM [D2^3 x 32] x [32 x 16]: the
-// threads write the im2col rows of up to four 128-row M tiles (taps 27..31
-// zero) into a staging area in the canonical K-major no-swizzle layout, one
+// threads write the im2col rows of up to four (N = 16) or eight (N = 21,
+// 23) 128-row M tiles (taps 27..31 zero) into a staging area in the
+// canonical K-major no-swizzle layout, one
 // thread issues two tcgen05.mma (K = 16) per tile into its own 16 TMEM
 // columns, and the epilogue (tcgen05.ld, bias, ReLU, BF16) writes the rows
 // into the group's conv1 activations [cube][D2^3][16] in shared memory.
 // conv2 (16 -> 32 channels) then gathers its im2col rows from there, nine
-// taps (K steps) per staging fill, accumulates each 128-row tile in 32 TMEM
-// columns and writes its activations [row][32] (BF16, channels last) to
+// taps (K steps) of every tile of the group per staging fill, accumulates
+// each 128-row tile in 32 TMEM columns and writes its activations [row][32]
+// (BF16, channels last) to
 // global memory, where the tile GEMMs of conv3 and the heads read them.
 //
 // Operands are the BF16 values the stand-alone convolution GEMMs read and
@@ -41,13 +43,20 @@ struct StemDims {
     static constexpr int ROWS2 = CUBES * P3;                         // conv2 rows per group
     static constexpr int MT2 = (ROWS2 + kUmmaM - 1) / kUmmaM;       // conv2 M tiles
     static constexpr int MT1 = (P2 + kUmmaM - 1) / kUmmaM;          // conv1 M tiles per cube
-    static constexpr int R1 = 4;     // conv1 M tiles per MMA batch (16 TMEM columns each)
-    static constexpr int TAPS = 9;   // conv2 taps (K steps of 16) per MMA batch
     static constexpr int NT = N <= 16 ? 256 : 512;
     static constexpr int CTAS = N <= 16 ? 2 : 1;
-    static_assert(MT2 <= 2, "conv2 accumulators: columns 64..127");
+    // conv1 M tiles per MMA batch (16 TMEM columns each): N = 21 / 23 cubes
+    // (11 / 14 tiles) take eight, so a cube needs two batches
+    static constexpr int R1 = N <= 16 ? 4 : 8;
+    static constexpr int TAPS = 9;         // conv2 taps (K steps of 16) per MMA batch
+    static constexpr int MT2B = NT / 256;  // conv2 M tiles per batch: one per 256 threads
+    static_assert(MT2 <= MT2B, "one conv2 batch holds every tile of a group");
+    static constexpr int C2 = 16 * R1;     // first TMEM column of the conv2 accumulators
+    static constexpr uint32_t TCOLS = N <= 16 ? 128 : 256;
+    static_assert(C2 + 32 * MT2 <= (int)TCOLS, "conv2 accumulators after conv1's columns");
     // dynamic shared memory (bytes); every operand block is 1024-aligned
-    static constexpr int OPA = R1 * 8192 > TAPS * 4096 ? R1 * 8192 : TAPS * 4096;
+    static constexpr int OPA =
+        R1 * 8192 > MT2B * TAPS * 4096 ? R1 * 8192 : MT2B * TAPS * 4096;
     static constexpr int W2B = 27 * 32 * 32;  // conv2 weights: 27 K steps x 32 rows x 32 B
     static constexpr int W1B = 2 * 16 * 32;   // conv1 weights: 2 K steps x 16 rows x 32 B
     static constexpr int A1B = CUBES * P2 * 32;
@@ -57,7 +66,6 @@ struct StemDims {
                          O_MAT = O_XS + XSB, O_B1 = O_MAT + MATB, O_B2 = O_B1 + 16 * 4,
                          O_BAR = O_B2 + 32 * 4, O_TSLOT = O_BAR + 8, O_ABORT = O_TSLOT + 4,
                          BYTES = (O_ABORT + 4 + 15) / 16 * 16;
-    static constexpr uint32_t TCOLS = 128;  // conv1: 4 x 16 columns; conv2: from column 64
 };
 
 // 16 columns of the warp's 32 TMEM lanes.
@@ -252,14 +260,16 @@ struct Stem {
     DRWC_DEV bool conv2(int nc, __nv_bfloat16* __restrict__ a2, int* err) {
         const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
         static_assert(S::TAPS == 9 && S::NT % 256 == 0, "a fill is one dz plane of taps");
-        // every thread keeps one (row, channel half) of the tile and walks
-        // the taps of each fill: the row's position is decoded once
-        const int pr = t & 255, r = pr >> 1, h = pr & 1;
-        unsigned char* dst = opa() + (r >> 3) * 256 + h * 128 + (r & 7) * 16;
-        for (int mt = 0; mt < S::MT2; ++mt) {
+        // every thread keeps one (row, channel half) of one tile (256 threads
+        // per tile) and walks the taps of each fill: the row's position is
+        // decoded once; a batch holds every tile of the group
+        const int pr = t & 255, r = pr >> 1, h = pr & 1, mt = t >> 8;
+        unsigned char* dst =
+            opa() + mt * (S::TAPS * 4096) + (r >> 3) * 256 + h * 128 + (r & 7) * 16;
+        {
             const int R = mt * kUmmaM + r;
             const int cube = R / S::P3, p = R % S::P3;
-            const bool row_ok = R < S::ROWS2 && cube < nc;
+            const bool row_ok = mt < S::MT2 && R < S::ROWS2 && cube < nc;
             const int z0 = 2 * (p / (S::D3 * S::D3)) - 1, y0 = 2 * ((p / S::D3) % S::D3) - 1,
                       x0 = 2 * (p % S::D3) - 1;
             unsigned yx_ok = 0;  // bit dy * 3 + dx: that tap's (y, x) lies inside the grid
@@ -271,22 +281,26 @@ struct Stem {
             for (int cc = 0; cc < 3; ++cc) {  // fill cc holds the taps with dz = cc
                 const int z = z0 + cc;
                 const bool z_ok = row_ok && (unsigned)z < (unsigned)S::D2;
+                if (mt < S::MT2) {
 #pragma unroll
-                for (int ti = S::NT == 256 ? 0 : t >> 8; ti < 9; ti += S::NT / 256) {
-                    uint4 val = make_uint4(0u, 0u, 0u, 0u);
-                    if (z_ok && ((yx_ok >> ti) & 1u))
-                        val = *reinterpret_cast<const uint4*>(
-                            src0 + (size_t)((z * S::D2 + y0 + ti / 3) * S::D2 + x0 + ti % 3) * 16);
-                    *reinterpret_cast<uint4*>(dst + ti * 4096) = val;
+                    for (int ti = 0; ti < 9; ++ti) {
+                        uint4 val = make_uint4(0u, 0u, 0u, 0u);
+                        if (z_ok && ((yx_ok >> ti) & 1u))
+                            val = *reinterpret_cast<const uint4*>(
+                                src0 + (size_t)((z * S::D2 + y0 + ti / 3) * S::D2 + x0 + ti % 3) * 16);
+                        *reinterpret_cast<uint4*>(dst + ti * 4096) = val;
+                    }
                 }
                 if (!staged()) return false;
                 if (t == 0) {
-                    for (int ti = 0; ti < S::TAPS; ++ti)
-                        umma_bf16(tmem + 64 + 32 * mt,
-                                  umma_smem_desc(smem_u32(opa() + ti * 4096), 128, 256),
-                                  umma_smem_desc(smem_u32(sm + S::O_W2 + (cc * S::TAPS + ti) * 1024),
-                                                 128, 256),
-                                  umma_idesc_bf16<32>(), (cc | ti) ? 1u : 0u);
+                    for (int j = 0; j < S::MT2; ++j)
+                        for (int ti = 0; ti < S::TAPS; ++ti)
+                            umma_bf16(tmem + S::C2 + 32 * j,
+                                      umma_smem_desc(smem_u32(opa() + j * (S::TAPS * 4096) + ti * 4096),
+                                                     128, 256),
+                                      umma_smem_desc(
+                                          smem_u32(sm + S::O_W2 + (cc * S::TAPS + ti) * 1024), 128, 256),
+                                      umma_idesc_bf16<32>(), (cc | ti) ? 1u : 0u);
                     umma_commit(bar());
                 }
                 complete(err);
@@ -296,7 +310,7 @@ struct Stem {
         for (int task = sub; task < 2 * S::MT2; task += S::NT / 128) {
             const int mt = task >> 1, half = task & 1;
             float v[16];
-            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + 64 + 32 * mt + 16 * half, v);
+            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + S::C2 + 32 * mt + 16 * half, v);
             const int R = mt * kUmmaM + 32 * q + lane;
             if (R < S::ROWS2 && R / S::P3 < nc)
                 stem_store16(v, b2() + 16 * half, a2 + (size_t)R * 32 + 16 * half);
