@@ -360,8 +360,10 @@ DRWC_DEV SvCubeHdr sv_cube_hdr(const SvArgs& A, int bucket, int row) {
 
 // Network rows in groups (two cubes at N = 16, one at 21 and 23), one group
 // at a time per CTA: each cube voxelised in shared memory (eps / max eps,
-// BF16) and the network's stem (conv1, conv2) applied to it on the tensor
-// cores there, so only conv2's activations reach global memory.
+// BF16; a cube that no dielectric block reaches is kept as its N per-index
+// values) and the network's stem (conv1, conv2) applied to it on the tensor
+// cores there, so only conv2's activations reach global memory. The next
+// group's cube headers are fetched while conv2 runs.
 template <int N>
 __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
     sv_stem_kernel(SvArgs A, int bucket) {

@@ -8,15 +8,14 @@
 // stride 2, zero padding) is an implicit GEMM [D2^3 x 32] x [32 x 16]: the
 // threads write the im2col rows of up to four (N = 16) or eight (N = 21,
 // 23) 128-row M tiles (taps 27..31 zero) into a staging area in the
-// canonical K-major no-swizzle layout, one
-// thread issues two tcgen05.mma (K = 16) per tile into its own 16 TMEM
-// columns, and the epilogue (tcgen05.ld, bias, ReLU, BF16) writes the rows
-// into the group's conv1 activations [cube][D2^3][16] in shared memory.
-// conv2 (16 -> 32 channels) then gathers its im2col rows from there, nine
-// taps (K steps) of every tile of the group per staging fill, accumulates
-// each 128-row tile in 32 TMEM columns and writes its activations [row][32]
-// (BF16, channels last) to
-// global memory, where the tile GEMMs of conv3 and the heads read them.
+// canonical K-major no-swizzle layout, one thread issues two tcgen05.mma
+// (K = 16) per tile into its own 16 TMEM columns, and the epilogue
+// (tcgen05.ld, bias, ReLU, BF16) writes the rows into the group's conv1
+// activations [cube][D2^3][16] in shared memory. conv2 (16 -> 32 channels)
+// then gathers its im2col rows from there, nine taps (K steps) of every
+// tile of the group per staging fill, accumulates each 128-row tile in 32
+// TMEM columns and writes its activations [row][32] (BF16, channels last)
+// to global memory, where the tile GEMMs of conv3 and the heads read them.
 //
 // Operands are the BF16 values the stand-alone convolution GEMMs read and
 // each MMA sums in FP32, so a row's result does not depend on the other rows
