@@ -382,7 +382,7 @@ def run_b200(args, world, rank, local):
     end = torch.empty(B, dtype=torch.int32, device=dev)
     hops = torch.empty(B, dtype=torch.int32, device=dev)
     wt = torch.empty(B, dtype=torch.float64, device=dev)
-    stats = torch.zeros((args.steps + args.warmup + 1, 3), dtype=torch.int64, device=dev)
+    stats = torch.zeros((args.steps + args.warmup + 1, 5), dtype=torch.int64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
     base = rank * (args.steps + args.warmup) * B
 
@@ -417,7 +417,7 @@ def run_b200(args, world, rank, local):
     step_ms = [a.elapsed_time(b) for a, b in evs]
     t_dev = sum(step_ms) / 1e3
     st = stats[args.warmup:args.warmup + args.steps].cpu().numpy()
-    hops_tot, iters_tot, sweeps_tot = (int(x) for x in st.sum(axis=0))
+    hops_tot, iters_tot, sweeps_tot, esc_tot, fail_tot = (int(x) for x in st.sum(axis=0))
     # max over ranks of device time, sum of hops
     if world > 1:
         t = torch.tensor([t_dev, float(hops_tot)], dtype=torch.float64, device=dev)
@@ -504,7 +504,8 @@ def run_b200(args, world, rank, local):
                        "l2": "flushed between steps (256 MB write)",
                        "hops_per_step": hops_tot / args.steps,
                        "fp32_iters_per_hop": iters_tot / max(1, hops_tot),
-                       "fp64_sweeps_per_hop": sweeps_tot / max(1, hops_tot)},
+                       "fp64_sweeps_per_hop": sweeps_tot / max(1, hops_tot),
+                       "solves_escalated": esc_tot, "solves_failed": fail_tot},
             "e2e": e2e,
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",

@@ -60,10 +60,11 @@ class DrwcError(RuntimeError):
 class FdmOpts(C.Structure):
     _fields_ = [("tol", C.c_double), ("inner_tol", C.c_double),
                 ("max_outer", C.c_int32), ("max_inner", C.c_int32),
-                ("warm_start", C.c_int32), ("reserved_", C.c_int32)]
+                ("warm_start", C.c_int32), ("extra_outer", C.c_int32)]
 
-    def __init__(self, tol=1e-10, inner_tol=1e-5, max_outer=8, max_inner=0, warm_start=1):
-        super().__init__(tol, inner_tol, max_outer, max_inner, warm_start, 0)
+    def __init__(self, tol=1e-10, inner_tol=1e-5, max_outer=8, max_inner=0, warm_start=1,
+                 extra_outer=8):
+        super().__init__(tol, inner_tol, max_outer, max_inner, warm_start, extra_outer)
 
 
 class Box(C.Structure):
@@ -117,7 +118,7 @@ class ServerStats(C.Structure):
         [(n, C.c_double) for n in ("busy_seconds", "fdm_seconds", "net_seconds", "net_rows",
                                    "audit_kl_mean")] + \
         [("fdm_iters", C.c_int64), ("fdm_sweeps", C.c_int64), ("fdm_bytes", C.c_double),
-         ("table_hops", C.c_int64)]
+         ("table_hops", C.c_int64), ("fdm_escalated", C.c_int64), ("fdm_failed", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -125,7 +126,8 @@ class ServerStats(C.Structure):
 
 class JobResult(C.Structure):
     _fields_ = [("n_entries", C.c_int32), ("converged", C.c_int32), ("walks", C.c_int64),
-                ("hops", C.c_int64), ("lost", C.c_int64), ("seconds", C.c_double),
+                ("hops", C.c_int64), ("lost", C.c_int64), ("solves_escalated", C.c_int64),
+                ("solves_failed", C.c_int64), ("seconds", C.c_double),
                 ("cap", C.c_double * (MAX_NETS + 1)), ("stderr_", C.c_double * (MAX_NETS + 1))]
 
 

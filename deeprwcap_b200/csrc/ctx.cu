@@ -3,6 +3,10 @@
 
 #include "host.cuh"
 
+namespace drwc {
+int noalloc_prepare(drwc_ctx* ctx);  // fdm_noalloc.cu
+}
+
 extern "C" {
 
 DRWC_API const char* drwc_version(void) { return "deeprwcap-b200 0.1.0 (sm_100a)"; }
@@ -40,6 +44,14 @@ DRWC_API int drwc_ctx_create(int device, drwc_ctx** out) {
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return DRWC_ERR_CUDA;
+    }
+    // the no-allocation solver's static arrays, set up here rather than in
+    // its first call (once per device)
+    const int rc = drwc::noalloc_prepare(c);
+    if (rc) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return rc;
     }
     *out = c;
     return DRWC_OK;

@@ -114,7 +114,7 @@ query_kernel(int n, const float* __restrict__ layers, const float* __restrict__ 
         FdmStats st;
         cube_solve<N>(EpsGlobal{es}, ys, ss, code, prm, &st);
         double* w = reinterpret_cast<double*>(sm.stage());  // 6N^2 doubles over p|cx|cy|cz
-        for_each_panel<N>(EpsGlobal{es}, ys, [&](int b, double v) { w[b] = v; });
+        for_each_panel<N>(EpsGlobal{es}, cube_y<N>(ys), [&](int b, double v) { w[b] = v; });
         __syncthreads();
         const double u = philox_uniform2(seed, stream + (uint64_t)q, 0, 0).x;
         double tot = 0.0;

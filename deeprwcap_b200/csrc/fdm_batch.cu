@@ -43,7 +43,7 @@ fdm_batch_kernel(int nsel, const int32_t* __restrict__ sel, const double* __rest
         if (st.status == 2) {
             for (int b = threadIdx.x; b < 6 * D::NN; b += blockDim.x) o[b] = 0.0;
         } else {
-            for_each_panel<N>(EpsGlobal{e}, ys, [&](int b, double v) { o[b] = v; });
+            for_each_panel<N>(EpsGlobal{e}, cube_y<N>(ys), [&](int b, double v) { o[b] = v; });
         }
         if (threadIdx.x == 0) {
             if (iters) iters[c] = st.iters;
@@ -87,6 +87,7 @@ FdmParams make_params(const drwc_fdm_opts* o, int N) {
     p.inner_tol = (float)(o->inner_tol > 0 ? o->inner_tol : d.inner_tol);
     p.max_outer = o->max_outer > 0 ? o->max_outer : d.max_outer;
     p.max_inner = o->max_inner > 0 ? o->max_inner : 4 * N * N;
+    p.extra_outer = o->extra_outer > 0 ? o->extra_outer : 0;
     for (int c = 0; c < 4; ++c) p.warm[c] = nullptr;  // set by the caller (warm_tables)
     return p;
 }
@@ -104,7 +105,7 @@ DRWC_API void drwc_fdm_opts_default(drwc_fdm_opts* opts) {
     opts->max_outer = 8;
     opts->max_inner = 0;
     opts->warm_start = 1;
-    opts->reserved_ = 0;
+    opts->extra_outer = 8;
 }
 
 DRWC_API int drwc_fdm_solve_batch_device(drwc_ctx* ctx, int ncubes, const int32_t* N,

@@ -34,6 +34,11 @@ struct FdmParams {
     float inner_tol;   // relative residual reduction per FP32 sweep
     int max_outer;     // FP64 refinement sweeps
     int max_inner;     // FP32 CG iterations per sweep
+    // Escalation: a cube still above tol after max_outer sweeps gets up to
+    // extra_outer more, each with 4 * max_inner iterations, before it is
+    // reported not converged (ggft falls back to a direct solve when its
+    // iterative one fails, ggft_solver.cpp:565-589).
+    int extra_outer;
     // Warm start per solver code (GFT, WVTZ, WVTX, WVTY): the cube solution
     // x = eps .* y of the uniform-permittivity problem (N^3 doubles), or null
     // for a cold start. ggft starts every solve from the same uniform
@@ -48,6 +53,7 @@ struct FdmStats {
     int sweeps;      // FP64 residual evaluations (refinement sweeps + final check)
     double relres;   // final ||e - K y|| / ||e||
     int status;      // 0 converged, 1 not converged, 2 invalid permittivity
+    int escalated;   // 1 when sweeps beyond max_outer were needed
 };
 
 #ifndef DRWC_CG_ONE_REDUCTION
@@ -56,11 +62,18 @@ struct FdmStats {
 #ifndef DRWC_SPLIT_MAX_N
 #define DRWC_SPLIT_MAX_N 0
 #endif
+// Largest N whose FP64 solution y lives in shared memory during the solve
+// (8 B per cell more; at N = 16 two cube CTAs still fit on one SM). Larger
+// cubes keep y in the caller's global scratch.
+#ifndef DRWC_YSMEM_MAX_N
+#define DRWC_YSMEM_MAX_N 16
+#endif
 
 template <int N>
 struct Cube {
     static constexpr int NN = N * N;
     static constexpr int NNN = N * N * N;
+    static constexpr bool YSMEM = N <= DRWC_YSMEM_MAX_N;
     // Threads per z-column: two (each owning half of the column) while 2*N^2
     // threads fit in a CTA, else one.
     static constexpr int SPLIT = (N <= DRWC_SPLIT_MAX_N && 2 * NN <= 1024) ? 2 : 1;
@@ -71,13 +84,15 @@ struct Cube {
     static constexpr int LEN = NNN + 2 * PAD;
     // dynamic shared memory: [red: 2*NW+8 doubles][rhs: 8 int + 8 double]
     //                        [flags: 8 int][p | cx | cy | cz : LEN floats each]
+    //                        [y: N^3 doubles, when YSMEM]
     static constexpr size_t kRedOff = 0;
     static constexpr size_t kRhsIdxOff = kRedOff + sizeof(double) * (2 * NW + 8);
     static constexpr size_t kRhsValOff = kRhsIdxOff + sizeof(int) * kMaxRhs;
     static constexpr size_t kFlagOff = kRhsValOff + sizeof(double) * kMaxRhs;
     static constexpr size_t kArrOff = ((kFlagOff + sizeof(int) * 8 + 127) / 128) * 128;
     static constexpr size_t kArrBytes = ((sizeof(float) * LEN + 15) / 16) * 16;
-    static constexpr size_t kSmemBytes = kArrOff + 4 * kArrBytes;
+    static constexpr size_t kYOff = kArrOff + 4 * kArrBytes;
+    static constexpr size_t kSmemBytes = kYOff + (YSMEM ? sizeof(double) * NNN : 0);
     static_assert(kSmemBytes <= 227 * 1024, "cube does not fit in shared memory");
 };
 
@@ -91,6 +106,7 @@ struct CubeSmem {
     float* cx;
     float* cy;
     float* cz;
+    double* y;       // the FP64 solution (YSMEM), else null
     DRWC_DEV static CubeSmem carve(unsigned char* base) {
         using D = Cube<N>;
         CubeSmem s;
@@ -104,6 +120,7 @@ struct CubeSmem {
         s.cx = a + stride + D::PAD;
         s.cy = a + 2 * stride + D::PAD;
         s.cz = a + 3 * stride + D::PAD;
+        s.y = D::YSMEM ? reinterpret_cast<double*>(base + D::kYOff) : nullptr;
         return s;
     }
     // Raw start of the p|cz region (2 arrays) for staging FP64 input.
@@ -318,10 +335,12 @@ struct CubeTraits {
 
 // --------------------------------------------------------------- the solver
 // eps:  permittivity source (EpsGlobal / EpsPalette), cell i + j*N + k*N*N.
-// ys:   N^3 doubles of global scratch (the FP64 solution y of K y = e).
-// ss:   N^3 floats of global scratch (the Jacobi scale S).
-// On return (all threads) ys holds y and the stats are filled; shared memory
-// p/cx/cy/cz are free for the caller.
+// ys:   N^3 doubles of global scratch for the FP64 solution y of K y = e
+//       (unused when Cube<N>::YSMEM: y then lives in shared memory).
+// ss:   N^3 floats of global scratch (the Jacobi scale S, each thread's own
+//       cells only).
+// On return (all threads) cube_y<N>(ys) holds y and the stats are filled;
+// shared memory p/cx/cy/cz are free for the caller.
 #ifndef DRWC_SOLVE_INLINE
 #define DRWC_SOLVE_INLINE 0
 #endif
@@ -335,6 +354,14 @@ struct CubeTraits {
 // Carving them from this symbol (not from pointers handed in) lets the
 // compiler address them as shared memory.
 extern __shared__ __align__(128) unsigned char drwc_dyn_smem[];
+
+// Where cube_solve leaves the solution y: shared memory for N <= the YSMEM
+// bound, else the caller's global scratch.
+template <int N>
+DRWC_DEV const double* cube_y(const double* ys) {
+    if constexpr (Cube<N>::YSMEM) return CubeSmem<N>::carve(drwc_dyn_smem).y;
+    else return ys;
+}
 
 template <int N, class E>
 DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __restrict__ ss,
@@ -352,9 +379,13 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
     const int k0 = active ? (t / NN) * KH : 0;       // first k of this thread's cells
     const int kend = active ? min(k0 + KH, N) : 0;    // one past the last k
     auto own = [&](int kk) { return k0 + kk < kend; };
+    double* __restrict__ Y;
+    if constexpr (D::YSMEM) Y = sm.y;
+    else Y = ys;
 
-    // ---- setup 1: validity, Jacobi scale S = diag(K)^-1/2 (FP32), y = the
-    //      warm start (or 0), guards zeroed, right-hand side.
+    // ---- setup 1: validity, Jacobi scale S = diag(K)^-1/2 (FP32; into p,
+    //      which is free until the CG starts, and into ss), y = the warm
+    //      start (or 0), guards zeroed, right-hand side.
     const double* __restrict__ warm = prm.warm[code & 3];
     if (t == 0) sm.flags[1] = 0;
     for (int g = t; g < D::PAD; g += D::NT) {
@@ -367,8 +398,10 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
     __syncthreads();
     {
         bool bad = false;
-#pragma unroll 1
-        for (int k = k0; k < kend; ++k) {
+#pragma unroll
+        for (int kk = 0; kk < KH; ++kk) {
+            if (!own(kk)) continue;
+            const int k = k0 + kk;
             const int c = col + k * NN;
             bad |= !eps.valid(c);
             const float ec = eps.e32(c);
@@ -379,37 +412,46 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
             d += (j > 0) ? eps.g32(c, c - N) : ec;
             d += (k + 1 < N) ? eps.g32(c, c + NN) : ec;
             d += (k > 0) ? eps.g32(c, c - NN) : ec;
-            ss[c] = rsqrtf(d);
-            ys[c] = warm ? warm[c] * eps.inv64(c) : 0.0;
+            const float sc = rsqrtf(d);
+            sm.p[c] = sc;
+            ss[c] = sc;
+            Y[c] = warm ? warm[c] * eps.inv64(c) : 0.0;
         }
         if (bad) atomicOr(&sm.flags[1], 1);
     }
     __syncthreads();
     if (sm.flags[1]) {
         st->status = 2; st->iters = 0; st->sweeps = 0; st->relres = CUDART_NAN;
+        st->escalated = 0;
         return;
     }
-    // ---- setup 2: scaled link coefficients cx/cy/cz = g * S_p * S_q.
-#pragma unroll 1
-    for (int k = k0; k < kend; ++k) {
-        const int c = col + k * NN;
-        const float sc = ss[c];
-        float vx = 0.f, vy = 0.f, vz = 0.f;
-        if (i + 1 < N) vx = eps.g32(c, c + 1) * sc * ss[c + 1];
-        if (j + 1 < N) vy = eps.g32(c, c + N) * sc * ss[c + N];
-        if (k + 1 < N) vz = eps.g32(c, c + NN) * sc * ss[c + NN];
-        sm.cx[c] = vx; sm.cy[c] = vy; sm.cz[c] = vz;
-    }
-    // ||e|| (FP64) from the rhs table
+    // ||e|| (FP64) from the rhs table; which of this thread's cells carry a
+    // source term (bit kk)
     double enorm2 = 0.0;
     const int nrhs = sm.flags[0];
-    for (int v = 0; v < nrhs; ++v) enorm2 += sm.rhs_val[v] * sm.rhs_val[v];
+    unsigned int rmask = 0u;
+    for (int v = 0; v < nrhs; ++v) {
+        const double ev = sm.rhs_val[v];
+        enorm2 += ev * ev;
+        const int cell = sm.rhs_idx[v];
+        const int kk = cell / NN - k0;
+        if (active && cell % NN == col && kk >= 0 && kk < KH) rmask |= 1u << kk;
+    }
     const double enorm = sqrt(enorm2);
 
     float r[KH], x[KH], q[KH], pr[(PR || DRWC_CG_ONE_REDUCTION) ? KH : 1];
     // FP64 residual r64 = e - K y into the next inner rhs b = S r64 (FP32
-    // registers); returns ||r64|| / ||e|| (all threads).
-    auto residual = [&]() -> double {
+    // registers); returns ||r64|| / ||e|| (all threads). first: the sweep
+    // from the warm start, where S is still in p and (y in global scratch)
+    // the neighbours' y are formed from the warm table instead of being read
+    // back from scratch the other threads just wrote.
+    auto residual = [&](bool first) -> double {
+        auto yv = [&](int cell) -> double {
+            if constexpr (!D::YSMEM) {
+                if (first) return warm[cell] * eps.inv64(cell);
+            }
+            return Y[cell];
+        };
         double rn2 = 0.0;
 #pragma unroll
         for (int kk = 0; kk < KH; ++kk) {
@@ -417,20 +459,22 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
             const int k = k0 + kk;
             const int c = col + k * NN;
             const double ec = eps.e64(c);
-            const double yc = ys[c];
+            const double yc = Y[c];
             double diag = 0.0, off = 0.0;
-            if (i + 1 < N) { const double g = eps.g64(c, c + 1); diag += g; off += g * ys[c + 1]; } else diag += ec;
-            if (i > 0) { const double g = eps.g64(c, c - 1); diag += g; off += g * ys[c - 1]; } else diag += ec;
-            if (j + 1 < N) { const double g = eps.g64(c, c + N); diag += g; off += g * ys[c + N]; } else diag += ec;
-            if (j > 0) { const double g = eps.g64(c, c - N); diag += g; off += g * ys[c - N]; } else diag += ec;
-            if (k + 1 < N) { const double g = eps.g64(c, c + NN); diag += g; off += g * ys[c + NN]; } else diag += ec;
-            if (k > 0) { const double g = eps.g64(c, c - NN); diag += g; off += g * ys[c - NN]; } else diag += ec;
+            if (i + 1 < N) { const double g = eps.g64(c, c + 1); diag += g; off += g * yv(c + 1); } else diag += ec;
+            if (i > 0) { const double g = eps.g64(c, c - 1); diag += g; off += g * yv(c - 1); } else diag += ec;
+            if (j + 1 < N) { const double g = eps.g64(c, c + N); diag += g; off += g * yv(c + N); } else diag += ec;
+            if (j > 0) { const double g = eps.g64(c, c - N); diag += g; off += g * yv(c - N); } else diag += ec;
+            if (k + 1 < N) { const double g = eps.g64(c, c + NN); diag += g; off += g * yv(c + NN); } else diag += ec;
+            if (k > 0) { const double g = eps.g64(c, c - NN); diag += g; off += g * yv(c - NN); } else diag += ec;
             double e_c = 0.0;
-            for (int v = 0; v < nrhs; ++v)
-                if (sm.rhs_idx[v] == c) e_c = sm.rhs_val[v];
+            if ((rmask >> kk) & 1u)
+                for (int v = 0; v < nrhs; ++v)
+                    if (sm.rhs_idx[v] == c) e_c = sm.rhs_val[v];
             const double r64 = e_c - (diag * yc - off);
             rn2 += r64 * r64;
-            r[kk] = (float)((double)ss[c] * r64);
+            const float sc = first ? sm.p[c] : ss[c];
+            r[kk] = (float)((double)sc * r64);
         }
         rn2 = block_sum_d<NW>(rn2, sm.red, 0);
         return sqrt(rn2) / enorm;
@@ -438,31 +482,44 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
     int sweeps = 0;
     double relres = 1.0;
     if (warm) {
-        // sweep 0 from the warm start (y written above; neighbours visible
-        // after the barrier that follows the coefficient set-up)
-        __syncthreads();
-        relres = residual();
+        // sweep 0 from the warm start (y and S written above, visible after
+        // the barrier that follows set-up 1)
+        relres = residual(true);
         sweeps = 1;
     } else {
         // y = 0, so e - K y = e (non-zero only at the centre source)
 #pragma unroll
-        for (int kk = 0; kk < KH; ++kk) r[kk] = 0.f;
-        if (active) {
-            for (int v = 0; v < nrhs; ++v) {
-                const int cell = sm.rhs_idx[v];
-                if (cell % NN == col) {
-#pragma unroll
-                    for (int kk = 0; kk < KH; ++kk)
-                        if (own(kk) && cell / NN == k0 + kk)
-                            r[kk] = (float)((double)ss[cell] * sm.rhs_val[v]);
-                }
+        for (int kk = 0; kk < KH; ++kk) {
+            r[kk] = 0.f;
+            if (own(kk) && ((rmask >> kk) & 1u)) {
+                const int c = col + (k0 + kk) * NN;
+                for (int v = 0; v < nrhs; ++v)
+                    if (sm.rhs_idx[v] == c) r[kk] = (float)((double)sm.p[c] * sm.rhs_val[v]);
             }
         }
+    }
+    if (relres > prm.tol) {
+        // ---- setup 2 (only when the warm start is not already the solution):
+        //      scaled link coefficients cx/cy/cz = g * S_p * S_q, S from p.
+#pragma unroll
+        for (int kk = 0; kk < KH; ++kk) {
+            if (!own(kk)) continue;
+            const int k = k0 + kk;
+            const int c = col + k * NN;
+            const float sc = sm.p[c];
+            float vx = 0.f, vy = 0.f, vz = 0.f;
+            if (i + 1 < N) vx = eps.g32(c, c + 1) * sc * sm.p[c + 1];
+            if (j + 1 < N) vy = eps.g32(c, c + N) * sc * sm.p[c + N];
+            if (k + 1 < N) vz = eps.g32(c, c + NN) * sc * sm.p[c + NN];
+            sm.cx[c] = vx; sm.cy[c] = vy; sm.cz[c] = vz;
+        }
+        __syncthreads();  // every S read before the CG overwrites p
     }
     int total_inner = 0, outer = 0;
     int status = relres <= prm.tol ? 0 : 1;
 #pragma unroll 1
-    for (outer = 0; status != 0 && outer < prm.max_outer; ++outer) {
+    for (outer = 0; status != 0 && outer < prm.max_outer + prm.extra_outer; ++outer) {
+        const int max_inner = outer < prm.max_outer ? prm.max_inner : 4 * prm.max_inner;
         // ---- FP32 CG on K~ d = b, d in x[], starting from 0. The reduction
         //      it needs is set so this sweep brings ||e - K y|| to about half
         //      the target (no deeper than inner_tol per sweep).
@@ -486,7 +543,7 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
         float sv[KH], gamma_old = 1.f, alpha_old = 1.f, stop2 = 0.f;
         int it = 0;
 #pragma unroll 1
-        for (it = 0; it <= prm.max_inner; ++it) {
+        for (it = 0; it <= max_inner; ++it) {
             __syncthreads();  // r published
             float gam = 0.f, del = 0.f;
             if (active) {
@@ -520,7 +577,7 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
                 const float want = fmaxf(prm.inner_tol, (float)(0.5 * prm.tol / relres));
                 stop2 = gd.x * want * want;
             }
-            if (gd.x <= stop2 || it == prm.max_inner) break;
+            if (gd.x <= stop2 || it == max_inner) break;
             const float beta = it == 0 ? 0.f : gd.x / gamma_old;
             const float alpha = gd.x / (gd.y - beta * gd.x / alpha_old);
             gamma_old = gd.x;
@@ -542,7 +599,7 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
         const float stop2 = rr * want * want;
         int it = 0;
 #pragma unroll 1
-        for (it = 0; it < prm.max_inner && rr > stop2; ++it) {
+        for (it = 0; it < max_inner && rr > stop2; ++it) {
             // q = K~ p  (K~_pp = 1)
             float pq = 0.f;
             if (active) {
@@ -613,15 +670,16 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
         for (int kk = 0; kk < KH; ++kk) {
             if (own(kk)) {
                 const int c = col + (k0 + kk) * NN;
-                ys[c] += (double)ss[c] * (double)x[kk];
+                Y[c] += (double)ss[c] * (double)x[kk];
             }
         }
         __syncthreads();  // y of the neighbours visible
-        relres = residual();
+        relres = residual(false);
         ++sweeps;
         if (relres <= prm.tol) status = 0;
     }
     st->status = status;
+    st->escalated = outer > prm.max_outer;
     st->iters = total_inner;
     st->sweeps = sweeps;
     st->relres = relres;

@@ -9,11 +9,16 @@
 // file as a statically sized __device__ array: the library allocates nothing
 // per call (no cudaMalloc / cudaFree, no pinned or pooled memory).
 //
-// The scratch array (kNoAllocScratchBytes) is part of the loaded module, so
-// every GPU that loads the library holds it until the process exits. All
-// calls share it: it keeps the last call's contents (the solver overwrites
-// every value it reads before reading it, so nothing needs clearing), and
-// calls that overlap on the GPU — on different streams, or from several host
+// The scratch array (kNoAllocScratchBytes) and the warm-start tables beside
+// it (kNoAllocWarmDoubles) are part of the loaded module, so every GPU that
+// loads the library holds them until the process exits. The module is loaded
+// and both arrays are set up when a context is created on the device
+// (drwc_ctx_create calls noalloc_prepare), not inside a solve: a caller that
+// creates its context before handing the GPU's memory to its own pool never
+// has this entry point allocate or load anything later. All calls share the
+// scratch: it keeps the last call's contents (the solver overwrites every
+// value it reads before reading it, so nothing needs clearing), and calls
+// that overlap on the GPU — on different streams, or from several host
 // threads on one device — race on it. Issue them on one stream.
 #include <mutex>
 #include <type_traits>
@@ -30,6 +35,32 @@ FdmParams make_params(const drwc_fdm_opts* o, int N);
 // resident) and N = 23 fits 114.
 constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Warm starts (the uniform-permittivity solution per N and solver code, as
+// the regular entry points use): 4 * N^3 doubles for every N in
+// [DRWC_N_MIN, DRWC_N_MAX], 2.4 MB in all, solved once per device at set-up.
+constexpr size_t warm_offset(int N) {  // doubles before resolution N's tables
+    size_t o = 0;
+    for (int n = DRWC_N_MIN; n < N; ++n) o += 4 * (size_t)n * n * n;
+    return o;
+}
+constexpr size_t kNoAllocWarmDoubles = warm_offset(DRWC_N_MAX + 1);
+static __device__ __align__(256) double g_noalloc_warm[kNoAllocWarmDoubles];
+
+// One CTA per solver code: the uniform-permittivity solve (the same solve,
+// with the same parameters, as the per-context warm tables of warm.cu).
+template <int N>
+__global__ void __launch_bounds__(Cube<N>::NT)
+noalloc_uniform_kernel(double* __restrict__ warm, float* __restrict__ scratch_s, FdmParams prm) {
+    const int code = blockIdx.x;
+    double* out = warm + (size_t)code * Cube<N>::NNN;
+    FdmStats st;
+    cube_solve<N>(EpsUniform{}, out, scratch_s + (size_t)code * Cube<N>::NNN, code, prm, &st);
+    if constexpr (Cube<N>::YSMEM) {
+        const double* y = cube_y<N>(out);
+        for (int c = threadIdx.x; c < Cube<N>::NNN; c += blockDim.x) out[c] = y[c];
+    }
+}
 
 // Cube c reads eps + c*N^3 and writes out + c*6N^2 (packed, same N).
 template <int N>
@@ -49,12 +80,17 @@ fdm_noalloc_kernel(int ncubes, const double* __restrict__ eps, const int32_t* __
         const double* e = eps + (size_t)c * D::NNN;
         const int cd = code ? code[c] : DRWC_GFT;
         FdmStats st;
-        cube_solve<N>(EpsGlobal{e}, ys, ss, cd, prm, &st);
+        if (cd < DRWC_GFT || cd > DRWC_WVTY) {  // not a solver code: status 2, zero rows
+            st.status = 2; st.iters = 0; st.sweeps = 0; st.relres = CUDART_NAN;
+            st.escalated = 0;
+        } else {
+            cube_solve<N>(EpsGlobal{e}, ys, ss, cd, prm, &st);
+        }
         double* o = out + (size_t)c * 6 * D::NN;
         if (st.status == 2) {
             for (int b = threadIdx.x; b < 6 * D::NN; b += blockDim.x) o[b] = 0.0;
         } else {
-            for_each_panel<N>(EpsGlobal{e}, ys, [&](int b, double v) { o[b] = v; });
+            for_each_panel<N>(EpsGlobal{e}, cube_y<N>(ys), [&](int b, double v) { o[b] = v; });
         }
         if (threadIdx.x == 0) {
             if (iters) iters[c] = st.iters;
@@ -64,27 +100,39 @@ fdm_noalloc_kernel(int ncubes, const double* __restrict__ eps, const int32_t* __
     }
 }
 
-// Per-device set-up, done once by the first call on that device: the device
-// address of the scratch array and, per N, the kernel's shared-memory limit
-// and its resident CTAs per SM.
+// Per-device set-up, done once per device when the first context on it is
+// created: the device addresses of the scratch and warm-table arrays and, per
+// N, the kernel's shared-memory limit, its resident CTAs per SM and the warm
+// tables.
 struct NoAllocDevice {
     bool ready = false;
     unsigned char* scratch = nullptr;
+    double* warm = nullptr;
     int per_sm[DRWC_N_MAX + 1] = {0};
 };
 constexpr int kMaxDevices = 64;
 static NoAllocDevice g_noalloc_dev[kMaxDevices];
 static std::mutex g_noalloc_mu;
 
-static int noalloc_setup(int device, NoAllocDevice** out) {
+// Set-up for ctx's device, once per device (ctx's device is current).
+static int noalloc_setup(drwc_ctx* ctx, NoAllocDevice** out) {
+    const int device = ctx->device;
     if (device < 0 || device >= kMaxDevices) return DRWC_ERR_INVALID;
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
     NoAllocDevice& d = g_noalloc_dev[device];
     if (!d.ready) {
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || p == nullptr) {
             std::fprintf(stderr, "drwc: cudaGetSymbolAddress(no-alloc scratch) failed: %s\n",
+                         cudaGetErrorString(e));
+            cudaGetLastError();
+            return DRWC_ERR_CUDA;
+        }
+        void* pw = nullptr;
+        e = cudaGetSymbolAddress(&pw, g_noalloc_warm);
+        if (e != cudaSuccess || pw == nullptr) {
+            std::fprintf(stderr, "drwc: cudaGetSymbolAddress(no-alloc warm tables) failed: %s\n",
                          cudaGetErrorString(e));
             cudaGetLastError();
             return DRWC_ERR_CUDA;
@@ -100,16 +148,38 @@ static int noalloc_setup(int device, NoAllocDevice** out) {
                 DRWC_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
                     &nb, fdm_noalloc_kernel<NC>, Dm::NT, Dm::kSmemBytes));
                 d.per_sm[NC] = nb < 1 ? 1 : nb;
-                return DRWC_OK;
+                // warm-start tables of this N (scratch: the Jacobi scales)
+                DRWC_CUDA_TRY(cudaFuncSetAttribute(noalloc_uniform_kernel<NC>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)Dm::kSmemBytes));
+                FdmParams prm{};
+                prm.tol = 1e-13;
+                prm.inner_tol = 1e-6f;
+                prm.max_outer = 12;
+                prm.max_inner = 8 * NC * NC;
+                noalloc_uniform_kernel<NC><<<4, Dm::NT, Dm::kSmemBytes, ctx->stream>>>(
+                    static_cast<double*>(pw) + warm_offset(NC), static_cast<float*>(p), prm);
+                int rc2 = launch_check(ctx);
+                if (rc2) return rc2;
+                // one launch with no cubes, so that the driver sizes the
+                // kernel's local memory now and not in a later solve
+                fdm_noalloc_kernel<NC><<<1, Dm::NT, Dm::kSmemBytes, ctx->stream>>>(
+                    0, nullptr, nullptr, nullptr, nullptr, nullptr, prm,
+                    static_cast<unsigned char*>(p));
+                return launch_check(ctx);
             });
             if (rc) return rc;
         }
+        DRWC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         d.scratch = static_cast<unsigned char*>(p);
+        d.warm = static_cast<double*>(pw);
         d.ready = true;
     }
-    *out = &d;
+    if (out) *out = &d;
     return DRWC_OK;
 }
+
+int noalloc_prepare(drwc_ctx* ctx) { return noalloc_setup(ctx, nullptr); }
 
 }  // namespace drwc
 
@@ -138,7 +208,7 @@ DRWC_API int drwc_fdm_solve_noalloc(drwc_ctx* ctx, int N, int ncubes, const doub
     std::lock_guard<std::mutex> lock(ctx->mu);
     DRWC_CUDA_TRY(cudaSetDevice(ctx->device));
     NoAllocDevice* d = nullptr;
-    int rc = noalloc_setup(ctx->device, &d);
+    int rc = noalloc_setup(ctx, &d);  // done already when the context was created
     if (rc) return rc;
     const size_t fit = kNoAllocScratchBytes / slot;
     size_t grid = (size_t)d->per_sm[N] * ctx->sm_count;
@@ -147,8 +217,11 @@ DRWC_API int drwc_fdm_solve_noalloc(drwc_ctx* ctx, int N, int ncubes, const doub
     return dispatch_N(N, [&](auto nc) -> int {
         constexpr int NC = decltype(nc)::value;
         using Dm = Cube<NC>;
+        FdmParams prm = make_params(opts, NC);
+        if (!opts || opts->warm_start)
+            for (int c = 0; c < 4; ++c) prm.warm[c] = d->warm + warm_offset(NC) + c * Dm::NNN;
         fdm_noalloc_kernel<NC><<<(int)grid, Dm::NT, Dm::kSmemBytes, ctx->stream>>>(
-            ncubes, eps, code, out, iters, status, make_params(opts, NC), d->scratch);
+            ncubes, eps, code, out, iters, status, prm, d->scratch);
         return launch_check(ctx);
     });
 }

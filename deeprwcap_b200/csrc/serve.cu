@@ -91,7 +91,7 @@ struct SvSlots {
 enum SvStat {
     SV_HOPS = 0, SV_NET_HOPS, SV_FDM_HOPS, SV_FALLBACKS, SV_AUDITS, SV_WALKS_DONE,
     SV_WALKS_DROPPED, SV_NET_ROWS, SV_FDM_ITERS, SV_FDM_SWEEPS, SV_FDM_BYTES, SV_TABLE_HOPS,
-    SV_NSTATS
+    SV_FDM_ESCALATED, SV_FDM_FAILED, SV_NSTATS
 };
 
 struct SvArgs {
@@ -584,7 +584,7 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
     VoxScratch<N>& vs =   // separable voxeliser (structures with blocks)
         *reinterpret_cast<VoxScratch<N>*>(smem + (WalkSmem<N>::base(maxP) + 15) / 16 * 16);
     int loaded = -1, P = 0;
-    unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0;
+    unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0, my_esc = 0, my_fail = 0;
     for (;;) {
         // rows are claimed one at a time: solve costs differ by cube
         if (threadIdx.x == 0) s_idx = atomicAdd(next_item, 1u);
@@ -629,7 +629,7 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
         FdmStats st;
         cube_solve<N>(E, ys, ss, code, J.W.prm, &st);
         double* wv = reinterpret_cast<double*>(sm.stage());
-        for_each_panel<N>(E, ys, [&](int b, double v) { wv[b] = v; });
+        for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
         __syncthreads();
         if ((kind & 1) && !first) {
             // audit: KL(FDM || network) over the panels
@@ -654,8 +654,10 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
         double tot = 0.0;
         const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
         if (threadIdx.x == 0) {
-            if (b < 0 || st.status == 2) {
-                sv_finish(A, slot, -1);  // no transition possible: the walk is lost
+            if (b < 0 || st.status != 0) {
+                // no transition possible, or the solve stayed unconverged
+                // after escalation: the walk is lost
+                sv_finish(A, slot, -1);
             } else {
                 if (first)
                     A.st.omega[slot] =
@@ -670,8 +672,14 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
             my_hops += 1;
             my_iters += (unsigned long long)st.iters;
             my_sweeps += (unsigned long long)st.sweeps;
+            my_esc += (unsigned long long)st.escalated;
+            my_fail += st.status == 1;
         }
         __syncthreads();
+    }
+    if (threadIdx.x == 0 && (my_esc || my_fail)) {
+        atomicAdd(A.stats + SV_FDM_ESCALATED, my_esc);
+        atomicAdd(A.stats + SV_FDM_FAILED, my_fail);
     }
     if (threadIdx.x == 0 && my_hops) {
         atomicAdd(A.stats + SV_FDM_HOPS, my_hops);
@@ -1328,6 +1336,8 @@ static void sv_thread(drwc_server* v) {
         v->st.fdm_sweeps = (int64_t)h[SV_FDM_SWEEPS];
         v->st.fdm_bytes = (double)h[SV_FDM_BYTES];
         v->st.table_hops = (int64_t)h[SV_TABLE_HOPS];
+        v->st.fdm_escalated = (int64_t)h[SV_FDM_ESCALATED];
+        v->st.fdm_failed = (int64_t)h[SV_FDM_FAILED];
         v->st.audit_kl_mean = v->h_akl[1] > 0 ? v->h_akl[0] / v->h_akl[1] : 0.0;
     }
     // stopped (destroy or an error): every job not done ends as failed

@@ -81,7 +81,7 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
     float* ss = scratch_s + (size_t)blockIdx.x * D::NNN;
     __syncthreads();
     const int t = threadIdx.x;
-    unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0;
+    unsigned long long my_hops = 0, my_iters = 0, my_sweeps = 0, my_esc = 0, my_fail = 0;
     for (;;) {
         if (t == 0) S.walk = (long long)atomicAdd(next, 1ull);
         __syncthreads();
@@ -140,7 +140,7 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
             FdmStats st;
             cube_solve<N>(E, ys, ss, code, W.prm, &st);
             double* wv = reinterpret_cast<double*>(sm.stage());
-            for_each_panel<N>(E, ys, [&](int b, double v) { wv[b] = v; });
+            for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
             __syncthreads();
             const double2 u = first ? philox_uniform2(W.seed, w, 0, 1)
                                     : philox_uniform2(W.seed, w, (uint32_t)S.hops, 0);
@@ -151,8 +151,12 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
                 my_hops += 1;
                 my_iters += (unsigned long long)st.iters;
                 my_sweeps += (unsigned long long)st.sweeps;
-                if (b < 0 || st.status == 2) {
-                    S.net = -1;  // no transition possible: count as lost
+                my_esc += (unsigned long long)st.escalated;
+                my_fail += st.status == 1;
+                if (b < 0 || st.status != 0) {
+                    // no transition possible, or the cube's solve did not
+                    // converge even after escalation: the walk is lost
+                    S.net = -1;
                     S.done = 2;
                 } else {
                     if (first)
@@ -178,6 +182,8 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
         atomicAdd(stats + 0, my_hops);
         atomicAdd(stats + 1, my_iters);
         atomicAdd(stats + 2, my_sweeps);
+        atomicAdd(stats + 3, my_esc);
+        atomicAdd(stats + 4, my_fail);
     }
 }
 
@@ -228,7 +234,7 @@ struct WalkBuffers {
     int32_t* end;
     int32_t* hops;
     double* w;
-    unsigned long long* counter;  // [0] claim counter, [1] hop sum, [2..4] solver stats
+    unsigned long long* counter;  // [0] claim counter, [1] hop sum, [2..6] solver stats
     double* sums;                 // 3 * (n_entries + 1)
 };
 
@@ -368,8 +374,9 @@ DRWC_API int drwc_job_walks_device(drwc_job* j, int64_t walk0, int64_t nwalks, i
     rc = launch_walks(ctx, j->hg, j->G, j->P, walk0, nwalks, wb);
     if (rc) return rc;
     if (solver_stats) {
-        // stats are (hops, FP32 iterations, FP64 sweeps) as unsigned 64-bit
-        DRWC_CUDA_TRY(cudaMemcpyAsync(solver_stats, wb.counter + 2, 3 * sizeof(int64_t),
+        // stats are (hops, FP32 iterations, FP64 sweeps, escalated solves,
+        // failed solves) as unsigned 64-bit
+        DRWC_CUDA_TRY(cudaMemcpyAsync(solver_stats, wb.counter + 2, 5 * sizeof(int64_t),
                                       cudaMemcpyDeviceToDevice, ctx->stream));
     }
     return DRWC_OK;
@@ -402,7 +409,7 @@ DRWC_API int drwc_frw_walks(drwc_ctx* ctx, const drwc_structure* s, const drwc_j
     int64_t* d_st = (int64_t*)(((uintptr_t)(d_hops + nwalks) + 7) & ~(uintptr_t)7);
     rc = drwc_job_walks_device(j, walk0, nwalks, d_end, d_hops, d_w, d_st);
     if (rc) { drwc_job_destroy(j); return rc; }
-    int64_t st[3] = {0, 0, 0};
+    int64_t st[5] = {0, 0, 0, 0, 0};
     {
         std::lock_guard<std::mutex> lock(ctx->mu);
         DRWC_CUDA_TRY(cudaMemcpyAsync(end_net, d_end, nwalks * 4, cudaMemcpyDeviceToHost, ctx->stream));
@@ -416,6 +423,8 @@ DRWC_API int drwc_frw_walks(drwc_ctx* ctx, const drwc_structure* s, const drwc_j
         solver_stats[1] = st[1];
         solver_stats[2] = st[2];
         solver_stats[3] = st[0] * p->N * p->N * p->N;
+        solver_stats[4] = st[3];
+        solver_stats[5] = st[4];
     }
     return drwc_job_destroy(j);
 }
@@ -446,7 +455,7 @@ DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job
         else c += (v - t) + s;
         s = t;
     };
-    long long walks = 0, lost = 0;
+    long long walks = 0, lost = 0, escalated = 0, failed = 0;
     unsigned long long hops_total = 0;
     std::vector<double> sums(3 * (ne + 1));
     int converged = 0;
@@ -462,10 +471,10 @@ DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job
                          ctx->stream>>>(nw, wb.hops, wb.counter + 1);
         rc = launch_check(ctx);
         if (rc) return rc;
-        unsigned long long hsum = 0;
+        unsigned long long hsum[7] = {0};  // [1] hop sum, [5] escalated, [6] failed solves
         DRWC_CUDA_TRY(cudaMemcpyAsync(sums.data(), wb.sums, sums.size() * 8,
                                       cudaMemcpyDeviceToHost, ctx->stream));
-        DRWC_CUDA_TRY(cudaMemcpyAsync(&hsum, wb.counter + 1, 8, cudaMemcpyDeviceToHost,
+        DRWC_CUDA_TRY(cudaMemcpyAsync(hsum, wb.counter, sizeof hsum, cudaMemcpyDeviceToHost,
                                       ctx->stream));
         DRWC_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
         for (int e = 0; e <= ne; ++e) {
@@ -473,7 +482,9 @@ DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job
             kadd(S2[e], S2c[e], sums[3 * e + 1]);
         }
         lost += (long long)sums[3 * ne + 2];
-        hops_total += hsum;
+        hops_total += hsum[1];
+        escalated += (long long)hsum[5];
+        failed += (long long)hsum[6];
         walks += nw;
         if (walks < p->min_walks) continue;
         // convergence: relative 1-sigma of the self term <= p_tol, and of every
@@ -511,6 +522,8 @@ DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job
     out->walks = walks;
     out->hops = (int64_t)hops_total;
     out->lost = lost;
+    out->solves_escalated = escalated;
+    out->solves_failed = failed;
     for (int e = 0; e < ne; ++e) {
         const double m = (S[e] + Sc[e]) / n;
         out->cap[e] = m;
@@ -1001,7 +1014,7 @@ lw_fdm_kernel(LwArgs A, double* __restrict__ scratch_y, float* __restrict__ scra
         FdmStats st;
         cube_solve<N>(E, ys, ss, code, A.W.prm, &st);
         double* wv = reinterpret_cast<double*>(sm.stage());
-        for_each_panel<N>(E, ys, [&](int b, double v) { wv[b] = v; });
+        for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
         __syncthreads();
         if (audit && !first) {
             // KL(FDM || network) over the panels
@@ -1026,7 +1039,7 @@ lw_fdm_kernel(LwArgs A, double* __restrict__ scratch_y, float* __restrict__ scra
         const double ud = first ? u2.y : u2.x;
         double tot = 0.0;
         const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
-        if (threadIdx.x == 0 && b >= 0 && st.status != 2) {
+        if (threadIdx.x == 0 && b >= 0 && st.status == 0) {
             if (first)
                 A.st.omega[slot] = first_hop_weight(A.G, A.st.sgn[slot], center_diel<N>(E, code),
                                                     tot, wv[b], a);
@@ -1038,7 +1051,8 @@ lw_fdm_kernel(LwArgs A, double* __restrict__ scratch_y, float* __restrict__ scra
             A.st.hops[slot] = h + 1;
             atomicAdd(A.ctr + 3, 1ull);
         }
-        if (threadIdx.x == 0 && (b < 0 || st.status == 2)) lw_finish(A, slot, -1);  // lost
+        // lost: no transition, or the solve stayed unconverged after escalation
+        if (threadIdx.x == 0 && (b < 0 || st.status != 0)) lw_finish(A, slot, -1);
         __syncthreads();
     }
 }

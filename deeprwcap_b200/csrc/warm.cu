@@ -20,6 +20,10 @@ uniform_kernel(double* __restrict__ out0, double* __restrict__ out1, double* __r
     FdmStats st;
     cube_solve<N>(EpsUniform{}, outs[code], scratch_s + (size_t)code * Cube<N>::NNN, code, prm,
                   &st);
+    if constexpr (Cube<N>::YSMEM) {  // the solution is in shared memory
+        const double* y = cube_y<N>(outs[code]);
+        for (int c = threadIdx.x; c < Cube<N>::NNN; c += blockDim.x) outs[code][c] = y[c];
+    }
 }
 
 int warm_tables(drwc_ctx* ctx, int N, const double* warm[4]) {

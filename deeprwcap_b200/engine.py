@@ -309,6 +309,8 @@ class JobResult:
         self.walks = r.walks
         self.hops = r.hops
         self.lost = r.lost
+        self.solves_escalated = r.solves_escalated
+        self.solves_failed = r.solves_failed
         self.seconds = r.seconds
         self.cap = np.array(r.cap[:n])
         self.stderr = np.array(r.stderr_[:n])
@@ -335,13 +337,14 @@ def frw_walks(structure, params, walk0: int, nwalks: int, ctx: Context | None = 
               stats: bool = False):
     """Per-walk records (end net, hops, weight in fF) for walks
     [walk0, walk0+nwalks); with stats=True also the solver counters
-    (hops, FP32 iterations, FP64 sweeps, cells solved)."""
+    (hops, FP32 iterations, FP64 sweeps, cells solved, escalated solves,
+    failed solves)."""
     ctx = ctx or default_context()
     s = structure.to_c() if hasattr(structure, "to_c") else structure
     end = np.zeros(nwalks, dtype=np.int32)
     hops = np.zeros(nwalks, dtype=np.int32)
     w = np.zeros(nwalks)
-    st = np.zeros(4, dtype=np.int64)
+    st = np.zeros(6, dtype=np.int64)
     check(ctx.lib.drwc_frw_walks(ctx.h, C.byref(s), C.byref(params), int(walk0), int(nwalks),
                                  end.ctypes.data, hops.ctypes.data, w.ctypes.data,
                                  st.ctypes.data),

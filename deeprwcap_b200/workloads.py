@@ -302,6 +302,7 @@ def job_params_plain(N: int = 16, master: int = 0, seed: int = 1, **kw) -> JobPa
     p.fdm.max_outer = kw.get("max_outer", 8)
     p.fdm.max_inner = kw.get("max_inner", 0)
     p.fdm.warm_start = kw.get("warm_start", 1)
+    p.fdm.extra_outer = kw.get("extra_outer", 8)
     return p
 
 

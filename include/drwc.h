@@ -95,7 +95,13 @@ typedef struct drwc_fdm_opts {
     int32_t max_inner;  /* FP32 PCG iterations per sweep, default 4 * N * N */
     int32_t warm_start; /* start from the uniform-permittivity solution, as ggft's
                            solveWithGuess (ggft_solver.cpp:554-560); default 1 */
-    int32_t reserved_;
+    int32_t extra_outer; /* escalation: a cube still above tol after max_outer
+                           sweeps gets up to this many more, each with 4 *
+                           max_inner iterations, before it is reported not
+                           converged (ggft falls back to a direct solve,
+                           ggft_solver.cpp:565-589); default 8, 0 = none.
+                           Walks drop a hop whose cube stays unconverged:
+                           the walk ends lost and is counted. */
 } drwc_fdm_opts;
 DRWC_API void drwc_fdm_opts_default(drwc_fdm_opts* opts);
 
@@ -138,14 +144,19 @@ DRWC_API int drwc_fdm_solve_batch(drwc_ctx* ctx, int ncubes, const int32_t* N,
  * its implicit synchronisation are not allowed). Cube c reads N^3 doubles at
  * eps + c*N^3 and writes 6*N^2 doubles at out + c*6*N^2; code (nullable: all
  * GFT), iters and status (nullable) are DEVICE arrays of ncubes entries, as
- * in drwc_fdm_solve_batch_device. Runs async on the context stream. Solver
- * scratch comes from a fixed 16 MiB static device array in the library
- * (12 bytes per cell per resident CTA; every GPU that loads the library holds
- * it until exit); N outside [DRWC_N_MIN, DRWC_N_MAX] is rejected with
- * DRWC_ERR_INVALID. The first call on a device sets up (looks up the array's
- * device address, sets kernel attributes) and should come before any stream
- * capture. Calls share the array: calls that overlap on the GPU race, so
- * issue them on one stream. */
+ * in drwc_fdm_solve_batch_device; a cube whose code is not a solver code
+ * gets status 2 and zero rows. opts->warm_start is honoured as in the other
+ * entry points. Runs async on the context stream. Solver scratch comes from a
+ * fixed 16 MiB static device array in the library (12 bytes per cell per
+ * resident CTA) and the warm starts from a 2.4 MB static array of
+ * uniform-permittivity solutions (every N and code); every GPU that loads the
+ * library holds both until exit. drwc_ctx_create loads their module, looks up
+ * their device addresses, sets the kernel attributes and solves the warm
+ * tables, once per device, so this call itself allocates and loads nothing:
+ * create the context before giving the GPU's memory to your own pool. N
+ * outside [DRWC_N_MIN, DRWC_N_MAX] is rejected with DRWC_ERR_INVALID. Calls
+ * share the scratch array: calls that overlap on the GPU race, so issue them
+ * on one stream. */
 DRWC_API int drwc_fdm_solve_noalloc(drwc_ctx* ctx, int N, int ncubes, const double* eps,
                                     const int32_t* code, const drwc_fdm_opts* opts, double* out,
                                     int32_t* iters, int32_t* status);
@@ -281,7 +292,9 @@ typedef struct drwc_job_result {
     int32_t converged;        /* 1 when -p/-c/--c-ratio were met */
     int64_t walks;
     int64_t hops;
-    int64_t lost;             /* walks cut at max_hops */
+    int64_t lost;             /* walks cut at max_hops or ended by a failed solve */
+    int64_t solves_escalated; /* cube solves that needed escalation sweeps */
+    int64_t solves_failed;    /* cube solves unconverged after escalation (walk lost) */
     double seconds;           /* job wall time on the device */
     double cap[DRWC_MAX_NETS + 1];     /* fF, row of the master */
     double stderr_[DRWC_MAX_NETS + 1]; /* 1-sigma standard error, fF */
@@ -296,8 +309,9 @@ DRWC_API int drwc_job_create(drwc_ctx* ctx, const drwc_structure* s, const drwc_
 DRWC_API int drwc_job_destroy(drwc_job* job);
 /* Launch walks [walk0, walk0 + nwalks) on the context stream (async). Per-walk
  * records go to DEVICE arrays end_net / hops / weight (fF); solver_stats
- * (DEVICE, nullable, 3 int64) receives total hops, FP32 CG iterations and FP64
- * residual sweeps of the launch. */
+ * (DEVICE, nullable, 5 int64) receives total hops, FP32 CG iterations, FP64
+ * residual sweeps, solves that needed escalation sweeps and solves that did
+ * not converge even then (their walks end lost) of the launch. */
 DRWC_API int drwc_job_walks_device(drwc_job* job, int64_t walk0, int64_t nwalks,
                                    int32_t* end_net, int32_t* hops, double* weight,
                                    int64_t* solver_stats);
@@ -424,6 +438,8 @@ typedef struct drwc_server_stats {
     int64_t fdm_iters, fdm_sweeps;    /* FP32 CG iterations and FP64 sweeps of the FDM hops */
     double fdm_bytes;                 /* streamed-PCG algorithmic bytes of the FDM hops */
     int64_t table_hops;               /* hops drawn from the uniform-permittivity tables */
+    int64_t fdm_escalated;            /* FDM solves that needed escalation sweeps */
+    int64_t fdm_failed;               /* FDM solves unconverged after escalation (walk lost) */
 } drwc_server_stats;
 /* Returns the request thread's error code, if it stopped on one. */
 DRWC_API int drwc_server_stats_get(drwc_server* srv, drwc_server_stats* out);
@@ -436,8 +452,9 @@ DRWC_API int drwc_frw_run(drwc_ctx* ctx, const drwc_structure* s, const drwc_job
 /* Run walks [walk0, walk0 + nwalks) of a job and return the per-walk records
  * (end net, hop count, weight in fF) to host arrays. Same walk ids give the
  * same records whatever the batch; this is what the parity tests compare.
- * solver_stats (nullable, 4 int64): total hops, FP32 CG iterations, FP64
- * residual sweeps and cube cells solved (sum of N^3 over hops). */
+ * solver_stats (nullable, 6 int64): total hops, FP32 CG iterations, FP64
+ * residual sweeps, cube cells solved (sum of N^3 over hops), escalated
+ * solves and failed solves (walk lost). */
 DRWC_API int drwc_frw_walks(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params* p,
                             int64_t walk0, int64_t nwalks, int32_t* end_net, int32_t* hops,
                             double* weight, int64_t* solver_stats);

@@ -25,11 +25,18 @@ _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 
 
+def reference_dir() -> Path:
+    """Where the reference tree is mounted: $DRWC_REFERENCE_DIR, else a
+    directory named ``reference`` beside this repository's folder."""
+    env = os.environ.get("DRWC_REFERENCE_DIR")
+    return Path(env) if env else HERE.parents[1] / "reference"
+
+
 def build(quiet: bool = True) -> None:
     """Compile liboracle.so (and the reference objects when the reference
     tree is present) with oracle/Makefile."""
     import subprocess
-    subprocess.run(["make", "-C", str(HERE), "-j8"], check=True,
+    subprocess.run(["make", "-C", str(HERE), "-j8", f"REF={reference_dir()}"], check=True,
                    stdout=subprocess.DEVNULL if quiet else None)
 
 

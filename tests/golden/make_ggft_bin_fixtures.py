@@ -15,7 +15,8 @@ reference's own generator and reader.
    ggft_bin_N8_reader.npz: greens_tensor, face_distribution (poisson) and
    normalised_gradient, face_grad_weights (gradient).
 
-Needs the reference tree, so it runs only where that tree is mounted; the
+Needs the reference tree ($DRWC_REFERENCE_DIR, else ``reference`` beside
+this repository's folder), so it runs only where that tree is mounted; the
 committed files are what the tests read.
 """
 from __future__ import annotations
@@ -30,12 +31,15 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parents[1]
-REF = Path("/root/reference")
 N, COUNT = 8, 6
 
 
 def main() -> None:
-    subprocess.run(["make", "-C", str(ROOT / "oracle"), f"_ref/ggft_gen_N{N}"], check=True)
+    sys.path.insert(0, str(ROOT))
+    from oracle.oracle import reference_dir
+    REF = reference_dir()
+    subprocess.run(["make", "-C", str(ROOT / "oracle"), f"REF={REF}", f"_ref/ggft_gen_N{N}"],
+                   check=True)
     gen = ROOT / "oracle" / "_ref" / f"ggft_gen_N{N}"
     out = {}
     sys.path.insert(0, str(REF / "training_pytorch" / "src"))
