@@ -207,11 +207,17 @@ def learned_section(ctx, args):
     for name, kw in (("served_learned", {}), ("served_learned_table", {"uniform_table": 1})):
         pj = W.job_params_plain(N=16, seed=4242, tol=FDM_TOL, min_walks=nw, max_walks=nw,
                                 batch_walks=1 << 16)
+        dev = torch.device("cuda", ctx.device)
+        rec_e = torch.full((nw,), -2, dtype=torch.int32, device=dev)
+        rec_w = torch.zeros(nw, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
         with engine.Server(ctx, net=net, timing=1 if not kw else 0, **kw) as srv:
             t2 = time.perf_counter()
-            r = srv.wait(srv.submit(s, pj), timeout=3600)
+            r = srv.wait(srv.submit(s, pj, records=(rec_e, rec_w)), timeout=3600)
             dt = time.perf_counter() - t2
             sst = srv.stats()
+        torch.cuda.synchronize()
+        acc = paired_accuracy(rec_e.cpu().numpy(), rec_w.cpu().numpy(), e0, w0, s.n_nets + 1)
         if not kw:
             # network stage of the served step (voxeliser + conv1, conv2, conv3, heads,
             # sampler) timed by graph event nodes; one gradient-head row per walk
@@ -225,7 +231,8 @@ def learned_section(ctx, args):
                         "audits": sst["audits"], "audit_kl_mean": sst["audit_kl_mean"],
                         "cap_fF": [float(x) for x in r.cap],
                         "self_rel_diff_vs_fdm": abs(r.cap[0] - c0[0]) / abs(c0[0]),
-                        "self_rel_stderr": float(r.stderr[0] / abs(r.cap[0]))}
+                        "self_rel_stderr": float(r.stderr[0] / abs(r.cap[0])),
+                        "accuracy": acc}
     # the network alone on a fixed batch (tensor-core fraction)
     B = 65536
     dev = torch.device("cuda", ctx.device)
@@ -251,11 +258,13 @@ def learned_section(ctx, args):
             "learned_hops_per_s": hl, "fdm_hops_per_s": hf, "gain": hl / hf,
             **served,
             "gain_served_learned_table": served["served_learned_table"]["hops_per_s"] / hf,
+            "gain_served_learned": served["served_learned"]["hops_per_s"] / hf,
             "net_hops": st["net_hops"], "fdm_hops": st["fdm_hops"],
             "fallbacks": st["fallbacks"], "audits": st["audits"],
             "audit_kl_mean": st["audit_kl"], "learned_launches": int(l_launch),
             "cap_learned_fF": c1, "cap_fdm_fF": c0,
             "self_rel_diff": abs(c1[0] - c0[0]) / abs(c0[0]),
+            "accuracy": paired_accuracy(e1, w1, e0, w0, s.n_nets + 1),
             "nn_forward": {"cubes": B, "seconds": t_nn, "tflops": flop / t_nn / 1e12,
                            "peak_tflops": bf16, "frac": flop / t_nn / 1e12 / bf16,
                            "peak_source": src, "path": "drwc_net_forward (conv1 as a GEMM)"},
@@ -306,22 +315,33 @@ def serving_section(ctx, args, net):
         hops += r.hops
     seq = summary(lat, hops, time.perf_counter() - t0)
 
+    import torch
+    dev = torch.device("cuda", ctx.device)
+
     def served(**opts):
+        # every job's walk records (end net, weight by walk id) for the
+        # walk-by-walk comparison of the forms
+        recs = [(torch.full((j.walks,), -2, dtype=torch.int32, device=dev),
+                 torch.zeros(j.walks, dtype=torch.float64, device=dev)) for j in stream]
+        torch.cuda.synchronize()
         with engine.Server(ctx, **opts) as srv:
             t0 = time.perf_counter()
             ids = []
-            for j in stream:
+            for j, rc in zip(stream, recs):
                 dt = t0 + j.arrival - time.perf_counter()
                 if dt > 0:
                     time.sleep(dt)
-                ids.append(srv.submit(j.structure, W.serve_params(j)))
+                ids.append(srv.submit(j.structure, W.serve_params(j), records=rc))
             res = [srv.wait(i, timeout=3600) for i in ids]
             wall = time.perf_counter() - t0
             lat = [srv.times(i)[1] for i in ids]
             st = srv.stats()
-        return summary(lat, sum(r.hops for r in res), wall, st), res
+        torch.cuda.synchronize()
+        host = [(e.cpu().numpy(), w.cpu().numpy()) for e, w in recs]
+        del recs
+        return summary(lat, sum(r.hops for r in res), wall, st), res, host
 
-    plain, res_p = served()
+    plain, res_p, rec_p = served()
     plain["fdm_roofline_frac_of_measured_hbm"] = plain["fdm_alg_GBps_over_busy"] / hbm
     out = {"jobs": len(stream), "rate_jobs_per_s": 50.0,
            "walks_range": [1e5, args.serve_walks_max],
@@ -346,7 +366,21 @@ def serving_section(ctx, args, net):
             del X, T, TG, Xt, Tt, TGt, Xv, Tv, TGv
             nets.append(nN)
         out["train_21_23"] = train_info
-        learned, res_l = served(net=nets, uniform_table=1)
+        learned, res_l, rec_l = served(net=nets, uniform_table=1)
+        # walk by walk against the FDM-served jobs (the same walk ids; the
+        # FDM-served walks are drwc_frw_run's)
+        per_job = [paired_accuracy(a[0], a[1], b[0], b[1], j.structure.n_nets + 1)
+                   for a, b, j in zip(rec_l, rec_p, stream)]
+        learned["accuracy"] = {
+            "jobs": len(per_job),
+            "jobs_consistent": int(sum(p["all_consistent"] for p in per_job)),
+            "jobs_pass": int(sum(p["all_pass"] for p in per_job)),
+            "self_rel_diff": [p["entries"]["self"]["rel_diff"] for p in per_job],
+            "self_rel_3sem": [p["entries"]["self"]["rel_3sem"] for p in per_job],
+            "max_abs_coupling_rel_diff": max(
+                (abs(v["rel_diff"]) for p in per_job for k, v in p["entries"].items()
+                 if k != "self"), default=0.0),
+            "per_job": per_job}
         # capacitance agreement of the learned+served form with the FDM walk, per job
         self_diff = [abs(a.cap[0] - b.cap[0]) / abs(b.cap[0]) for a, b in zip(res_l, res_p)]
         learned["self_cap_rel_diff_vs_fdm"] = {"max": float(max(self_diff)),
@@ -362,6 +396,73 @@ def serving_section(ctx, args, net):
         out["speedup_hops_per_s_vs_sequential_fdm"] = learned["hops_per_s"] / seq["hops_per_s"]
         out["speedup_p50_vs_sequential_fdm"] = seq["p50_s"] / learned["p50_s"]
     return out
+
+
+def summary_of(line):
+    """The headline figures of every section in a few keys, printed last in the
+    JSON line so that a truncated log keeps them."""
+    g = lambda d, *ks: (None if d is None else (g(d.get(ks[0]), *ks[1:]) if len(ks) > 1
+                                                 else d.get(ks[0])))
+    s = {"frw_hops_per_s": line["value"], "frw_e2e_hops_per_s": g(line, "e2e", "value"),
+         "roofline_frac": g(line, "roofline", "frac"),
+         "roofline_bound": g(line, "roofline", "bound"),
+         "job_s": g(line, "job", "seconds"), "job_converged": g(line, "job", "converged"),
+         "job_walks": g(line, "job", "walks"),
+         "cfg0_gpu_cubes_per_s": g(line, "fdm_config0", "gpu_cubes_per_s"),
+         "cfg0_vs_ggft_cores": g(line, "fdm_config0", "gpu_vs_cpu"),
+         "cfg0_max_rel_err": g(line, "fdm_config0", "max_rel_err_normwise"),
+         "cfg2_cubes_per_s": g(line, "fdm_config2", "cubes_per_s"),
+         "cfg2_max_rel_err": g(line, "fdm_config2", "max_rel_err_vs_fp64_oracle"),
+         "cpu_baseline_hops_per_s": g(line, "cpu_baseline", "value")}
+    lr = line.get("learned")
+    if lr:
+        s["dense_gain_learned_walker"] = lr.get("gain")
+        s["dense_gain_served_net"] = lr.get("gain_served_learned")
+        s["dense_gain_served_net_table"] = lr.get("gain_served_learned_table")
+        s["dense_accuracy_all_consistent"] = {
+            k: g(lr, *path, "accuracy", "all_consistent") for k, path in
+            (("learned_walker", ()), ("served_net", ("served_learned",)),
+             ("served_net_table", ("served_learned_table",)))}
+    sv = line.get("serving")
+    if sv:
+        s["stream_speedup_vs_sequential_fdm"] = sv.get("speedup_hops_per_s_vs_sequential_fdm")
+        s["stream_p50_s"] = {k: g(sv, k, "p50_s") for k in
+                             ("sequential_frw_run", "served_fdm", "served_learned_table")}
+        s["stream_jobs_consistent"] = g(sv, "served_learned_table", "accuracy",
+                                        "jobs_consistent")
+    return s
+
+
+def paired_accuracy(e1, w1, e0, w0, n_entries, master=0, self_tol=0.01, cpl_tol=0.02):
+    """Walk-by-walk comparison of two forms of one job on the same walk ids
+    (records e*, w*): per entry the relative difference of the estimates and
+    3x the standard error of the walk-by-walk difference, for the self term
+    and the couplings that make up 95 % of the coupling magnitude. pass:
+    |difference| + 3 sigma within the tolerance (1 % self, 2 % couplings);
+    consistent: |difference| within the tolerance + 3 sigma."""
+    n = len(w0)
+    cap = lambda e, w, j: float(np.where(e == j, w, 0.0).sum() / n)
+    c0 = np.array([cap(e0, w0, j) for j in range(n_entries)])
+    order = [j for j in np.argsort(-np.abs(c0)) if j != master]
+    tot = np.abs(c0[order]).sum()
+    cpl, acc = [], 0.0
+    for j in order:
+        if acc >= 0.95 * tot:
+            break
+        cpl.append(int(j))
+        acc += abs(c0[j])
+    rows = {}
+    ok = True
+    for j, tol in [(master, self_tol)] + [(j, cpl_tol) for j in cpl]:
+        d = np.where(e1 == j, w1, 0.0) - np.where(e0 == j, w0, 0.0)
+        rel = float(d.mean() / abs(c0[j]))
+        sem3 = float(3 * d.std() / np.sqrt(n) / abs(c0[j]))
+        rows[("self" if j == master else f"c{j}")] = {
+            "rel_diff": rel, "rel_3sem": sem3, "tol": tol,
+            "pass": abs(rel) + sem3 <= tol, "consistent": abs(rel) <= tol + sem3}
+        ok &= abs(rel) <= tol + sem3
+    return {"walks": n, "entries": rows, "all_consistent": bool(ok),
+            "all_pass": bool(all(r["pass"] for r in rows.values()))}
 
 
 def run_b200(args, world, rank, local):
@@ -464,6 +565,13 @@ def run_b200(args, world, rank, local):
                     "cap_fF": [float(x) for x in r.cap],
                     "stderr_fF": [float(x) for x in r.stderr]}
 
+    # ---- the FDM Green's-function workloads on their own: 64 cubes of N = 16
+    #      against the reference ggft, and the 8192-cube mixed batch
+    fdm0 = fdm2 = None
+    if rank == 0 and not args.no_fdm:
+        fdm0 = fdm_config0_section(ctx, args)
+        fdm2 = fdm_batch_section(ctx, args, 3, 2)
+
     # ---- learned transition kernels (network trained here on engine-generated
     #      FDM data) vs the FDM walk on the dense 24-conductor structure
     learned = None
@@ -517,31 +625,108 @@ def run_b200(args, world, rank, local):
             "clocks": clk.summary(),
             "wall_s_timed": t_wall,
             "job": job_info,
+            "fdm_config0": fdm0,
+            "fdm_config2": fdm2,
             "learned": learned,
             "serving": serving,
             "cpu_baseline": cpu,
         }
+        line["summary"] = summary_of(line)
         print(json.dumps(line), flush=True)
     job.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 
 
-def run_fdm_batch(args, world, rank, local):
-    """Secondary workload: 8192 cubes, N drawn from {16, 21, 23}, layered
-    permittivity with 10% of cubes carrying voxel noise (eps log-uniform in
-    [1, 12]), one mixed-precision solve per cube to a 1e-8 FP64 relative
-    residual. A step is one drwc_fdm_solve_batch_device call over all cubes
-    (inputs resident in HBM)."""
+def _fdm_timed(ctx, torch, stream, call, steps, warmup, flush):
+    """Device time per call (CUDA events on the library's stream, L2 flushed
+    before each call), after `warmup` untimed calls."""
+    for _ in range(warmup):
+        call()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        evs[k][0].record(stream)
+        call()
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    return sum(x.elapsed_time(y) for x, y in evs) / 1e3 / steps
+
+
+def fdm_config0_section(ctx, args):
+    """64 transition cubes, N = 16 (1-4 horizontal layers with uniform-random z
+    cuts and eps ~ U[2, 8], 0-2 random boxes with eps ~ U[2, 8]), each solved
+    for the Poisson kernel and the three gradient codes: on the GPU in one
+    batched call (inputs resident in HBM, tol 1e-10) and by the reference
+    ggft (compiled from its sources, tol 1e-12, as ggft/src/main.cpp:38-57
+    loops over cubes) on all host cores. Max relative error per cube and
+    code (normwise and elementwise over the row's largest value)."""
     import ctypes as C
     import torch
-    from deeprwcap_b200 import abi, engine
+    from deeprwcap_b200 import abi
     from deeprwcap_b200 import workloads as W
-    torch.cuda.set_device(local)
-    ctx = engine.Context(local)
-    stream = torch.cuda.ExternalStream(ctx.stream, device=torch.device("cuda", local))
+    from oracle import oracle as O
+    dev = torch.device("cuda", ctx.device)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    n, N = 64, 16
+    eps, _ = W.fdm_cubes(n, N, seed=20260, noise_frac=0.0)
+    m = 4 * n  # (cube, code) pairs
+    Ns = np.full(m, N, dtype=np.int32)
+    eoff = (np.arange(m, dtype=np.int64) // 4) * N ** 3
+    codes = (np.arange(m) % 4).astype(np.int32)
+    ooff = np.arange(m, dtype=np.int64) * 6 * N * N
+    eps_d = torch.from_numpy(eps.reshape(-1).copy()).to(dev)
+    out_d = torch.zeros(m * 6 * N * N, dtype=torch.float64, device=dev)
+    st_d = torch.zeros(m, dtype=torch.int32, device=dev)
+    opts = abi.FdmOpts(1e-10, 1e-5, 8, 0)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
+
+    def call():
+        abi.check(ctx.lib.drwc_fdm_solve_batch_device(
+            ctx.h, m, Ns.ctypes.data, eoff.ctypes.data, eps_d.data_ptr(), codes.ctypes.data,
+            C.byref(opts), ooff.ctypes.data, out_d.data_ptr(), None, None, None,
+            st_d.data_ptr()), "drwc_fdm_solve_batch_device")
+    t_gpu = _fdm_timed(ctx, torch, stream, call, 5, 3, flush)
+    got = out_d.cpu().numpy().reshape(n, 4, -1)
+    out = {"workload": "64 cubes, N = 16, GFT + WVTZ/WVTX/WVTY each", "cubes": n,
+           "gpu_cubes_per_s": n / t_gpu, "gpu_ms": 1e3 * t_gpu,
+           "converged": int((st_d.cpu().numpy() == 0).sum()), "solves": m}
+    if O.ref_available(N):
+        nthreads = os.cpu_count() or 1
+        ref = np.zeros((n, 4, 6 * N * N))
+        t_cpu = 0.0
+        for code in range(4):
+            r, ok, sec = O.ggft_ref(eps, code, tol=1e-12, nthreads=nthreads)
+            ref[:, code] = r
+            t_cpu += sec
+        nrm = np.linalg.norm(got - ref, axis=2) / np.linalg.norm(ref, axis=2)
+        elt = np.abs(got - ref).max(axis=2) / np.abs(ref).max(axis=2)
+        out.update({"cpu_cubes_per_s": n / t_cpu, "cpu_cores": nthreads,
+                    "cpu_kind": "reference ggft, tol 1e-12",
+                    "gpu_vs_cpu": t_cpu / t_gpu,
+                    "max_rel_err_normwise": float(nrm.max()),
+                    "max_rel_err_elementwise": float(elt.max()), "tolerance": 1e-6})
+    return out
+
+
+def fdm_batch_section(ctx, args, steps, warmup, rank=0):
+    """8192 cubes, N drawn from {16, 21, 23}, layered permittivity with 10 % of
+    cubes carrying voxel noise (eps log-uniform in [1, 12]), one mixed-
+    precision solve per cube to a 1e-8 FP64 relative residual. A step is one
+    drwc_fdm_solve_batch_device call over all cubes (inputs resident in HBM,
+    L2 flushed between steps). Per-cube error vs the FP64 oracle on a sample;
+    the reference ggft on a sample of the same cubes, all host cores."""
+    import ctypes as C
+    import torch
+    from deeprwcap_b200 import abi
+    from deeprwcap_b200 import workloads as W
+    dev = torch.device("cuda", ctx.device)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
     b = W.mixed_fdm_batch(args.cubes, seed=2026 + rank)
-    dev = torch.device("cuda", local)
     eps = torch.from_numpy(b.eps).to(dev)
     out = torch.empty(b.out_size, dtype=torch.float64, device=dev)
     n = b.ncubes
@@ -552,64 +737,39 @@ def run_fdm_batch(args, world, rank, local):
     opts = abi.FdmOpts(FDM_TOL, 1e-5, 8, 0)
     Ns = np.ascontiguousarray(b.N, dtype=np.int32)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize()
 
-    def step(rec=None):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        if rec:
-            rec[0].record(stream)
-        rc = ctx.lib.drwc_fdm_solve_batch_device(
+    def call():
+        abi.check(ctx.lib.drwc_fdm_solve_batch_device(
             ctx.h, n, Ns.ctypes.data, b.eps_off.ctypes.data, eps.data_ptr(), None,
             C.byref(opts), b.out_off.ctypes.data, out.data_ptr(), iters.data_ptr(),
-            sweeps.data_ptr(), relres.data_ptr(), status.data_ptr())
-        abi.check(rc, "drwc_fdm_solve_batch_device")
-        if rec:
-            rec[1].record(stream)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
+            sweeps.data_ptr(), relres.data_ptr(), status.data_ptr()), "drwc_fdm_solve_batch_device")
     l0 = ctx.launches
-    with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            step(evs[k])
-        torch.cuda.synchronize()
-    launches = ctx.launches - l0
-    t = sum(a.elapsed_time(c) for a, c in evs) / 1e3 / args.steps
+    t = _fdm_timed(ctx, torch, stream, call, steps, warmup, flush)
+    launches = (ctx.launches - l0) // max(1, steps + warmup)
     it = iters.cpu().numpy().astype(np.int64)
     sw = sweeps.cpu().numpy().astype(np.int64)
     cells = b.N.astype(np.int64) ** 3
     alg = float(np.sum(cells * (48 * it + 40 * sw)) + 8 * cells.sum() +
                 8 * 6 * np.sum(b.N.astype(np.int64) ** 2))
     hbm, _, src = peaks()
-    achieved = alg / t / 1e9
     st = status.cpu().numpy()
-    line = {"metric": "batched uneven FDM surface Green's functions", "value": n / t,
-            "unit": "cubes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t, "higher_is_better": True, "dtype": "f32+f64",
-            "data": "synthetic",
-            "config": {"workload": "mixed_fdm_batch", "cubes": n, "N": [16, 21, 23],
-                       "noise_frac": 0.1, "fdm_tol": FDM_TOL,
-                       "fp32_iters_per_cube": float(it.mean()),
-                       "fp64_sweeps_per_cube": float(sw.mean()),
-                       "converged": int((st == 0).sum()),
-                       "max_relres": float(relres.max().item()),
-                       "l2": "flushed between steps (256 MB write)"},
-            "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": None, "peak_source": src},
-            "clocks": clk.summary()}
+    res = {"workload": "mixed_fdm_batch", "cubes": n, "N": [16, 21, 23], "noise_frac": 0.1,
+           "fdm_tol": FDM_TOL, "cubes_per_s": n / t, "ms_per_step": 1e3 * t,
+           "launches_per_step": int(launches),
+           "fp32_iters_per_cube": float(it.mean()), "fp64_sweeps_per_cube": float(sw.mean()),
+           "converged": int((st == 0).sum()), "max_relres": float(relres.max().item()),
+           "streamed_pcg_GBps": alg / t / 1e9, "streamed_pcg_frac_of_hbm": alg / t / 1e9 / hbm,
+           "hbm_peak_source": src,
+           "note": "streamed_pcg_* = the bytes a streamed (HBM-resident) PCG would move for "
+                   "these iterations; the solver keeps each cube on chip"}
     if not args.no_cpu:
-        # CPU baseline: reference ggft (tol FDM_TOL) on a sample of the same cubes, all cores;
-        # the same sample checks the device output against the FP64 oracle.
         from oracle import oracle as O
         nthreads = os.cpu_count() or 1
-        res = out.cpu().numpy()
+        resv = out.cpu().numpy()
         errs = []
-        cps_num = 0.0
-        cps_den = 0.0
+        cps_num = cps_den = 0.0
+        kind = "port"
         for N in (16, 21, 23):
             idx = np.nonzero(b.N == N)[0][:max(nthreads, 24)]
             cubes = np.stack([b.cube(int(c)) for c in idx])
@@ -618,18 +778,36 @@ def run_fdm_batch(args, world, rank, local):
                 kind = "reference"
             else:
                 _, ok, sec = O.fdm_solve_batch(cubes, 0, tol=FDM_TOL, nthreads=nthreads)
-                kind = "port"
             cps_num += len(idx) * np.mean(b.N == N)
             cps_den += sec * np.mean(b.N == N)
             for c in idx[:8]:
                 ref, *_ = O.fdm_solve(b.cube(int(c)), 0, tol=1e-13)
-                g = res[b.out_off[c]:b.out_off[c] + 6 * N * N]
+                g = resv[b.out_off[c]:b.out_off[c] + 6 * N * N]
                 errs.append(float(np.linalg.norm(g - ref) / np.linalg.norm(ref)))
-        line["cpu_baseline"] = {"value": cps_num / cps_den, "unit": "cubes/s", "cores": nthreads,
-                                "kind": kind,
-                                "sample": "reference ggft (compiled from its sources) on up to "
-                                          "24 cubes per N of the same batch, tol 1e-8"}
-        line["max_rel_err_vs_fp64_oracle"] = max(errs)
+        res["cpu_baseline"] = {"value": cps_num / cps_den, "unit": "cubes/s", "cores": nthreads,
+                               "kind": kind,
+                               "sample": "reference ggft (compiled from its sources) on up to "
+                                         "24 cubes per N of the same batch, tol 1e-8"}
+        res["max_rel_err_vs_fp64_oracle"] = max(errs)
+        res["error_sample_cubes"] = len(errs)
+    return res
+
+
+def run_fdm_batch(args, world, rank, local):
+    """Secondary workload alone: the batched uneven FDM (fdm_batch_section) as
+    its own JSON line."""
+    import torch
+    from deeprwcap_b200 import engine
+    torch.cuda.set_device(local)
+    ctx = engine.Context(local)
+    with ClockSampler(local) as clk:
+        r = fdm_batch_section(ctx, args, args.steps, args.warmup, rank)
+    line = {"metric": "batched uneven FDM surface Green's functions", "value": r["cubes_per_s"],
+            "unit": "cubes/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["ms_per_step"], "higher_is_better": True, "dtype": "f32+f64",
+            "data": "synthetic", "config": {k: v for k, v in r.items() if k != "cpu_baseline"},
+            "gpu_launches": r["launches_per_step"] * args.steps,
+            "clocks": clk.summary(), "cpu_baseline": r.get("cpu_baseline")}
     print(json.dumps(line), flush=True)
 
 
@@ -652,6 +830,7 @@ def main():
     ap.add_argument("--learned-walks", type=int, default=1 << 20)
     ap.add_argument("--cubes", type=int, default=8192)
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-fdm", action="store_true")
     ap.add_argument("--serve-jobs", type=int, default=10)
     ap.add_argument("--serve-walks-max", type=float, default=1e6)
     ap.add_argument("--serve-train-samples", type=int, default=1 << 18)

@@ -48,6 +48,7 @@ EXPORTS = [
     "drwc_frw_walks_learned",
     "drwc_server_opts_default", "drwc_server_create", "drwc_server_destroy", "drwc_server_submit",
     "drwc_server_poll", "drwc_server_wait", "drwc_server_job_times", "drwc_server_stats_get",
+    "drwc_server_submit_records",
 ]
 
 
@@ -205,6 +206,8 @@ def load():
     L.drwc_server_destroy.argtypes = [vp]
     L.drwc_server_submit.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams),
                                      C.POINTER(i64)]
+    L.drwc_server_submit_records.argtypes = [vp, C.POINTER(Structure), C.POINTER(JobParams),
+                                             vp, vp, C.POINTER(i64)]
     L.drwc_server_poll.argtypes = [vp, i64, C.POINTER(i32), C.POINTER(JobResult)]
     L.drwc_server_wait.argtypes = [vp, i64, dbl, C.POINTER(JobResult)]
     L.drwc_server_job_times.argtypes = [vp, i64, C.POINTER(dbl), C.POINTER(dbl)]

@@ -41,12 +41,26 @@ def _headers():
     return list(CSRC.glob("*.cuh")) + list((ROOT / "include").glob("*.h"))
 
 
+def _deps(dep: Path) -> list[Path] | None:
+    """Headers a source included at its last compile (nvcc -MD output)."""
+    if not dep.exists():
+        return None
+    text = dep.read_text().replace("\\\n", " ")
+    names = text.split(":", 1)[1].split() if ":" in text else []
+    return [Path(n) for n in names]
+
+
 def _compile(src: Path, verbose: bool, ptxas_v: bool) -> tuple[Path, str]:
     obj = BUILD / (src.stem + ".o")
-    newest = max([src.stat().st_mtime] + [h.stat().st_mtime for h in _headers()])
+    dep = BUILD / (src.stem + ".d")
+    deps = _deps(dep)
+    if deps is None or not all(d.exists() for d in deps):
+        deps = _headers()
+    newest = max([src.stat().st_mtime] + [h.stat().st_mtime for h in deps])
     if obj.exists() and obj.stat().st_mtime >= newest and not ptxas_v:
         return obj, ""
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *EXTRA, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *EXTRA, "-MD", "-MF", str(dep), "-c", str(src),
+           "-o", str(obj)]
     if ptxas_v:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -112,7 +112,10 @@ query_kernel(int n, const float* __restrict__ layers, const float* __restrict__ 
             code = a == 0 ? DRWC_WVTX : a == 1 ? DRWC_WVTY : DRWC_WVTZ;
         }
         FdmStats st;
-        cube_solve<N>(EpsGlobal{es}, ys, ss, code, prm, &st);
+        if (planar_cube<N>(es))  // no cuboid reaches a cell centre: the per-plane solver
+            cube_solve_planar<N>(EpsGlobalPlanar<N>{es}, ys, code, prm, &st);
+        else
+            cube_solve<N>(EpsGlobal{es}, ys, ss, code, prm, &st);
         double* w = reinterpret_cast<double*>(sm.stage());  // 6N^2 doubles over p|cx|cy|cz
         for_each_panel<N>(EpsGlobal{es}, cube_y<N>(ys), [&](int b, double v) { w[b] = v; });
         __syncthreads();

@@ -38,7 +38,10 @@ fdm_batch_kernel(int nsel, const int32_t* __restrict__ sel, const double* __rest
         const double* e = eps + eps_off[c];
         const int cd = code ? code[c] : DRWC_GFT;
         FdmStats st;
-        cube_solve<N>(EpsGlobal{e}, ys, ss, cd, prm, &st);
+        if (planar_cube<N>(e))  // one permittivity per z plane: the per-plane solver
+            cube_solve_planar<N>(EpsGlobalPlanar<N>{e}, ys, cd, prm, &st);
+        else
+            cube_solve<N>(EpsGlobal{e}, ys, ss, cd, prm, &st);
         double* o = out + out_off[c];
         if (st.status == 2) {
             for (int b = threadIdx.x; b < 6 * D::NN; b += blockDim.x) o[b] = 0.0;

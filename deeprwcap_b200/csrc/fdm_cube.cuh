@@ -223,6 +223,88 @@ struct EpsPalette {
     DRWC_DEV bool valid(int c) const { return true; }  // palette checked on the host
 };
 
+// EpsPlanar: a stratified cube, whose material depends only on the z index
+// (every cell of plane k holds material lm[k]); same palette tables as
+// EpsPalette. cube_solve_planar solves such cubes without per-cell
+// coefficient arrays.
+template <int N>
+struct EpsPlanar {
+    const int* lm;          // N material ids, one per z index (shared memory)
+    const double* pal;
+    const double* palinv;
+    const double* pair64;
+    const float* pair32;
+    int P;
+    DRWC_DEV int m(int c) const { return lm[c / (N * N)]; }
+    DRWC_DEV double e64(int c) const { return pal[m(c)]; }
+    DRWC_DEV double inv64(int c) const { return palinv[m(c)]; }
+    DRWC_DEV float e32(int c) const { return (float)pal[m(c)]; }
+    DRWC_DEV double g64(int c, int q) const { return pair64[m(c) * P + m(q)]; }
+    DRWC_DEV float g32(int c, int q) const { return pair32[m(c) * P + m(q)]; }
+    DRWC_DEV bool valid(int) const { return true; }  // palette checked on the host
+    // Plane k's permittivity, its inverse and the conductances of its x/y
+    // links and of the z links up (k, k+1) and down (k-1, k), FP64 and FP32
+    // (0 for a link that leaves the cube).
+    DRWC_DEV void plane(int k, double& e, double& einv, double& gxy, double& gzu, double& gzd,
+                        float& gxy32, float& gzu32, float& gzd32) const {
+        const int mk = lm[k];
+        e = pal[mk];
+        einv = palinv[mk];
+        gxy = pair64[mk * P + mk];
+        gzu = k + 1 < N ? pair64[mk * P + lm[k + 1]] : 0.0;
+        gzd = k > 0 ? pair64[lm[k - 1] * P + mk] : 0.0;
+        gxy32 = pair32[mk * P + mk];
+        gzu32 = k + 1 < N ? pair32[mk * P + lm[k + 1]] : 0.f;
+        gzd32 = k > 0 ? pair32[lm[k - 1] * P + mk] : 0.f;
+    }
+};
+
+// EpsGlobalPlanar: an FP64 permittivity array in global memory (as EpsGlobal)
+// known to hold one value per z plane (planar_cube checked it); conductances
+// as EpsGlobal computes them.
+template <int N>
+struct EpsGlobalPlanar {
+    const double* __restrict__ eps;
+    DRWC_DEV double e64(int c) const { return eps[c]; }
+    DRWC_DEV double inv64(int c) const { return 1.0 / eps[c]; }
+    DRWC_DEV float e32(int c) const { return (float)eps[c]; }
+    DRWC_DEV void plane(int k, double& e, double& einv, double& gxy, double& gzu, double& gzd,
+                        float& gxy32, float& gzu32, float& gzd32) const {
+        constexpr int NN = N * N;
+        e = eps[k * NN];
+        einv = 1.0 / e;
+        gxy = e * e / (e + e);
+        const float f = (float)e;
+        gxy32 = f * f / (f + f);
+        gzu = 0.0; gzd = 0.0; gzu32 = 0.f; gzd32 = 0.f;
+        if (k + 1 < N) {
+            const double b = eps[(k + 1) * NN];
+            const float fb = (float)b;
+            gzu = e * b / (e + b);
+            gzu32 = f * fb / (f + fb);
+        }
+        if (k > 0) {
+            const double b = eps[(k - 1) * NN];
+            const float fb = (float)b;
+            gzd = b * e / (b + e);
+            gzd32 = fb * f / (fb + f);
+        }
+    }
+};
+
+// Whether an FP64 permittivity array holds one valid value per z plane
+// (CTA-wide; all threads get the answer).
+template <int N>
+DRWC_DEV bool planar_cube(const double* __restrict__ eps) {
+    constexpr int NN = N * N;
+    bool ok = true;
+    for (int c = threadIdx.x; c < N * NN; c += blockDim.x) {
+        const double v = eps[c], v0 = eps[(c / NN) * NN];
+        ok &= v == v0 && v > 0.0 && isfinite(v);
+    }
+    return __syncthreads_and(ok) != 0;
+}
+
 // EpsUniform: permittivity 1 everywhere (the warm-start bootstrap).
 struct EpsUniform {
     DRWC_DEV double e64(int) const { return 1.0; }
@@ -675,6 +757,248 @@ DRWC_SOLVE_ATTR void cube_solve(const E eps, double* __restrict__ ys, float* __r
         }
         __syncthreads();  // y of the neighbours visible
         relres = residual(false);
+        ++sweeps;
+        if (relres <= prm.tol) status = 0;
+    }
+    st->status = status;
+    st->escalated = outer > prm.max_outer;
+    st->iters = total_inner;
+    st->sweeps = sweeps;
+    st->relres = relres;
+    __syncthreads();
+}
+
+// Block sum of a float through FP32 partials read back four at a time (one
+// shared-memory wavefront per four warps); fixed order, all threads get it.
+// Its two slots lie after red[0..NW) (block_sum_d's slot 0), so it can follow
+// a block_sum_d without a barrier in between.
+template <int NW>
+DRWC_DEV float block_sum_f4(float v, double* red, int slot) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    float* rf = reinterpret_cast<float*>(red + NW) + slot * ((NW + 3) / 4) * 4;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) rf[warp] = v;
+    __syncthreads();
+    float s = 0.f;
+    if constexpr (NW % 4 == 0) {
+        const float4* r4 = reinterpret_cast<const float4*>(rf);
+#pragma unroll
+        for (int w = 0; w < NW / 4; ++w) {
+            const float4 q = r4[w];
+            s += q.x; s += q.y; s += q.z; s += q.w;
+        }
+    } else {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) s += rf[w];
+    }
+    return s;
+}
+
+// ------------------------------------------------------------ stratified cubes
+// The system K y = e of cube_solve for a cube whose material depends only on
+// the z index: every x/y link of plane k has conductance g(k,k) and the z
+// link between planes k and k+1 has g(k,k+1), so K is four numbers per plane.
+// The FP32 inner solve is Jacobi-preconditioned CG on K itself (the same
+// iteration as cube_solve's CG on S K S: r.D^-1 r is that solve's residual
+// norm), the FP64 refinement is cube_solve's; there are no per-cell
+// coefficient arrays, so a CG iteration reads four neighbour values of p and
+// two per-plane table entries per cell.
+//   per plane k (FP64 and FP32 tables in the cx / cy / cz regions):
+//     gxy = g(k,k), gz = g(k,k+1) (0 for the top plane),
+//     zd = (k+1 < N ? g(k,k+1) : eps_k) + (k > 0 ? g(k-1,k) : eps_k), eps_k;
+//   D_c = nxy*gxy + (4-nxy)*eps_k + zd, nxy = the interior x/y neighbours of
+//   the cell's column (i, j).
+// E provides plane(k, ...) (EpsPlanar, EpsGlobalPlanar) and e64(c). On
+// return cube_y<N>(ys) holds y, as after cube_solve.
+template <int N, class E>
+DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int code,
+                                       const FdmParams& prm, FdmStats* st) {
+    const CubeSmem<N> sm = CubeSmem<N>::carve(drwc_dyn_smem);
+    using D = Cube<N>;
+    static_assert(D::SPLIT == 1, "planar solve: one thread per column");
+    constexpr int NN = D::NN;
+    constexpr int NW = D::NW;
+    const int t = threadIdx.x;
+    const bool active = t < NN;
+    const int col = active ? t : 0;
+    const int i = col % N, j = col / N;
+    const bool xm = i > 0, xp = i + 1 < N, ym = j > 0, yp = j + 1 < N;
+    const int nxy = (int)xm + (int)xp + (int)ym + (int)yp;
+    // x/y neighbour offsets, clamped to the cell itself where the neighbour
+    // is outside the cube, and 0/1 weights: every load is unconditional and
+    // in bounds, so the stencils have no branches
+    const int oxm = xm ? -1 : 0, oxp = xp ? 1 : 0, oym = ym ? -N : 0, oyp = yp ? N : 0;
+    const float fxm = xm, fxp = xp, fym = ym, fyp = yp;
+    double* __restrict__ Y;
+    if constexpr (D::YSMEM) Y = sm.y;
+    else Y = ys;
+    // tables at the 16-byte aligned starts of the cx / cy / cz regions
+    double2* T64 = reinterpret_cast<double2*>(sm.cx - D::PAD);  // 3N: {gxy, gz}, {zd, eps}, {1/eps, 0}
+    float4* T32 = reinterpret_cast<float4*>(sm.cy - D::PAD);    // N: {gxy, gz, zd, eps}
+    float2* DI = reinterpret_cast<float2*>(sm.cz - D::PAD);     // 3N: {D, 1/D} per (k, nxy-2)
+    const double* __restrict__ warm = prm.warm[code & 3];
+
+    // ---- set-up: plane tables, right-hand side, y = the warm start (or 0)
+    for (int g = t; g < D::PAD; g += D::NT) {
+        sm.p[-D::PAD + g] = 0.f;
+        sm.p[D::NNN + g] = 0.f;
+    }
+    if (t < N) {
+        const int k = t;
+        double e, einv, gxy, gzu, gzd;
+        float gxy32, gzu32, gzd32;
+        eps.plane(k, e, einv, gxy, gzu, gzd, gxy32, gzu32, gzd32);
+        const double zd = (k + 1 < N ? gzu : e) + (k > 0 ? gzd : e);
+        T64[3 * k] = make_double2(gxy, gzu);
+        T64[3 * k + 1] = make_double2(zd, e);
+        T64[3 * k + 2] = make_double2(einv, 0.0);
+        const float e32 = (float)e;
+        const float zd32 = (k + 1 < N ? gzu32 : e32) + (k > 0 ? gzd32 : e32);
+        T32[k] = make_float4(gxy32, gzu32, zd32, e32);
+#pragma unroll
+        for (int nb = 2; nb <= 4; ++nb) {
+            const float dv = (float)nb * gxy32 + (float)(4 - nb) * e32 + zd32;
+            DI[3 * k + nb - 2] = make_float2(dv, 1.f / dv);
+        }
+    }
+    build_rhs<N>(eps, code, sm);
+    __syncthreads();  // tables written
+    if (active) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const int c = col + k * NN;
+            Y[c] = warm ? warm[c] * T64[3 * k + 2].x : 0.0;
+        }
+    }
+    __syncthreads();
+    double enorm2 = 0.0;
+    const int nrhs = sm.flags[0];
+    unsigned int rmask = 0u;  // bit k: cell (col, k) carries a source term
+    for (int v = 0; v < nrhs; ++v) {
+        const double ev = sm.rhs_val[v];
+        enorm2 += ev * ev;
+        const int cell = sm.rhs_idx[v];
+        if (active && cell % NN == col) rmask |= 1u << (cell / NN);
+    }
+    const double enorm = sqrt(enorm2);
+    const int di = nxy >= 2 ? nxy - 2 : 0;  // N >= 4: every column has >= 2 x/y neighbours
+
+    float r[N], x[N], q[N], pr[N];
+    // FP64 residual r64 = e - K y into r (FP32); returns ||r64|| / ||e||
+    auto residual = [&]() -> double {
+        double rn2 = 0.0;
+        double yb = 0.0;              // y of the cell below
+        double yc = Y[col];
+        double gzb = 0.0;             // g(k-1,k)
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            const int c = col + k * NN;
+            const double ya = k + 1 < N ? Y[c + NN] : 0.0;
+            const double2 a = T64[3 * k], b = T64[3 * k + 1];
+            const double sxy = (double)fxm * Y[c + oxm] + (double)fxp * Y[c + oxp] +
+                               (double)fym * Y[c + oym] + (double)fyp * Y[c + oyp];
+            const double diag = (double)nxy * a.x + (double)(4 - nxy) * b.y + b.x;
+            const double off = a.x * sxy + a.y * ya + gzb * yb;
+            double e_c = 0.0;
+            if ((rmask >> k) & 1u)
+                for (int v = 0; v < nrhs; ++v)
+                    if (sm.rhs_idx[v] == c) e_c = sm.rhs_val[v];
+            const double r64 = e_c - (diag * yc - off);
+            if (active) rn2 += r64 * r64;
+            r[k] = active ? (float)r64 : 0.f;
+            yb = yc;
+            yc = ya;
+            gzb = a.y;
+        }
+        rn2 = block_sum_d<NW>(rn2, sm.red, 0);
+        return sqrt(rn2) / enorm;
+    };
+    int sweeps = 0;
+    double relres = 1.0;
+    if (warm) {
+        relres = residual();
+        sweeps = 1;
+    } else {
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            r[k] = 0.f;
+            if ((rmask >> k) & 1u) {
+                const int c = col + k * NN;
+                for (int v = 0; v < nrhs; ++v)
+                    if (sm.rhs_idx[v] == c) r[k] = (float)sm.rhs_val[v];
+            }
+        }
+    }
+    int total_inner = 0, outer = 0;
+    int status = relres <= prm.tol ? 0 : 1;
+#pragma unroll 1
+    for (outer = 0; status != 0 && outer < prm.max_outer + prm.extra_outer; ++outer) {
+        const int max_inner = outer < prm.max_outer ? prm.max_inner : 4 * prm.max_inner;
+        // ---- FP32 Jacobi-PCG on K d = r64, d in x[]: z = D^-1 r, p = z
+        float rz = 0.f;
+#pragma unroll
+        for (int k = 0; k < N; ++k) {
+            x[k] = 0.f;
+            const float z = r[k] * DI[3 * k + di].y;
+            pr[k] = z;
+            if (active) sm.p[col + k * NN] = z;
+            rz += r[k] * z;
+        }
+        rz = block_sum_f4<NW>(rz, sm.red, 1);  // barrier also publishes p
+        const float want = fmaxf(prm.inner_tol, (float)(0.5 * prm.tol / relres));
+        const float stop2 = rz * want * want;
+        int it = 0;
+#pragma unroll 1
+        for (it = 0; it < max_inner && rz > stop2; ++it) {
+            float pq = 0.f;
+            if (active) {
+                float pb = 0.f, gzb = 0.f;
+#pragma unroll
+                for (int k = 0; k < N; ++k) {
+                    const int c = col + k * NN;
+                    const float4 tk = T32[k];
+                    const float dk = DI[3 * k + di].x;
+                    const float pa = k + 1 < N ? pr[k + 1] : 0.f;
+                    const float sxy = fxm * sm.p[c + oxm] + fxp * sm.p[c + oxp] +
+                                      fym * sm.p[c + oym] + fyp * sm.p[c + oyp];
+                    q[k] = dk * pr[k] - tk.x * sxy - tk.y * pa - gzb * pb;
+                    pq += pr[k] * q[k];
+                    pb = pr[k];
+                    gzb = tk.y;
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < N; ++k) q[k] = 0.f;
+            }
+            pq = block_sum_f4<NW>(pq, sm.red, 0);
+            const float alpha = rz / pq;
+            float rz2 = 0.f;
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                x[k] += alpha * pr[k];
+                r[k] -= alpha * q[k];
+                q[k] = r[k] * DI[3 * k + di].y;  // z
+                rz2 += r[k] * q[k];
+            }
+            rz2 = block_sum_f4<NW>(rz2, sm.red, 1);
+            const float beta = rz2 / rz;
+            rz = rz2;
+#pragma unroll
+            for (int k = 0; k < N; ++k) {
+                pr[k] = q[k] + beta * pr[k];
+                if (active) sm.p[col + k * NN] = pr[k];
+            }
+            __syncthreads();
+        }
+        total_inner += it;
+        // ---- y += d
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) Y[col + k * NN] += (double)x[k];
+        }
+        __syncthreads();  // y of the neighbours visible
+        relres = residual();
         ++sweeps;
         if (relres <= prm.tol) status = 0;
     }

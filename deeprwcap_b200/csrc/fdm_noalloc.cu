@@ -83,6 +83,8 @@ fdm_noalloc_kernel(int ncubes, const double* __restrict__ eps, const int32_t* __
         if (cd < DRWC_GFT || cd > DRWC_WVTY) {  // not a solver code: status 2, zero rows
             st.status = 2; st.iters = 0; st.sweeps = 0; st.relres = CUDART_NAN;
             st.escalated = 0;
+        } else if (planar_cube<N>(e)) {  // one permittivity per z plane
+            cube_solve_planar<N>(EpsGlobalPlanar<N>{e}, ys, cd, prm, &st);
         } else {
             cube_solve<N>(EpsGlobal{e}, ys, ss, cd, prm, &st);
         }

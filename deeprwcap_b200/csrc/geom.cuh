@@ -231,13 +231,20 @@ DRWC_DEV void voxelise(const DevGeom& g, const double c[3], double a, const doub
 // its z index (mat_at's layer rule at that index's centre z), decided once
 // per index into lm (shared, N ints).
 template <int N>
-DRWC_DEV void voxelise_planes(const DevGeom& g, const double c[3], double a, const double* tco,
-                              uint8_t* mat, int* lm) {
+DRWC_DEV void plane_layers(const DevGeom& g, const double c[3], double a, const double* tco,
+                           int* lm) {
     const int t = threadIdx.x;
     if (t < N) {
         const double z = dadd(c[2], dmul(a, tco[t]));
         lm[t] = g.n_layers > 0 ? g.lmat[layer_index(g, z)] : 0;
     }
+}
+
+template <int N>
+DRWC_DEV void voxelise_planes(const DevGeom& g, const double c[3], double a, const double* tco,
+                              uint8_t* mat, int* lm) {
+    const int t = threadIdx.x;
+    plane_layers<N>(g, c, a, tco, lm);
     __syncthreads();
     for (int v = t; v < N * N * N; v += blockDim.x) mat[v] = (uint8_t)lm[v / (N * N)];
 }

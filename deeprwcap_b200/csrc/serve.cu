@@ -67,6 +67,8 @@ struct SvJob {
     double* rec_w;     // records: slot q at q * batch
     int32_t* rec_end;
     int32_t* rec_hops;
+    int32_t* out_end;  // the caller's per-walk records by walk id (nullable)
+    double* out_w;
 };
 
 struct SvCtr {
@@ -178,6 +180,10 @@ DRWC_DEV void sv_finish(const SvArgs& A, int slot, int net) {
         J.rec_end[r] = net;
         J.rec_hops[r] = A.st.hops[slot];
         J.rec_w[r] = A.st.omega[slot];
+        if (J.out_end) {
+            J.out_end[w] = net;
+            J.out_w[w] = A.st.omega[slot];
+        }
         atomicAdd(&A.ctr[j].done[p], 1ull);
     }
     atomicAdd(&A.ctr[j].inflight, ~0ull);
@@ -617,19 +623,33 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
         const int code = first ? A.st.code[slot] : DRWC_GFT;
         const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
         const double a = A.st.a[slot];
+        // a stratified cube (no dielectric block reaches it) goes to the
+        // per-plane solver
+        const int* lmc = nullptr;
         if (gs.n_diel > 0) {
             vox_prepare<N>(gs, c, a, tco, vs);
-            for (int v = threadIdx.x; v < D::NNN; v += blockDim.x)
-                mat[v] = (uint8_t)vox_material<N>(gs, vs, c, a, tco, v % N, (v / N) % N,
-                                                  v / D::NN, 0);
+            if (vs.nrel == 0) {
+                lmc = vs.lm;
+            } else {
+                for (int v = threadIdx.x; v < D::NNN; v += blockDim.x)
+                    mat[v] = (uint8_t)vox_material<N>(gs, vs, c, a, tco, v % N, (v / N) % N,
+                                                      v / D::NN, 0);
+            }
         } else {
-            voxelise_planes<N>(gs, c, a, tco, mat, lm);
+            plane_layers<N>(gs, c, a, tco, lm);
+            lmc = lm;
         }
         __syncthreads();
         FdmStats st;
-        cube_solve<N>(E, ys, ss, code, J.W.prm, &st);
         double* wv = reinterpret_cast<double*>(sm.stage());
-        for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+        const EpsPlanar<N> EP{lmc, pal, palinv, pair64, pair32, P};
+        if (lmc) {
+            cube_solve_planar<N>(EP, ys, code, J.W.prm, &st);
+            for_each_panel<N>(EP, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+        } else {
+            cube_solve<N>(E, ys, ss, code, J.W.prm, &st);
+            for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+        }
         __syncthreads();
         if ((kind & 1) && !first) {
             // audit: KL(FDM || network) over the panels
@@ -660,8 +680,9 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
                 sv_finish(A, slot, -1);
             } else {
                 if (first)
-                    A.st.omega[slot] =
-                        first_hop_weight(J.G, A.st.sgn[slot], center_diel<N>(E, code), tot, wv[b], a);
+                    A.st.omega[slot] = first_hop_weight(
+                        J.G, A.st.sgn[slot],
+                        lmc ? center_diel<N>(EP, code) : center_diel<N>(E, code), tot, wv[b], a);
                 double loc[3];
                 locate_f64(N, b, loc);
                 A.st.px[slot] = dadd(A.st.px[slot], dmul(a, loc[0]));
@@ -789,6 +810,8 @@ struct SvHostJob {
     size_t arena_off = 0, arena_bytes = 0, blob_bytes = 0;
     bool draining = false;
     std::vector<double> S, Sc, S2, S2c;
+    int32_t* out_end = nullptr;                     // caller's per-walk records (device)
+    double* out_w = nullptr;
     long long walks = 0, lost = 0, next_batch = 0;  // next_batch: next to fold
     long long next_assign = 0;                       // next batch to get a record slot
     std::map<long long, std::vector<double>> pending; // reduced, not yet folded
@@ -1108,6 +1131,8 @@ static int sv_admit(drwc_server* v) {
         T.rec_w = (double*)(base + blob);
         T.rec_end = (int32_t*)(base + blob + nb * batch * 8);
         T.rec_hops = T.rec_end + nb * batch;
+        T.out_end = J->out_end;
+        T.out_w = J->out_w;
         std::memset(&v->h_ctr[t], 0, sizeof(SvCtr));
         J->table = t;
         J->arena_off = off;
@@ -1614,7 +1639,13 @@ DRWC_API int drwc_server_destroy(drwc_server* v) {
 
 DRWC_API int drwc_server_submit(drwc_server* v, const drwc_structure* s, const drwc_job_params* p,
                                 int64_t* job_id) {
-    if (!v || !s || !p || !job_id) return DRWC_ERR_INVALID;
+    return drwc_server_submit_records(v, s, p, nullptr, nullptr, job_id);
+}
+
+DRWC_API int drwc_server_submit_records(drwc_server* v, const drwc_structure* s,
+                                        const drwc_job_params* p, int32_t* end_net,
+                                        double* weight, int64_t* job_id) {
+    if (!v || !s || !p || !job_id || (!end_net) != (!weight)) return DRWC_ERR_INVALID;
     *job_id = 0;
     if (!n_supported(p->N) || v->bucket_of_N[p->N] < 0 || p->batch_walks < 1 ||
         p->max_walks < 1 || p->min_walks < 0 || s->n_nets > v->o.max_nets || s->n_boxes < 0 ||
@@ -1633,6 +1664,8 @@ DRWC_API int drwc_server_submit(drwc_server* v, const drwc_structure* s, const d
     J->s.layer_eps = J->leps.empty() ? nullptr : J->leps.data();
     J->s.diel = J->diel.empty() ? nullptr : J->diel.data();
     J->p = *p;
+    J->out_end = end_net;
+    J->out_w = weight;
     // validation, Gaussian surface and packing run on the host; the
     // warm-start tables of the served sizes were made at creation, so this
     // needs neither the device nor the context lock

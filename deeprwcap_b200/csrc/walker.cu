@@ -126,21 +126,35 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
                     W.log_code[li] = code;
                 }
             }
+            // a stratified cube (no dielectric block reaches it) is solved by
+            // the per-plane solver from its layer materials alone
+            const int* lm = nullptr;
             if (g.n_diel > 0) {  // separable: per-axis index ranges of the blocks
                 VoxScratch<N>& vs = *reinterpret_cast<VoxScratch<N>*>(
                     smem + (WalkSmem<N>::base(P) + 15) / 16 * 16);
                 vox_prepare<N>(g, c, a, tco, vs);
-                for (int v = t; v < D::NNN; v += blockDim.x)
-                    mat[v] = (uint8_t)vox_material<N>(g, vs, c, a, tco, v % N, (v / N) % N,
-                                                      v / D::NN, 0);
+                if (vs.nrel == 0) {
+                    lm = vs.lm;
+                } else {
+                    for (int v = t; v < D::NNN; v += blockDim.x)
+                        mat[v] = (uint8_t)vox_material<N>(g, vs, c, a, tco, v % N, (v / N) % N,
+                                                          v / D::NN, 0);
+                }
             } else {
-                voxelise_planes<N>(g, c, a, tco, mat, S.lm);
+                plane_layers<N>(g, c, a, tco, S.lm);
+                lm = S.lm;
             }
             __syncthreads();
             FdmStats st;
-            cube_solve<N>(E, ys, ss, code, W.prm, &st);
             double* wv = reinterpret_cast<double*>(sm.stage());
-            for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+            const EpsPlanar<N> EP{lm, pal, palinv, pair64, pair32, P};
+            if (lm) {
+                cube_solve_planar<N>(EP, ys, code, W.prm, &st);
+                for_each_panel<N>(EP, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+            } else {
+                cube_solve<N>(E, ys, ss, code, W.prm, &st);
+                for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+            }
             __syncthreads();
             const double2 u = first ? philox_uniform2(W.seed, w, 0, 1)
                                     : philox_uniform2(W.seed, w, (uint32_t)S.hops, 0);
@@ -160,8 +174,9 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
                     S.done = 2;
                 } else {
                     if (first)
-                        S.omega = first_hop_weight(G, S.sgn_out, center_diel<N>(E, code), tot,
-                                                   wv[b], a);
+                        S.omega = first_hop_weight(
+                            G, S.sgn_out, lm ? center_diel<N>(EP, code) : center_diel<N>(E, code),
+                            tot, wv[b], a);
                     double loc[3];
                     locate_f64(N, b, loc);
                     for (int d = 0; d < 3; ++d) S.r[d] = dadd(S.r[d], dmul(a, loc[d]));
@@ -1002,19 +1017,31 @@ lw_fdm_kernel(LwArgs A, double* __restrict__ scratch_y, float* __restrict__ scra
         const int code = first ? A.st.code[slot] : DRWC_GFT;
         const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
         const double a = A.st.a[slot];
+        const int* lmc = nullptr;  // stratified cube: the per-plane solver
         if (g.n_diel > 0) {
             vox_prepare<N>(g, c, a, tco, vs);
-            for (int v = threadIdx.x; v < D::NNN; v += blockDim.x)
-                mat[v] = (uint8_t)vox_material<N>(g, vs, c, a, tco, v % N, (v / N) % N,
-                                                  v / D::NN, 0);
+            if (vs.nrel == 0) {
+                lmc = vs.lm;
+            } else {
+                for (int v = threadIdx.x; v < D::NNN; v += blockDim.x)
+                    mat[v] = (uint8_t)vox_material<N>(g, vs, c, a, tco, v % N, (v / N) % N,
+                                                      v / D::NN, 0);
+            }
         } else {
-            voxelise_planes<N>(g, c, a, tco, mat, lm);
+            plane_layers<N>(g, c, a, tco, lm);
+            lmc = lm;
         }
         __syncthreads();
         FdmStats st;
-        cube_solve<N>(E, ys, ss, code, A.W.prm, &st);
         double* wv = reinterpret_cast<double*>(sm.stage());
-        for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+        const EpsPlanar<N> EP{lmc, pal, palinv, pair64, pair32, P};
+        if (lmc) {
+            cube_solve_planar<N>(EP, ys, code, A.W.prm, &st);
+            for_each_panel<N>(EP, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+        } else {
+            cube_solve<N>(E, ys, ss, code, A.W.prm, &st);
+            for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+        }
         __syncthreads();
         if (audit && !first) {
             // KL(FDM || network) over the panels
@@ -1041,8 +1068,9 @@ lw_fdm_kernel(LwArgs A, double* __restrict__ scratch_y, float* __restrict__ scra
         const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
         if (threadIdx.x == 0 && b >= 0 && st.status == 0) {
             if (first)
-                A.st.omega[slot] = first_hop_weight(A.G, A.st.sgn[slot], center_diel<N>(E, code),
-                                                    tot, wv[b], a);
+                A.st.omega[slot] = first_hop_weight(
+                    A.G, A.st.sgn[slot], lmc ? center_diel<N>(EP, code) : center_diel<N>(E, code),
+                    tot, wv[b], a);
             double loc[3];
             locate_f64(N, b, loc);
             A.st.px[slot] = dadd(A.st.px[slot], dmul(a, loc[0]));

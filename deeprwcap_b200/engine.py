@@ -593,11 +593,21 @@ class Server:
         self.h = h
         self.nets = nets  # the server holds them
 
-    def submit(self, structure, params) -> int:
+    def submit(self, structure, params, records=None) -> int:
+        """Queue a job. records = (end_net, weight) device tensors of
+        params.max_walks entries: every finished walk writes its end net and
+        weight there at its walk id (drwc_server_submit_records)."""
         s = structure.to_c() if hasattr(structure, "to_c") else structure
         jid = C.c_int64()
-        check(self.ctx.lib.drwc_server_submit(self.h, C.byref(s), C.byref(params), C.byref(jid)),
-              "drwc_server_submit")
+        if records is None:
+            check(self.ctx.lib.drwc_server_submit(self.h, C.byref(s), C.byref(params),
+                                                  C.byref(jid)), "drwc_server_submit")
+        else:
+            end, w = records
+            torch_ready()
+            check(self.ctx.lib.drwc_server_submit_records(self.h, C.byref(s), C.byref(params),
+                                                          ptr(end), ptr(w), C.byref(jid)),
+                  "drwc_server_submit_records")
         return jid.value
 
     def poll(self, jid: int):

@@ -410,6 +410,16 @@ DRWC_API int drwc_server_destroy(drwc_server* srv);
  * max_materials. */
 DRWC_API int drwc_server_submit(drwc_server* srv, const drwc_structure* s,
                                 const drwc_job_params* p, int64_t* job_id);
+/* As drwc_server_submit, and every walk that finishes also writes its end net
+ * (-1: lost) and weight (fF) at its walk id into the caller's DEVICE arrays
+ * end_net / weight (p->max_walks entries each; ids a converged job never ran
+ * keep what the caller put there). Walk w of a job is walk w of
+ * drwc_frw_walks with the same parameters, so the records can be compared
+ * walk by walk with another form of the same job. The arrays must stay
+ * valid until the job is done. */
+DRWC_API int drwc_server_submit_records(drwc_server* srv, const drwc_structure* s,
+                                        const drwc_job_params* p, int32_t* end_net,
+                                        double* weight, int64_t* job_id);
 enum { DRWC_JOB_QUEUED = 0, DRWC_JOB_RUNNING = 1, DRWC_JOB_DONE = 2, DRWC_JOB_FAILED = 3 };
 /* state (host): queued / running / done / failed; out (nullable) gets the
  * result once done, with seconds = submission to completion. Returns the
