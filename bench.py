@@ -158,19 +158,57 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def traffic_from_profile():
-    """Per-launch DRAM bytes of the walk kernel from the committed ncu
-    summary (profiles/walk_kernel_two_layer_crossing_N16.txt), if present."""
+def walk_roofline(prof, hops_tot, t_dev, steps, clocks, streamed_gbs, hbm, src):
+    """Roofline of the walk kernel. The kernel keeps each cube in shared
+    memory and registers, so its bound is the shared-memory pipe: achieved =
+    the ncu shared-memory wavefronts per hop x 128 B x the hops per second
+    measured here; peak = 148 SMs x 128 B per clock at the sampled median SM
+    clock; traffic = ncu DRAM bytes per hop x hops per launch. The streamed-
+    PCG figure (the HBM bytes an HBM-resident solver would move for the same
+    iterations) is kept as a secondary field."""
+    mhz = clocks.get("sm_mhz") or 1965.0
+    wf = prof.get("smem_wavefronts_per_hop")
+    dram = prof.get("dram_bytes_per_hop")
+    hps = hops_tot / t_dev
+    out = {"bound": "smem", "unit": "GB/s", "peak": smem_peak_gbs(mhz),
+           "peak_source": f"148 SMs x 128 B/clk x {mhz:.0f} MHz (sampled median)",
+           "achieved": None, "frac": None,
+           "traffic": None if dram is None else dram * hops_tot / steps,
+           "smem_wavefronts_per_hop": wf, "dram_bytes_per_hop": dram,
+           "fma_pipe_frac_profiled": prof.get("fma_pipe_frac"),
+           "fp64_pipe_frac_profiled": prof.get("fp64_pipe_frac"),
+           "issue_frac_profiled": prof.get("issue_active_frac"),
+           "streamed_pcg_hbm_equivalent": {"achieved": streamed_gbs, "peak": hbm,
+                                           "frac": streamed_gbs / hbm, "peak_source": src},
+           "note": "achieved = ncu shared-memory wavefronts per hop x 128 B x live hops/s; "
+                   "*_profiled are fractions from the ncu capture (a 2048-walk launch)"}
+    if wf:
+        out["achieved"] = wf * 128.0 * hps / 1e9
+        out["frac"] = out["achieved"] / out["peak"]
+    return out
+
+
+def profile_figures():
+    """Per-hop figures of the walk kernel from the committed ncu summary
+    (profiles/walk_kernel_two_layer_crossing_N16.txt): lines "key: value"."""
     p = ROOT / "profiles" / "walk_kernel_two_layer_crossing_N16.txt"
+    out = {}
     if not p.exists():
-        return None
+        return out
     for line in p.read_text().splitlines():
-        if line.startswith("dram_bytes_per_launch_scaled:"):
+        if ":" in line and not line.startswith(" "):
+            k, v = line.split(":", 1)
             try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
-    return None
+                out[k.strip()] = float(v.split()[0])
+            except (ValueError, IndexError):
+                pass
+    return out
+
+
+def smem_peak_gbs(sm_mhz):
+    """Shared-memory pipe bandwidth of the GPU: 148 SMs x 128 B (one wavefront)
+    per SM clock at the sampled SM clock."""
+    return 148 * 128 * float(sm_mhz) * 1e6 / 1e9
 
 
 def learned_section(ctx, args):
@@ -590,7 +628,7 @@ def run_b200(args, world, rank, local):
     alg_bytes = (48.0 * iters_tot + 40.0 * sweeps_tot) * NNN + hops_tot * (8.0 * NNN +
                                                                           8.0 * 6 * N_CUBE ** 2)
     achieved = alg_bytes / args.steps / (t_dev / args.steps) / 1e9
-    traffic = traffic_from_profile()
+    prof = profile_figures()
 
     # ---- CPU baseline (rank 0, N = 1 only): reference CPU path on the host cores
     cpu = None
@@ -616,12 +654,8 @@ def run_b200(args, world, rank, local):
                        "solves_escalated": esc_tot, "solves_failed": fail_tot},
             "e2e": e2e,
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": traffic,
-                         "peak_source": src,
-                         "note": "achieved = streamed-PCG algorithmic bytes (48 B/cell/FP32 iter + "
-                                 "40 B/cell/FP64 sweep + eps in + 6N^2 out) / walk-kernel time; "
-                                 "the kernel keeps the cube on chip, so DRAM traffic is far lower"},
+            "roofline": walk_roofline(prof, hops_tot, t_dev, args.steps, clk.summary(),
+                                      achieved, hbm, src),
             "clocks": clk.summary(),
             "wall_s_timed": t_wall,
             "job": job_info,
