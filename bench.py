@@ -109,8 +109,9 @@ def workload():
     return s, p
 
 
-def cpu_walks(nthreads: int, budget_s: float, walk0: int, batch: int):
-    """Reference CPU path: restated walk loop + reference ggft per hop."""
+def cpu_walks(nthreads: int, budget_s: float, walk0: int, batch: int, records=None):
+    """Reference CPU path: restated walk loop + reference ggft per hop. With
+    records = [] the per-walk (end net, weight) arrays are appended to it."""
     from oracle import oracle as O
     s, p = workload()
     sc = s.to_c()
@@ -121,6 +122,8 @@ def cpu_walks(nthreads: int, budget_s: float, walk0: int, batch: int):
     w0 = walk0
     while time.perf_counter() - t0 < budget_s:
         e, h, w, _ = O.frw_walks(sc, p, w0, batch, fdm=fdm, fdm_tol=FDM_TOL, nthreads=nthreads)
+        if records is not None:
+            records.append((e, w))
         hops += int(h.sum())
         walks += batch
         w0 += batch
@@ -452,6 +455,10 @@ def summary_of(line):
          "cfg2_cubes_per_s": g(line, "fdm_config2", "cubes_per_s"),
          "cfg2_max_rel_err": g(line, "fdm_config2", "max_rel_err_vs_fp64_oracle"),
          "cpu_baseline_hops_per_s": g(line, "cpu_baseline", "value")}
+    pv = g(line, "cpu_baseline", "precision_vs_fp64_walk")
+    if pv:
+        s["precision_max_entry_rel_diff_vs_fp64_walk"] = max(
+            (abs(v["rel_diff"]) for v in pv["entries"].values()), default=None)
     lr = line.get("learned")
     if lr:
         s["dense_gain_learned_walker"] = lr.get("gain")
@@ -634,10 +641,35 @@ def run_b200(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         nthreads = os.cpu_count() or 1
-        h, w, dt, kind = cpu_walks(nthreads, args.cpu_s, 50_000_000, 2 * nthreads)
+        recs = []
+        h, w, dt, kind = cpu_walks(nthreads, args.cpu_s, 50_000_000, 2 * nthreads, recs)
         cpu = {"value": h / dt, "unit": "hops/s", "cores": nthreads, "kind": kind,
                "sample": f"{w} walks ({h} hops) of the same job, ~{args.cpu_s:.0f} s; restated "
                          f"CPU walk loop + reference ggft per hop (N={N_CUBE}, tol {FDM_TOL:g})"}
+        # precision form: the FP32 CG + FP64 refinement walk against the FP64
+        # FDM walk (the CPU walker above, reference ggft per hop) on the same
+        # walk ids, per capacitance entry
+        e_c = np.concatenate([r[0] for r in recs])
+        w_c = np.concatenate([r[1] for r in recs])
+        e_g, _, w_g = engine.frw_walks(s, p, 50_000_000, len(w_c), ctx=ctx)
+        same = (e_g == e_c)
+        ent = {}
+        for j in range(s.n_nets + 1):
+            x_c = np.where(e_c == j, w_c, 0.0)
+            x_g = np.where(e_g == j, w_g, 0.0)
+            c0 = x_c.mean()
+            if c0 == 0.0:
+                continue
+            d = x_g - x_c
+            ent[str(j)] = {"rel_diff": float(d.mean() / abs(c0)),
+                           "rel_3sem": float(3 * d.std() / np.sqrt(len(d)) / abs(c0))}
+        cpu["precision_vs_fp64_walk"] = {
+            "walks": int(len(w_c)), "same_end_net": float(same.mean()),
+            "max_weight_rel_diff_same_walks": float(np.max(
+                np.abs(w_g[same] - w_c[same]) / np.maximum(np.abs(w_c[same]), 1e-300))),
+            "entries": ent,
+            "note": "walk-by-walk: the device walk (FP32 CG + FP64 refinement to 1e-8) vs the "
+                    "CPU walk with the reference FP64 ggft per hop, same Philox streams"}
 
     if rank == 0:
         line = {

@@ -49,7 +49,8 @@ struct FdmParams {
 
 // Per-cube solve outcome.
 struct FdmStats {
-    int iters;       // FP32 CG iterations (all sweeps)
+    int iters;       // FP32 CG iterations (all sweeps); for stratified cubes the
+                     // FP32 direct solves (cube_solve_planar)
     int sweeps;      // FP64 residual evaluations (refinement sweeps + final check)
     double relres;   // final ||e - K y|| / ||e||
     int status;      // 0 converged, 1 not converged, 2 invalid permittivity
@@ -91,7 +92,16 @@ struct Cube {
     static constexpr size_t kFlagOff = kRhsValOff + sizeof(double) * kMaxRhs;
     static constexpr size_t kArrOff = ((kFlagOff + sizeof(int) * 8 + 127) / 128) * 128;
     static constexpr size_t kArrBytes = ((sizeof(float) * LEN + 15) / 16) * 16;
-    static constexpr size_t kYOff = kArrOff + 4 * kArrBytes;
+    // The stratified-cube solver (cube_solve_planar) uses the p|cx|cy|cz
+    // region as one block: two transform buffers of N planes x N rows of TS
+    // floats (rows 16-byte aligned and padded) and its per-plane tables.
+    static constexpr int TS = (N + 3) / 4 * 4 + 4;
+    static constexpr size_t kTBuf = (size_t)N * N * TS;            // floats per buffer
+    static constexpr size_t kPlanarTables = 16 * 3 * N + 16 * N + 4 * NN + 4 * N + 64;
+    static constexpr size_t kPlanarBytes = 2 * kTBuf * sizeof(float) + kPlanarTables;
+    static constexpr size_t kArrTotal =
+        4 * kArrBytes > kPlanarBytes ? 4 * kArrBytes : (kPlanarBytes + 15) / 16 * 16;
+    static constexpr size_t kYOff = kArrOff + kArrTotal;
     static constexpr size_t kSmemBytes = kYOff + (YSMEM ? sizeof(double) * NNN : 0);
     static_assert(kSmemBytes <= 227 * 1024, "cube does not fit in shared memory");
 };
@@ -797,18 +807,31 @@ DRWC_DEV float block_sum_f4(float v, double* red, int slot) {
 
 // ------------------------------------------------------------ stratified cubes
 // The system K y = e of cube_solve for a cube whose material depends only on
-// the z index: every x/y link of plane k has conductance g(k,k) and the z
-// link between planes k and k+1 has g(k,k+1), so K is four numbers per plane.
-// The FP32 inner solve is Jacobi-preconditioned CG on K itself (the same
-// iteration as cube_solve's CG on S K S: r.D^-1 r is that solve's residual
-// norm), the FP64 refinement is cube_solve's; there are no per-cell
-// coefficient arrays, so a CG iteration reads four neighbour values of p and
-// two per-plane table entries per cell.
-//   per plane k (FP64 and FP32 tables in the cx / cy / cz regions):
-//     gxy = g(k,k), gz = g(k,k+1) (0 for the top plane),
-//     zd = (k+1 < N ? g(k,k+1) : eps_k) + (k > 0 ? g(k-1,k) : eps_k), eps_k;
-//   D_c = nxy*gxy + (4-nxy)*eps_k + zd, nxy = the interior x/y neighbours of
-//   the cell's column (i, j).
+// the z index. Every x/y link of plane k has conductance g_k = g(k,k) =
+// eps_k / 2 and a cell on an x or y face adds eps_k = 2 g_k to its diagonal,
+// so the x/y part of K on plane k is g_k (T (x) I + I (x) T), where T is the
+// N x N matrix tridiag(-1, 2, -1) with 3 at both ends, the same for every
+// plane. T's eigenvectors are the cell-centred sine modes
+//   u_m(i) = s_m sin(pi (m+1) (2i+1) / (2N)),  lambda_m = 4 sin^2(pi (m+1) / (2N)),
+// m = 0..N-1, s_m = sqrt(2/N) (sqrt(1/N) for m = N-1), orthonormal. In that
+// basis K splits into N^2 independent tridiagonal systems along z, one per
+// mode (m, n):  (zd_k + (lambda_m + lambda_n) g_k) v_k - gz_k v_{k+1}
+// - gz_{k-1} v_{k-1} = rhs_k,  with gz_k = g(k,k+1) and zd_k the z part of
+// the diagonal (eps_k on the top and bottom faces). So K d = r is solved
+// exactly, without iterations: a 2-D sine transform of r (two passes through
+// shared memory), one Thomas solve per mode (one thread each, in registers)
+// and the inverse transform (two passes). This direct solve runs in FP32
+// as the inner solver of cube_solve's FP64 iterative refinement: the FP64
+// residual e - K y is formed from the FP64 permittivity (so the refinement
+// converges to the FP64 solution whatever the x/y operator's last-bit
+// agreement with g_k T), and every sweep gains about as many digits as FP32
+// carries. FdmStats::iters counts the direct solves.
+//
+// Shared memory (the p|cx|cy|cz block of the cube layout): two transform
+// buffers of N planes x N rows x TS floats, then the tables
+//   T64 (3N double2): {g_k, gz_k}, {zd_k, eps_k}, {1/eps_k, 0}
+//   T32 (N float4):   {g_k, gz_k, zd_k, eps_k} in FP32
+//   U (N x N floats): U[m][i] = u_m(i);  L (N floats): lambda_m.
 // E provides plane(k, ...) (EpsPlanar, EpsGlobalPlanar) and e64(c). On
 // return cube_y<N>(ys) holds y, as after cube_solve.
 template <int N, class E>
@@ -819,31 +842,27 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
     static_assert(D::SPLIT == 1, "planar solve: one thread per column");
     constexpr int NN = D::NN;
     constexpr int NW = D::NW;
+    constexpr int TS = D::TS;          // transform row stride (floats)
+    constexpr int TP = N * TS;         // transform plane stride
     const int t = threadIdx.x;
     const bool active = t < NN;
     const int col = active ? t : 0;
     const int i = col % N, j = col / N;
-    const bool xm = i > 0, xp = i + 1 < N, ym = j > 0, yp = j + 1 < N;
-    const int nxy = (int)xm + (int)xp + (int)ym + (int)yp;
-    // x/y neighbour offsets, clamped to the cell itself where the neighbour
-    // is outside the cube, and 0/1 weights: every load is unconditional and
-    // in bounds, so the stencils have no branches
-    const int oxm = xm ? -1 : 0, oxp = xp ? 1 : 0, oym = ym ? -N : 0, oyp = yp ? N : 0;
-    const float fxm = xm, fxp = xp, fym = ym, fyp = yp;
+    // the other index pair of the transform passes: a = t % N (lanes), b = t / N
+    const int ta = col % N, tb = col / N;
     double* __restrict__ Y;
     if constexpr (D::YSMEM) Y = sm.y;
     else Y = ys;
-    // tables at the 16-byte aligned starts of the cx / cy / cz regions
-    double2* T64 = reinterpret_cast<double2*>(sm.cx - D::PAD);  // 3N: {gxy, gz}, {zd, eps}, {1/eps, 0}
-    float4* T32 = reinterpret_cast<float4*>(sm.cy - D::PAD);    // N: {gxy, gz, zd, eps}
-    float2* DI = reinterpret_cast<float2*>(sm.cz - D::PAD);     // 3N: {D, 1/D} per (k, nxy-2)
+    float* XB = sm.p - D::PAD;               // transform buffer 1
+    float* ZB = XB + D::kTBuf;               // transform buffer 2
+    double2* T64 = reinterpret_cast<double2*>(ZB + D::kTBuf);
+    float4* T32 = reinterpret_cast<float4*>(T64 + 3 * N);
+    float* U = reinterpret_cast<float*>(T32 + N);
+    float* L = U + NN;
     const double* __restrict__ warm = prm.warm[code & 3];
 
-    // ---- set-up: plane tables, right-hand side, y = the warm start (or 0)
-    for (int g = t; g < D::PAD; g += D::NT) {
-        sm.p[-D::PAD + g] = 0.f;
-        sm.p[D::NNN + g] = 0.f;
-    }
+    // ---- set-up: plane tables, sine modes, right-hand side, y = the warm
+    //      start (or 0)
     if (t < N) {
         const int k = t;
         double e, einv, gxy, gzu, gzd;
@@ -856,11 +875,12 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
         const float e32 = (float)e;
         const float zd32 = (k + 1 < N ? gzu32 : e32) + (k > 0 ? gzd32 : e32);
         T32[k] = make_float4(gxy32, gzu32, zd32, e32);
-#pragma unroll
-        for (int nb = 2; nb <= 4; ++nb) {
-            const float dv = (float)nb * gxy32 + (float)(4 - nb) * e32 + zd32;
-            DI[3 * k + nb - 2] = make_float2(dv, 1.f / dv);
-        }
+        const float sl = sinpif((float)(k + 1) / (float)(2 * N));
+        L[k] = 4.f * sl * sl;
+    }
+    if (active) {  // U[m][i], m = tb, i = ta
+        const float s = tb + 1 < N ? sqrtf(2.f / N) : sqrtf(1.f / N);
+        U[tb * N + ta] = s * sinpif((float)((tb + 1) * (2 * ta + 1)) / (float)(2 * N));
     }
     build_rhs<N>(eps, code, sm);
     __syncthreads();  // tables written
@@ -882,9 +902,14 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
         if (active && cell % NN == col) rmask |= 1u << (cell / NN);
     }
     const double enorm = sqrt(enorm2);
-    const int di = nxy >= 2 ? nxy - 2 : 0;  // N >= 4: every column has >= 2 x/y neighbours
+    // x/y neighbour offsets clamped to the cell itself outside the cube, and
+    // 0/1 weights: the residual's loads are unconditional and in bounds
+    const bool xm = i > 0, xp = i + 1 < N, ym = j > 0, yp = j + 1 < N;
+    const int nxy = (int)xm + (int)xp + (int)ym + (int)yp;
+    const int oxm = xm ? -1 : 0, oxp = xp ? 1 : 0, oym = ym ? -N : 0, oyp = yp ? N : 0;
+    const double fxm = xm, fxp = xp, fym = ym, fyp = yp;
 
-    float r[N], x[N], q[N], pr[N];
+    float r[N];
     // FP64 residual r64 = e - K y into r (FP32); returns ||r64|| / ||e||
     auto residual = [&]() -> double {
         double rn2 = 0.0;
@@ -896,8 +921,8 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
             const int c = col + k * NN;
             const double ya = k + 1 < N ? Y[c + NN] : 0.0;
             const double2 a = T64[3 * k], b = T64[3 * k + 1];
-            const double sxy = (double)fxm * Y[c + oxm] + (double)fxp * Y[c + oxp] +
-                               (double)fym * Y[c + oym] + (double)fyp * Y[c + oyp];
+            const double sxy = fxm * Y[c + oxm] + fxp * Y[c + oxp] + fym * Y[c + oym] +
+                               fyp * Y[c + oyp];
             const double diag = (double)nxy * a.x + (double)(4 - nxy) * b.y + b.x;
             const double off = a.x * sxy + a.y * ya + gzb * yb;
             double e_c = 0.0;
@@ -913,6 +938,90 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
         }
         rn2 = block_sum_d<NW>(rn2, sm.red, 0);
         return sqrt(rn2) / enorm;
+    };
+    // one sum of a transform pass: row[0..N) . w[0..N) (w in registers)
+    auto dot_row = [&](const float* row, const float (&w)[N]) -> float {
+        float acc = 0.f;
+        if constexpr (N % 4 == 0) {
+#pragma unroll
+            for (int q = 0; q < N / 4; ++q) {
+                const float4 v = reinterpret_cast<const float4*>(row)[q];
+                acc = fmaf(v.x, w[4 * q], acc);
+                acc = fmaf(v.y, w[4 * q + 1], acc);
+                acc = fmaf(v.z, w[4 * q + 2], acc);
+                acc = fmaf(v.w, w[4 * q + 3], acc);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < N; ++q) acc = fmaf(row[q], w[q], acc);
+        }
+        return acc;
+    };
+    // FP32 direct solve K d = r (r in this thread's column): d into r
+    auto direct_solve = [&]() {
+        float w[N];
+        // r -> buffer 1 as [k][j][i]
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) XB[k * TP + j * TS + i] = r[k];
+        }
+        __syncthreads();
+        // pass 1 (thread m = ta, j = tb): P[k][m][j] = sum_i U[m][i] X[k][j][i]
+        if (active) {
+#pragma unroll
+            for (int q = 0; q < N; ++q) w[q] = U[ta * N + q];
+#pragma unroll 4
+            for (int k = 0; k < N; ++k) ZB[k * TP + ta * TS + tb] = dot_row(XB + k * TP + tb * TS, w);
+        }
+        __syncthreads();
+        // pass 2 (thread n = ta, m = tb): mode (m, n) = sum_j U[n][j] P[k][m][j],
+        // then the mode's tridiagonal solve along k, all in registers
+        float v[N];
+        if (active) {
+#pragma unroll
+            for (int q = 0; q < N; ++q) w[q] = U[ta * N + q];
+#pragma unroll 4
+            for (int k = 0; k < N; ++k) v[k] = dot_row(ZB + k * TP + tb * TS, w);
+            const float lam = L[ta] + L[tb];
+            float gprev = 0.f, fprev = 0.f, gzb = 0.f;
+            float g[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) {  // Thomas, forward
+                const float4 tk = T32[k];
+                // sub- and super-diagonal -gz: den_k = b_k - gz_{k-1}^2 / den_{k-1}
+                const float den = fmaf(lam, tk.x, tk.z) + gzb * gprev;
+                const float inv = 1.f / den;
+                g[k] = -tk.y * inv;
+                fprev = (v[k] + gzb * fprev) * inv;
+                v[k] = fprev;
+                gprev = g[k];
+                gzb = tk.y;
+            }
+#pragma unroll
+            for (int k = N - 2; k >= 0; --k) v[k] -= g[k] * v[k + 1];  // back
+        }
+        __syncthreads();  // buffer 1 free
+        // modes -> buffer 1 as [k][m][n]
+        if (active) {
+#pragma unroll
+            for (int k = 0; k < N; ++k) XB[k * TP + tb * TS + ta] = v[k];
+        }
+        __syncthreads();
+        // pass 3 (thread j = ta, m = tb): Q[k][j][m] = sum_n U[n][j] V[k][m][n]
+        if (active) {
+#pragma unroll
+            for (int q = 0; q < N; ++q) w[q] = U[q * N + ta];
+#pragma unroll 4
+            for (int k = 0; k < N; ++k) ZB[k * TP + ta * TS + tb] = dot_row(XB + k * TP + tb * TS, w);
+        }
+        __syncthreads();
+        // pass 4 (thread i, j): d[k] = sum_m U[m][i] Q[k][j][m]
+        if (active) {
+#pragma unroll
+            for (int q = 0; q < N; ++q) w[q] = U[q * N + i];
+#pragma unroll 4
+            for (int k = 0; k < N; ++k) r[k] = dot_row(ZB + k * TP + j * TS, w);
+        }
     };
     int sweeps = 0;
     double relres = 1.0;
@@ -930,72 +1039,16 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
             }
         }
     }
-    int total_inner = 0, outer = 0;
+    int solves = 0, outer = 0;
     int status = relres <= prm.tol ? 0 : 1;
 #pragma unroll 1
     for (outer = 0; status != 0 && outer < prm.max_outer + prm.extra_outer; ++outer) {
-        const int max_inner = outer < prm.max_outer ? prm.max_inner : 4 * prm.max_inner;
-        // ---- FP32 Jacobi-PCG on K d = r64, d in x[]: z = D^-1 r, p = z
-        float rz = 0.f;
-#pragma unroll
-        for (int k = 0; k < N; ++k) {
-            x[k] = 0.f;
-            const float z = r[k] * DI[3 * k + di].y;
-            pr[k] = z;
-            if (active) sm.p[col + k * NN] = z;
-            rz += r[k] * z;
-        }
-        rz = block_sum_f4<NW>(rz, sm.red, 1);  // barrier also publishes p
-        const float want = fmaxf(prm.inner_tol, (float)(0.5 * prm.tol / relres));
-        const float stop2 = rz * want * want;
-        int it = 0;
-#pragma unroll 1
-        for (it = 0; it < max_inner && rz > stop2; ++it) {
-            float pq = 0.f;
-            if (active) {
-                float pb = 0.f, gzb = 0.f;
-#pragma unroll
-                for (int k = 0; k < N; ++k) {
-                    const int c = col + k * NN;
-                    const float4 tk = T32[k];
-                    const float dk = DI[3 * k + di].x;
-                    const float pa = k + 1 < N ? pr[k + 1] : 0.f;
-                    const float sxy = fxm * sm.p[c + oxm] + fxp * sm.p[c + oxp] +
-                                      fym * sm.p[c + oym] + fyp * sm.p[c + oyp];
-                    q[k] = dk * pr[k] - tk.x * sxy - tk.y * pa - gzb * pb;
-                    pq += pr[k] * q[k];
-                    pb = pr[k];
-                    gzb = tk.y;
-                }
-            } else {
-#pragma unroll
-                for (int k = 0; k < N; ++k) q[k] = 0.f;
-            }
-            pq = block_sum_f4<NW>(pq, sm.red, 0);
-            const float alpha = rz / pq;
-            float rz2 = 0.f;
-#pragma unroll
-            for (int k = 0; k < N; ++k) {
-                x[k] += alpha * pr[k];
-                r[k] -= alpha * q[k];
-                q[k] = r[k] * DI[3 * k + di].y;  // z
-                rz2 += r[k] * q[k];
-            }
-            rz2 = block_sum_f4<NW>(rz2, sm.red, 1);
-            const float beta = rz2 / rz;
-            rz = rz2;
-#pragma unroll
-            for (int k = 0; k < N; ++k) {
-                pr[k] = q[k] + beta * pr[k];
-                if (active) sm.p[col + k * NN] = pr[k];
-            }
-            __syncthreads();
-        }
-        total_inner += it;
+        direct_solve();
+        ++solves;
         // ---- y += d
         if (active) {
 #pragma unroll
-            for (int k = 0; k < N; ++k) Y[col + k * NN] += (double)x[k];
+            for (int k = 0; k < N; ++k) Y[col + k * NN] += (double)r[k];
         }
         __syncthreads();  // y of the neighbours visible
         relres = residual();
@@ -1004,7 +1057,7 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
     }
     st->status = status;
     st->escalated = outer > prm.max_outer;
-    st->iters = total_inner;
+    st->iters = solves;
     st->sweeps = sweeps;
     st->relres = relres;
     __syncthreads();
