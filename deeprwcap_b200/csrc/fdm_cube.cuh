@@ -327,10 +327,12 @@ struct EpsUniform {
 
 // ------------------------------------------------------------ right-hand side
 // Centre sources of ggft_solver.cpp:137-274 (unit source / centre gradient,
-// h = 2/N). Written by thread 0 into smem as (cell, value) pairs.
+// h = 2/N), into smem as (cell, value) pairs. Threads 0..7 each write one
+// entry (the shared sums are formed by each of them in the same order).
 template <int N, class E>
 DRWC_DEV void build_rhs(const E& eps, int code, const CubeSmem<N>& sm) {
-    if (threadIdx.x != 0) return;
+    const int t = threadIdx.x;
+    if (t >= kMaxRhs) return;
     const double h = 2.0 / N;
     const int c = N / 2;
     auto id = [](int i, int j, int k) { return i + j * N + k * N * N; };
@@ -339,15 +341,16 @@ DRWC_DEV void build_rhs(const E& eps, int code, const CubeSmem<N>& sm) {
     if (N % 2) {
         const int zzz = id(c, c, c);
         if (code == DRWC_GFT) {
-            sm.rhs_idx[0] = zzz; sm.rhs_val[0] = 1.0; n = 1;
+            if (t == 0) { sm.rhs_idx[0] = zzz; sm.rhs_val[0] = 1.0; }
+            n = 1;
         } else {
             const int stride = code == DRWC_WVTZ ? N * N : code == DRWC_WVTX ? 1 : N;
             const int pp = zzz + stride, mm = zzz - stride;
             const double d_plus = Ev(pp) + Ev(zzz);
             const double d_minus = -(Ev(zzz) + Ev(mm));
-            sm.rhs_idx[0] = pp;  sm.rhs_val[0] = Ev(pp) / d_plus / h;
-            sm.rhs_idx[1] = zzz; sm.rhs_val[1] = Ev(zzz) * (1. / d_plus + 1. / d_minus) / h;
-            sm.rhs_idx[2] = mm;  sm.rhs_val[2] = Ev(mm) / d_minus / h;
+            if (t == 0) { sm.rhs_idx[0] = pp;  sm.rhs_val[0] = Ev(pp) / d_plus / h; }
+            if (t == 1) { sm.rhs_idx[1] = zzz; sm.rhs_val[1] = Ev(zzz) * (1. / d_plus + 1. / d_minus) / h; }
+            if (t == 2) { sm.rhs_idx[2] = mm;  sm.rhs_val[2] = Ev(mm) / d_minus / h; }
             n = 3;
         }
     } else {
@@ -357,10 +360,8 @@ DRWC_DEV void build_rhs(const E& eps, int code, const CubeSmem<N>& sm) {
         const double dsum = Ev(zzz) + Ev(zmz) + Ev(zzm) + Ev(zmm) + Ev(mzz) + Ev(mmz) + Ev(mzm) + Ev(mmm);
         if (code == DRWC_GFT) {
             const int cells[8] = {zzz, mzz, zmz, zzm, mmz, mzm, zmm, mmm};
-            for (int t = 0; t < 8; ++t) {
-                sm.rhs_idx[t] = cells[t];
-                sm.rhs_val[t] = Ev(cells[t]) / dsum;
-            }
+            sm.rhs_idx[t] = cells[t];
+            sm.rhs_val[t] = Ev(cells[t]) / dsum;
         } else {
             int plus[4], minus[4];
             double d_minus;
@@ -377,16 +378,17 @@ DRWC_DEV void build_rhs(const E& eps, int code, const CubeSmem<N>& sm) {
                 minus[0] = zmz; minus[1] = mmz; minus[2] = zmm; minus[3] = mmm;
                 d_minus = -(Ev(zmz) + Ev(mmz) + Ev(zmm) + Ev(mmm));
             }
-            for (int t = 0; t < 4; ++t) {
+            if (t < 4) {
                 sm.rhs_idx[t] = plus[t];
                 sm.rhs_val[t] = Ev(plus[t]) / dsum / h * 2;
-                sm.rhs_idx[4 + t] = minus[t];
-                sm.rhs_val[4 + t] = Ev(minus[t]) * (1. / dsum + 1. / d_minus) / h * 2;
+            } else {
+                sm.rhs_idx[t] = minus[t - 4];
+                sm.rhs_val[t] = Ev(minus[t - 4]) * (1. / dsum + 1. / d_minus) / h * 2;
             }
         }
         n = 8;
     }
-    sm.flags[0] = n;
+    if (t == 0) sm.flags[0] = n;
 }
 
 // Permittivity the first-hop weight is scaled by (ggft_solver.cpp:649-671):
@@ -862,7 +864,13 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
     const double* __restrict__ warm = prm.warm[code & 3];
 
     // ---- set-up: plane tables, sine modes, right-hand side, y = the warm
-    //      start (or 0)
+    //      start (or 0). The warm-start values of this thread's column are
+    //      requested first, so their trip to L2 overlaps the table set-up.
+    double w0[N];
+    if (active && warm) {
+#pragma unroll
+        for (int k = 0; k < N; ++k) w0[k] = warm[col + k * NN];
+    }
     if (t < N) {
         const int k = t;
         double e, einv, gxy, gzu, gzd;
@@ -886,10 +894,7 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
     __syncthreads();  // tables written
     if (active) {
 #pragma unroll
-        for (int k = 0; k < N; ++k) {
-            const int c = col + k * NN;
-            Y[c] = warm ? warm[c] * T64[3 * k + 2].x : 0.0;
-        }
+        for (int k = 0; k < N; ++k) Y[col + k * NN] = warm ? w0[k] * T64[3 * k + 2].x : 0.0;
     }
     __syncthreads();
     double enorm2 = 0.0;
@@ -912,7 +917,7 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
     float r[N];
     // FP64 residual r64 = e - K y into r (FP32); returns ||r64|| / ||e||
     auto residual = [&]() -> double {
-        double rn2 = 0.0;
+        double rn2 = 0.0, rn2b = 0.0;
         double yb = 0.0;              // y of the cell below
         double yc = Y[col];
         double gzb = 0.0;             // g(k-1,k)
@@ -930,32 +935,41 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
                 for (int v = 0; v < nrhs; ++v)
                     if (sm.rhs_idx[v] == c) e_c = sm.rhs_val[v];
             const double r64 = e_c - (diag * yc - off);
-            if (active) rn2 += r64 * r64;
+            if (active) {
+                if (k & 1) rn2b += r64 * r64;
+                else rn2 += r64 * r64;
+            }
             r[k] = active ? (float)r64 : 0.f;
             yb = yc;
             yc = ya;
             gzb = a.y;
         }
-        rn2 = block_sum_d<NW>(rn2, sm.red, 0);
+        rn2 = block_sum_d<NW>(rn2 + rn2b, sm.red, 0);
         return sqrt(rn2) / enorm;
     };
     // one sum of a transform pass: row[0..N) . w[0..N) (w in registers)
+    // (four partial sums: short dependency chains)
     auto dot_row = [&](const float* row, const float (&w)[N]) -> float {
-        float acc = 0.f;
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
         if constexpr (N % 4 == 0) {
 #pragma unroll
             for (int q = 0; q < N / 4; ++q) {
                 const float4 v = reinterpret_cast<const float4*>(row)[q];
-                acc = fmaf(v.x, w[4 * q], acc);
-                acc = fmaf(v.y, w[4 * q + 1], acc);
-                acc = fmaf(v.z, w[4 * q + 2], acc);
-                acc = fmaf(v.w, w[4 * q + 3], acc);
+                a0 = fmaf(v.x, w[4 * q], a0);
+                a1 = fmaf(v.y, w[4 * q + 1], a1);
+                a2 = fmaf(v.z, w[4 * q + 2], a2);
+                a3 = fmaf(v.w, w[4 * q + 3], a3);
             }
         } else {
 #pragma unroll
-            for (int q = 0; q < N; ++q) acc = fmaf(row[q], w[q], acc);
+            for (int q = 0; q < N; ++q) {
+                if (q % 4 == 0) a0 = fmaf(row[q], w[q], a0);
+                else if (q % 4 == 1) a1 = fmaf(row[q], w[q], a1);
+                else if (q % 4 == 2) a2 = fmaf(row[q], w[q], a2);
+                else a3 = fmaf(row[q], w[q], a3);
+            }
         }
-        return acc;
+        return (a0 + a1) + (a2 + a3);
     };
     // FP32 direct solve K d = r (r in this thread's column): d into r
     auto direct_solve = [&]() {
@@ -990,7 +1004,7 @@ DRWC_SOLVE_ATTR void cube_solve_planar(const E eps, double* __restrict__ ys, int
                 const float4 tk = T32[k];
                 // sub- and super-diagonal -gz: den_k = b_k - gz_{k-1}^2 / den_{k-1}
                 const float den = fmaf(lam, tk.x, tk.z) + gzb * gprev;
-                const float inv = 1.f / den;
+                const float inv = __frcp_rn(den);
                 g[k] = -tk.y * inv;
                 fprev = (v[k] + gzb * fprev) * inv;
                 v[k] = fprev;
@@ -1079,6 +1093,32 @@ DRWC_DEV void for_each_panel(const E& eps, const double* __restrict__ ys, Put pu
             case 3: c = a + (N - 1) * N + bb * NN; break;         // y+
             case 4: c = a * N + bb * NN; break;                   // x-: (0,j,k)
             default: c = (N - 1) + a * N + bb * NN; break;        // x+
+        }
+        put(b, eps.e64(c) * ys[c]);
+    }
+}
+
+
+// The same values with panel b written by thread b / chunk (contiguous chunks
+// of chunk = ceil(6N^2 / NT) panels, the chunks cta_sample<NT> reads): a
+// thread can sample right after writing its own chunk, without a barrier.
+template <int N, int NT, class E, class Put>
+DRWC_DEV void for_each_panel_chunked(const E& eps, const double* __restrict__ ys, Put put) {
+    constexpr int NN = N * N;
+    constexpr int M = 6 * NN;
+    constexpr int CH = (M + NT - 1) / NT;
+    const int b0 = min((int)threadIdx.x * CH, M), b1 = min(b0 + CH, M);
+    for (int b = b0; b < b1; ++b) {
+        const int f = b / NN, tt = b % NN;
+        const int a = tt % N, bb = tt / N;
+        int c;
+        switch (f) {
+            case 0: c = a + bb * N; break;
+            case 1: c = a + bb * N + (N - 1) * NN; break;
+            case 2: c = a + bb * NN; break;
+            case 3: c = a + (N - 1) * N + bb * NN; break;
+            case 4: c = a * N + bb * NN; break;
+            default: c = (N - 1) + a * N + bb * NN; break;
         }
         put(b, eps.e64(c) * ys[c]);
     }

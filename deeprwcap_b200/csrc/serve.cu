@@ -124,6 +124,7 @@ struct SvArgs {
     // of the uniform-permittivity Green's function and their running sums
     int table;
     int fair;                           // claim policy (drwc_server_opts.fair_share)
+    int fdm_hops;                       // hops an FDM-only walk takes per step
     const double* tval[DRWC_SERVER_MAX_SIZES][4];
     const double* tcdf[DRWC_SERVER_MAX_SIZES][4];
 };
@@ -585,6 +586,7 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
     const unsigned count = A.cnt[4 * bucket + 2];
     unsigned* next_item = A.cnt + 4 * bucket + 3;
     __shared__ unsigned s_idx;
+    __shared__ int s_go;
     __shared__ int lm[N];  // layer material per z index (structures without blocks)
     __shared__ DevGeom gs;  // the current job's geometry header
     VoxScratch<N>& vs =   // separable voxeliser (structures with blocks)
@@ -616,87 +618,114 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
             loaded = j;
         }
         __syncthreads();
-        const EpsPalette E{mat, pal, palinv, pair64, pair32, P};
-        const long long w = A.st.walk[slot];
-        const int h = A.st.hops[slot];
-        const bool first = h == 0;
-        const int code = first ? A.st.code[slot] : DRWC_GFT;
-        const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
-        const double a = A.st.a[slot];
-        // a stratified cube (no dielectric block reaches it) goes to the
-        // per-plane solver
-        const int* lmc = nullptr;
-        if (gs.n_diel > 0) {
-            vox_prepare<N>(gs, c, a, tco, vs);
-            if (vs.nrel == 0) {
-                lmc = vs.lm;
+        // Once every walk of a job without a network (and without the uniform
+        // table) has been claimed, its remaining walks continue here for up to
+        // fdm_hops hops per step: otherwise each hop of such a tail walk waits
+        // a whole step (every other slot's hop), and the job's completion
+        // waits for its longest walks.
+        for (int hh = 0;; ++hh) {
+            const EpsPalette E{mat, pal, palinv, pair64, pair32, P};
+            const long long w = A.st.walk[slot];
+            const int h = A.st.hops[slot];
+            const bool first = h == 0;
+            const int code = first ? A.st.code[slot] : DRWC_GFT;
+            const double c[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
+            const double a = A.st.a[slot];
+            // a stratified cube (no dielectric block reaches it) goes to the
+            // per-plane solver
+            const int* lmc = nullptr;
+            if (gs.n_diel > 0) {
+                vox_prepare<N>(gs, c, a, tco, vs);
+                if (vs.nrel == 0) {
+                    lmc = vs.lm;
+                } else {
+                    for (int v = threadIdx.x; v < D::NNN; v += blockDim.x)
+                        mat[v] = (uint8_t)vox_material<N>(gs, vs, c, a, tco, v % N, (v / N) % N,
+                                                          v / D::NN, 0);
+                }
             } else {
-                for (int v = threadIdx.x; v < D::NNN; v += blockDim.x)
-                    mat[v] = (uint8_t)vox_material<N>(gs, vs, c, a, tco, v % N, (v / N) % N,
-                                                      v / D::NN, 0);
+                plane_layers<N>(gs, c, a, tco, lm);
+                lmc = lm;
             }
-        } else {
-            plane_layers<N>(gs, c, a, tco, lm);
-            lmc = lm;
-        }
-        __syncthreads();
-        FdmStats st;
-        double* wv = reinterpret_cast<double*>(sm.stage());
-        const EpsPlanar<N> EP{lmc, pal, palinv, pair64, pair32, P};
-        if (lmc) {
-            cube_solve_planar<N>(EP, ys, code, J.W.prm, &st);
-            for_each_panel<N>(EP, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
-        } else {
-            cube_solve<N>(E, ys, ss, code, J.W.prm, &st);
-            for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
-        }
-        __syncthreads();
-        if ((kind & 1) && !first) {
-            // audit: KL(FDM || network) over the panels
-            const float* o = A.O[bucket] + (size_t)(kind >> 1) * A.out_row[bucket];
-            const double ls = block_lse<D::NW>(o, M, sm.red);
             __syncthreads();
-            double kl = 0.0;
-            for (int q = threadIdx.x; q < M; q += blockDim.x) {
-                const double gq = fmax(wv[q], 0.0);
-                if (gq > 0.0) kl += gq * (log(gq) - ((double)o[q] - ls));
+            FdmStats st;
+            double* wv = reinterpret_cast<double*>(sm.stage());
+            const EpsPlanar<N> EP{lmc, pal, palinv, pair64, pair32, P};
+            if (lmc) {
+                cube_solve_planar<N>(EP, ys, code, J.W.prm, &st);
+                for_each_panel<N>(EP, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+            } else {
+                cube_solve<N>(E, ys, ss, code, J.W.prm, &st);
+                for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
             }
-            kl = block_sum_d<D::NW>(kl, sm.red, 1);
+            __syncthreads();
+            if ((kind & 1) && !first) {
+                // audit: KL(FDM || network) over the panels
+                const float* o = A.O[bucket] + (size_t)(kind >> 1) * A.out_row[bucket];
+                const double ls = block_lse<D::NW>(o, M, sm.red);
+                __syncthreads();
+                double kl = 0.0;
+                for (int q = threadIdx.x; q < M; q += blockDim.x) {
+                    const double gq = fmax(wv[q], 0.0);
+                    if (gq > 0.0) kl += gq * (log(gq) - ((double)o[q] - ls));
+                }
+                kl = block_sum_d<D::NW>(kl, sm.red, 1);
+                if (threadIdx.x == 0) {
+                    atomicAdd(A.audit_kl + 0, kl);
+                    atomicAdd(A.audit_kl + 1, 1.0);
+                }
+                __syncthreads();
+            }
+            const double2 u2 = first ? philox_uniform2(J.W.seed, (uint64_t)w, 0, 1)
+                                     : philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 0);
+            const double ud = first ? u2.y : u2.x;
+            double tot = 0.0;
+            const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
             if (threadIdx.x == 0) {
-                atomicAdd(A.audit_kl + 0, kl);
-                atomicAdd(A.audit_kl + 1, 1.0);
+                if (b < 0 || st.status != 0) {
+                    // no transition possible, or the solve stayed unconverged
+                    // after escalation: the walk is lost
+                    sv_finish(A, slot, -1);
+                } else {
+                    if (first)
+                        A.st.omega[slot] = first_hop_weight(
+                            J.G, A.st.sgn[slot],
+                            lmc ? center_diel<N>(EP, code) : center_diel<N>(E, code), tot, wv[b], a);
+                    double loc[3];
+                    locate_f64(N, b, loc);
+                    A.st.px[slot] = dadd(A.st.px[slot], dmul(a, loc[0]));
+                    A.st.py[slot] = dadd(A.st.py[slot], dmul(a, loc[1]));
+                    A.st.pz[slot] = dadd(A.st.pz[slot], dmul(a, loc[2]));
+                    A.st.hops[slot] = h + 1;
+                }
+                my_hops += 1;
+                my_iters += (unsigned long long)st.iters;
+                my_sweeps += (unsigned long long)st.sweeps;
+                my_esc += (unsigned long long)st.escalated;
+                my_fail += st.status == 1;
             }
             __syncthreads();
-        }
-        const double2 u2 = first ? philox_uniform2(J.W.seed, (uint64_t)w, 0, 1)
-                                 : philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 0);
-        const double ud = first ? u2.y : u2.x;
-        double tot = 0.0;
-        const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
-        if (threadIdx.x == 0) {
-            if (b < 0 || st.status != 0) {
-                // no transition possible, or the solve stayed unconverged
-                // after escalation: the walk is lost
-                sv_finish(A, slot, -1);
-            } else {
-                if (first)
-                    A.st.omega[slot] = first_hop_weight(
-                        J.G, A.st.sgn[slot],
-                        lmc ? center_diel<N>(EP, code) : center_diel<N>(E, code), tot, wv[b], a);
-                double loc[3];
-                locate_f64(N, b, loc);
-                A.st.px[slot] = dadd(A.st.px[slot], dmul(a, loc[0]));
-                A.st.py[slot] = dadd(A.st.py[slot], dmul(a, loc[1]));
-                A.st.pz[slot] = dadd(A.st.pz[slot], dmul(a, loc[2]));
-                A.st.hops[slot] = h + 1;
+            if (kind != 0 || J.use_net || A.table || hh + 1 >= A.fdm_hops) break;
+            if (*(volatile unsigned long long*)&A.ctr[j].next < (unsigned long long)J.total) break;
+            if (A.st.mode[slot] == 0) break;  // the walk finished on this hop
+            // the next hop's cube: nearest conductor, absorption (the prepare
+            // kernel's geometry step for this slot)
+            if (threadIdx.x < 32) {
+                const double r[3] = {A.st.px[slot], A.st.py[slot], A.st.pz[slot]};
+                double d;
+                int net;
+                nearest(gs, r, &d, &net);
+                if (threadIdx.x == 0) {
+                    int go = 0;
+                    if (d < J.W.stop) sv_finish(A, slot, net);
+                    else if (A.st.hops[slot] >= J.W.max_hops) sv_finish(A, slot, -1);
+                    else { A.st.a[slot] = d; go = 1; }
+                    s_go = go;
+                }
             }
-            my_hops += 1;
-            my_iters += (unsigned long long)st.iters;
-            my_sweeps += (unsigned long long)st.sweeps;
-            my_esc += (unsigned long long)st.escalated;
-            my_fail += st.status == 1;
+            __syncthreads();
+            if (!s_go) break;
         }
-        __syncthreads();
     }
     if (threadIdx.x == 0 && (my_esc || my_fail)) {
         atomicAdd(A.stats + SV_FDM_ESCALATED, my_esc);
@@ -1456,6 +1485,7 @@ static int sv_alloc(drwc_server* v) {
     }
     A.table = v->o.uniform_table;
     A.fair = v->o.fair_share;
+    A.fdm_hops = v->o.fdm_hops;
     for (int b = 0; b < v->o.n_sizes; ++b) {
         v->fdm_sy[b] = (double*)(B + o_sy[b]);
         v->fdm_ss[b] = (float*)(B + o_ss[b]);
@@ -1508,7 +1538,7 @@ extern "C" {
 DRWC_API void drwc_server_opts_default(drwc_server_opts* o) {
     if (!o) return;
     std::memset(o, 0, sizeof(*o));
-    o->slots = 65536;
+    o->slots = 0;
     o->max_jobs = 32;
     o->hbm_budget = 1LL << 30;
     o->n_sizes = 3;
@@ -1523,6 +1553,7 @@ DRWC_API void drwc_server_opts_default(drwc_server_opts* o) {
     o->timing = 0;
     o->uniform_table = 0;
     o->fair_share = 0;
+    o->fdm_hops = 0;
 }
 
 DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts,
@@ -1532,12 +1563,12 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts,
     drwc_server_opts o;
     drwc_server_opts_default(&o);
     if (opts) o = *opts;
-    if (o.slots < 1 || o.slots > (1 << 22) || o.max_jobs < 1 || o.max_jobs > kSvMaxJobs ||
+    if (o.slots < 0 || o.slots > (1 << 22) || o.max_jobs < 1 || o.max_jobs > kSvMaxJobs ||
         o.hbm_budget < 4096 || o.n_sizes < 1 || o.n_sizes > DRWC_SERVER_MAX_SIZES ||
         o.steps_per_graph < 1 || o.steps_per_graph > kSvMaxSteps || o.max_materials < 1 ||
         o.max_materials > kMaxMaterials || o.max_nets < 1 || o.max_nets > DRWC_MAX_NETS ||
         !(o.audit_frac >= 0.f && o.audit_frac <= 1.f) || o.uniform_table < 0 || o.uniform_table > 1 ||
-        o.fair_share < 0 || o.fair_share > 1)
+        o.fair_share < 0 || o.fair_share > 1 || o.fdm_hops < 0 || o.fdm_hops > 64)
         return DRWC_ERR_INVALID;
     if (n_nets < 0 || n_nets > DRWC_SERVER_MAX_SIZES || (n_nets > 0 && !nets))
         return DRWC_ERR_INVALID;
@@ -1561,6 +1592,9 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts,
         v->bnet[b] = net;
         v->any_net = true;
     }
+    if (v->o.slots == 0) v->o.slots = 65536;
+    if (v->o.fdm_hops == 0) v->o.fdm_hops = 64;
+    o = v->o;
     {
         std::lock_guard<std::mutex> lock(ctx->mu);
         DRWC_CUDA_TRY(cudaSetDevice(ctx->device));

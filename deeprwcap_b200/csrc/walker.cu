@@ -148,14 +148,15 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
             FdmStats st;
             double* wv = reinterpret_cast<double*>(sm.stage());
             const EpsPlanar<N> EP{lm, pal, palinv, pair64, pair32, P};
+            // each thread writes the panel chunk it samples from (no barrier
+            // before the draw; cta_sample's own barriers order the rest)
             if (lm) {
                 cube_solve_planar<N>(EP, ys, code, W.prm, &st);
-                for_each_panel<N>(EP, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+                for_each_panel_chunked<N, D::NT>(EP, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
             } else {
                 cube_solve<N>(E, ys, ss, code, W.prm, &st);
-                for_each_panel<N>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
+                for_each_panel_chunked<N, D::NT>(E, cube_y<N>(ys), [&](int b, double v) { wv[b] = v; });
             }
-            __syncthreads();
             const double2 u = first ? philox_uniform2(W.seed, w, 0, 1)
                                     : philox_uniform2(W.seed, w, (uint32_t)S.hops, 0);
             const double ud = first ? u.y : u.x;

@@ -32,7 +32,8 @@ def main() -> None:
     ap.add_argument("--net-sizes", default="16",
                     help="with --net random: the cube resolutions to build networks for, e.g. 16,21,23")
     ap.add_argument("--uniform-table", type=int, default=0)
-    ap.add_argument("--slots", type=int, default=65536)
+    ap.add_argument("--slots", type=int, default=0,
+                    help="walks in flight (0: 65536)")
     ap.add_argument("--stream", type=int, default=0)
     ap.add_argument("--walks-max", type=float, default=1e6)
     a = ap.parse_args()

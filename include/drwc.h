@@ -374,7 +374,7 @@ DRWC_API int drwc_frw_walks_learned(drwc_ctx* ctx, const drwc_structure* s,
 typedef struct drwc_server drwc_server;
 #define DRWC_SERVER_MAX_SIZES 4
 typedef struct drwc_server_opts {
-    int32_t slots;            /* walks in flight over all jobs (default 65536) */
+    int32_t slots;            /* walks in flight over all jobs; 0 (default) = 65536 */
     int32_t max_jobs;         /* job-table entries, <= 64 (default 32) */
     int64_t hbm_budget;       /* bytes of the job arena (default 1 GiB) */
     int32_t n_sizes;          /* cube resolutions served (default 3) */
@@ -392,7 +392,12 @@ typedef struct drwc_server_opts {
     int32_t fair_share;       /* 0: free slots go to the oldest running job first (first in,
                                  first out, later jobs fill what it leaves); 1: slots rotate
                                  over the running jobs (an even share) */
-    int32_t reserved_;
+    int32_t fdm_hops;         /* once all walks of a job without a network have been
+                                 claimed (uniform_table = 0), each of its remaining walks
+                                 takes up to this many hops per step inside the FDM solve,
+                                 1..64; 0 (default) = 64. Otherwise each hop of such a
+                                 tail walk waits a whole step, and the job's completion
+                                 waits for its longest walks */
 } drwc_server_opts;
 DRWC_API void drwc_server_opts_default(drwc_server_opts* o);
 /* nets (n_nets of them, each of a different served resolution; none: every
