@@ -89,7 +89,7 @@ class JobParams(C.Structure):
     _fields_ = [("master", C.c_int32), ("N", C.c_int32), ("gauss_offset", C.c_double),
                 ("stop_dist", C.c_double), ("p_tol", C.c_double), ("c_tol", C.c_double),
                 ("c_ratio", C.c_double), ("min_walks", C.c_int64), ("max_walks", C.c_int64),
-                ("batch_walks", C.c_int64), ("max_hops", C.c_int32), ("pad_", C.c_int32),
+                ("batch_walks", C.c_int64), ("max_hops", C.c_int32), ("gauss_surface", C.c_int32),
                 ("seed", C.c_uint64), ("fdm", FdmOpts)]
 
 

@@ -10,7 +10,7 @@ testcases/cap3d/*.cap3d); lengths in um:
 
     <window> v1(x,y,z) v2(x,y,z)        the simulation box: the grounded enclosure
     <plate_medium> diel, z_top           stratified dielectric, stacked by z_top
-    <medium> <block>...</block> diel     dielectric blocks (first listed wins)
+    <medium> <block>...</block> diel     dielectric blocks (a later one overrides an earlier)
     <conductor> name <block>...</block>  conductors; a "<k>__" name prefix numbers
                                          the pieces of one net, and conductors
                                          of the same name are one net
@@ -172,12 +172,43 @@ def parse(source) -> Cap3d:
     return cap
 
 
-def to_structure(c: Cap3d) -> W.StructureSpec:
+def dump_case(c: Cap3d, ref: dict | None = None) -> str:
+    """The parsed case (and a reference result, {master: {net: F}}) as JSON
+    text; ``load_case`` reads it back."""
+    def boxes(bl):
+        return [list(map(float, b)) for b in bl]
+    return json.dumps({
+        "window_lo": list(map(float, c.window_lo)), "window_hi": list(map(float, c.window_hi)),
+        "plates": [[n, float(e), float(z)] for n, e, z in c.plates],
+        "media": [[n, float(e), boxes(bl)] for n, e, bl in c.media],
+        "conductors": [[n, boxes(bl)] for n, bl in c.conductors],
+        "masters": list(c.masters), "c_ratio": c.c_ratio, "ref": ref})
+
+
+def load_case(text: str) -> tuple[Cap3d, dict | None]:
+    d = json.loads(text)
+    c = Cap3d(np.asarray(d["window_lo"]), np.asarray(d["window_hi"]),
+              [tuple(p) for p in d["plates"]], [(n, e, bl) for n, e, bl in d["media"]],
+              [(n, bl) for n, bl in d["conductors"]], list(d["masters"]), d["c_ratio"])
+    return c, d["ref"]
+
+
+# Which of several overlapping media blocks holds a point: the one listed
+# last ("last": a later <medium> is painted over the earlier ones, as the
+# reference's cases nest conformal shells outer to inner), the one listed
+# first ("first"), or the smallest ("smallest"). Scored against QuickCap on
+# the reference's cases, "last" is the format's rule (case7: 3.2 % error,
+# 37 % with "first").
+MEDIA_ORDER = "last"
+
+
+def to_structure(c: Cap3d, media_order: str | None = None) -> W.StructureSpec:
     """The engine structure: conductor boxes with net ids in order of the
     nets' first appearance (pieces of one net merged, see ``net_of``),
     plate media as layers (layer l from the previous z_top, the first from
-    the window bottom), media blocks as dielectric blocks, the window as the
-    grounded enclosure."""
+    the window bottom), media blocks as dielectric blocks ordered so that
+    the engine's first containing block is the one ``media_order`` (default
+    MEDIA_ORDER) picks, the window as the grounded enclosure."""
     boxes, nets = [], []
     ids = {n: i for i, n in enumerate(c.net_names)}
     for name, bl in c.conductors:
@@ -190,6 +221,11 @@ def to_structure(c: Cap3d) -> W.StructureSpec:
     else:
         zlo, eps = [float(c.window_lo[2])], [1.0]
     diel = [[*b, e] for _, e, bl in c.media for b in bl]
+    order = media_order or MEDIA_ORDER
+    if order == "last":
+        diel = diel[::-1]
+    elif order == "smallest":
+        diel = sorted(diel, key=lambda d: (d[3] - d[0]) * (d[4] - d[1]) * (d[5] - d[2]))
     return W.StructureSpec(np.asarray(boxes, dtype=np.float64).reshape(-1, 6),
                            np.asarray(nets, dtype=np.int32), len(ids),
                            np.asarray(zlo, dtype=np.float64), np.asarray(eps, dtype=np.float64),
@@ -210,19 +246,47 @@ def clearance(s: W.StructureSpec, master: int) -> float:
     return gap
 
 
+def box_clearance(s: W.StructureSpec, master: int) -> float:
+    """L-infinity gap between the master's own boxes and the nearest other
+    conductor box or window wall."""
+    mb = s.boxes[s.nets == master]
+    gap = min(float((mb[:, :3] - s.encl_lo).min()), float((s.encl_hi - mb[:, 3:]).min()))
+    other = s.boxes[s.nets != master]
+    if len(other):
+        sep = np.maximum(other[None, :, :3] - mb[:, None, 3:],
+                         mb[:, None, :3] - other[None, :, 3:]).max(axis=2)
+        gap = min(gap, float(sep.min()))
+    return gap
+
+
 def job_params(s: W.StructureSpec, master: int, N: int = 16, p_tol: float = 0.01,
                c_tol: float = 0.01, c_ratio: float = 0.95, offset: float | None = None,
                stop_rel: float = 1e-4, seed: int = 1, max_walks: int = 10_000_000,
                batch_walks: int = 1 << 16):
+    """Job parameters for one master. The Gaussian surface is the master's
+    bounding box grown by half its clearance when that box cuts no other
+    net; otherwise (a master of many pieces wrapped around other nets) the
+    outer boundary of the master's boxes, each grown by half its own gap to
+    the other nets (gauss_surface = 1, the engine sizes each box's offset;
+    gauss_offset is then the largest offset allowed, stop_dist scales with
+    the smallest)."""
     gap = clearance(s, master)
+    mode = 0
+    stop_ref = None
     if not gap > 0:
-        raise ValueError("the master's bounding box touches another conductor; no Gaussian "
-                         "surface around it avoids the other nets")
+        gap = box_clearance(s, master)
+        mode = 1
+        if not gap > 0:
+            raise ValueError("the master's boxes touch another conductor; no Gaussian "
+                             "surface around them avoids the other nets")
+        stop_ref = 0.5 * gap
+        gap = float(np.max(s.encl_hi - s.encl_lo))  # no cap below each box's own half gap
     off = 0.5 * gap if offset is None else float(offset)
+    stop = stop_rel * (off if stop_ref is None else min(off, stop_ref))
     return W.job_params_plain(N=N, master=master, seed=seed, p_tol=p_tol, c_tol=c_tol,
-                              c_ratio=c_ratio, gauss_offset=off, stop_dist=stop_rel * off,
+                              c_ratio=c_ratio, gauss_offset=off, stop_dist=stop,
                               min_walks=min(batch_walks, max_walks), max_walks=max_walks,
-                              batch_walks=batch_walks, tol=1e-8)
+                              batch_walks=batch_walks, tol=1e-8, gauss_surface=mode)
 
 
 def extract(c: Cap3d, master: str | None = None, ctx=None, **kw) -> dict:
@@ -249,7 +313,8 @@ def extract(c: Cap3d, master: str | None = None, ctx=None, **kw) -> dict:
     return {"master": name, "row_F": row, "cap_fF": [float(v) for v in r.cap[:len(names)]],
             "stderr_fF": [float(v) for v in r.stderr[:len(names)]], "walks": int(r.walks),
             "hops": int(r.hops), "converged": bool(r.converged), "seconds": secs,
-            "gauss_offset_um": p.gauss_offset, "stop_dist_um": p.stop_dist}
+            "gauss_offset_um": p.gauss_offset, "stop_dist_um": p.stop_dist,
+            "gauss_surface": int(p.gauss_surface), "lost": int(r.lost)}
 
 
 def write_dspf(results, path) -> None:

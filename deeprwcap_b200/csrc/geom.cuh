@@ -8,6 +8,7 @@
 #pragma once
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -46,6 +47,11 @@ struct DevGeom {
     double gmin_cell;
     const int* gstart;      // ncells + 1
     const int* gitems;
+    // Gaussian surface made of rectangles (the union of the master's grown
+    // boxes): n_grect x 9 doubles {axis, side, x, u0, u1, v0, v1, cumulative
+    // sampling mass, 1 / sampling density factor}; none: the Gauss box
+    const double* grect;
+    int n_grect;
 };
 
 struct Gauss {
@@ -303,11 +309,31 @@ DRWC_DEV void reduce_entry(int e, int n_entries, long long nw, const int32_t* __
 // Start point of walk w on the Gaussian surface (Philox counter (w, 0, 0..1)):
 // a face chosen by area, a uniform point on it; the outward sign of that
 // face and the solver code of its normal (WVTX/Y/Z) for the first hop.
-DRWC_DEV void walk_start_point(const Gauss& G, uint64_t seed, uint64_t w, double r[3],
-                               double* sgn_out, int* code) {
+DRWC_DEV void walk_start_point(const Gauss& G, const DevGeom& g, uint64_t seed, uint64_t w,
+                               double r[3], double* sgn_out, int* code) {
     const double2 u = philox_uniform2(seed, w, 0, 0);
     const double2 v = philox_uniform2(seed, w, 0, 1);
     const double target = dmul(u.x, G.total);
+    if (g.n_grect > 0) {
+        // the first rectangle whose cumulative area exceeds the target
+        int lo = 0, hi = g.n_grect - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (g.grect[9 * mid + 7] > target) hi = mid;
+            else lo = mid + 1;
+        }
+        const double* R = g.grect + 9 * lo;
+        const int axis = (int)R[0], side = (int)R[1];
+        const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
+        r[t0] = dadd(R[3], dmul(u.y, dsub(R[4], R[3])));
+        r[t1] = dadd(R[5], dmul(v.x, dsub(R[6], R[5])));
+        r[axis] = R[2];
+        // the outward sign, times the importance ratio of this rectangle
+        // (first_hop_weight multiplies by G.total, the total sampling mass)
+        *sgn_out = side ? R[8] : -R[8];
+        *code = axis == 0 ? DRWC_WVTX : axis == 1 ? DRWC_WVTY : DRWC_WVTZ;
+        return;
+    }
     double run = 0.0;
     int f = 5;
     for (int q = 0; q < 6; ++q) {
@@ -577,14 +603,14 @@ DRWC_DEV double block_lse(const float* o, int M, double* red) {
 }
 
 struct HostGeom {
-    std::vector<double> box, zlo, diel, pal, pair64;
+    std::vector<double> box, zlo, diel, pal, pair64, grect;
     std::vector<float> pair32;
     std::vector<int> net, gstart, gitems, lmat, dmat;
     DevGeom dev{};
     void* dbuf = nullptr;
     std::vector<unsigned char> blob;  // every device array, 256-byte aligned, in one block
     size_t o_box = 0, o_net = 0, o_zlo = 0, o_lmat = 0, o_dmat = 0, o_pal = 0, o_p64 = 0,
-           o_p32 = 0, o_diel = 0, o_gs = 0, o_gi = 0;
+           o_p32 = 0, o_diel = 0, o_gs = 0, o_gi = 0, o_gr = 0;
 };
 
 inline int validate(const drwc_structure* s) {
@@ -715,6 +741,7 @@ inline int pack_geom(const drwc_structure* s, HostGeom* h) {
     h->o_diel = take(std::max<size_t>(1, h->diel.size()) * 8);
     h->o_gs = take(h->gstart.size() * 4);
     h->o_gi = take(h->gitems.size() * 4);
+    h->o_gr = take(std::max<size_t>(1, h->grect.size()) * 8);
     std::vector<unsigned char>& hb = h->blob;
     hb.assign(off, 0);
     std::memcpy(hb.data() + h->o_box, h->box.data(), h->box.size() * 8);
@@ -728,7 +755,9 @@ inline int pack_geom(const drwc_structure* s, HostGeom* h) {
     if (!h->diel.empty()) std::memcpy(hb.data() + h->o_diel, h->diel.data(), h->diel.size() * 8);
     std::memcpy(hb.data() + h->o_gs, h->gstart.data(), h->gstart.size() * 4);
     std::memcpy(hb.data() + h->o_gi, h->gitems.data(), h->gitems.size() * 4);
+    if (!h->grect.empty()) std::memcpy(hb.data() + h->o_gr, h->grect.data(), h->grect.size() * 8);
     DevGeom& g = h->dev;
+    g.n_grect = (int)(h->grect.size() / 9);
     g.n_boxes = nb;
     g.n_nets = s->n_nets;
     g.n_layers = s->n_layers;
@@ -759,6 +788,7 @@ inline void bind_geom(HostGeom* h, void* d) {
     g.diel = (const double*)(base + h->o_diel);
     g.gstart = (const int*)(base + h->o_gs);
     g.gitems = (const int*)(base + h->o_gi);
+    g.grect = (const double*)(base + h->o_gr);
     h->dbuf = d;
 }
 
@@ -773,6 +803,129 @@ inline int upload_geom(drwc_ctx* ctx, const drwc_structure* s, HostGeom* h) {
     DRWC_CUDA_TRY(cudaMemcpyAsync(d, h->blob.data(), h->blob.size(), cudaMemcpyHostToDevice,
                                   ctx->stream));
     bind_geom(h, d);
+    return DRWC_OK;
+}
+
+// Gaussian surface of gauss_surface = 1: the outer boundary of the union of
+// the master's boxes, each grown by min(gauss_offset, half its L-infinity
+// clearance to the other nets' boxes and the enclosure), as rectangles on the faces
+// of the grown boxes. A face point belongs to the surface when no grown box
+// covers the space just outside it, and, among the coplanar faces of the same
+// orientation that contain it, to the lowest box. Each face is cut along the
+// other boxes' edges that cross it, and every cell of that grid is kept or
+// dropped whole (tested at its centre). Rectangles come box by box, faces in
+// the Gauss box order (z-, z+, y-, y+, x-, x+), so a master of one box gives
+// the six faces of the Gauss box with the same areas and running sums.
+inline int gauss_union(const drwc_structure* s, const drwc_job_params* p, Gauss* G,
+                       std::vector<double>* rects) {
+    std::vector<std::array<double, 6>> B;
+    std::vector<double> offs;
+    for (int b = 0; b < s->n_boxes; ++b) {
+        if (s->boxes[b].net != p->master) continue;
+        // this box's clearance: walls and every other net's box (L-infinity)
+        const drwc_box& M = s->boxes[b];
+        double gap = INFINITY;
+        for (int a = 0; a < 3; ++a)
+            gap = std::min(gap, std::min(M.lo[a] - s->encl_lo[a], s->encl_hi[a] - M.hi[a]));
+        for (int q = 0; q < s->n_boxes; ++q) {
+            if (s->boxes[q].net == p->master) continue;
+            double sep = -INFINITY;
+            for (int a = 0; a < 3; ++a)
+                sep = std::max(sep, std::max(s->boxes[q].lo[a] - M.hi[a], M.lo[a] - s->boxes[q].hi[a]));
+            gap = std::min(gap, sep);
+        }
+        if (!(gap > 0)) return DRWC_ERR_GEOMETRY;
+        const double off = std::min(p->gauss_offset, 0.5 * gap);
+        offs.push_back(off);
+        std::array<double, 6> g;
+        for (int a = 0; a < 3; ++a) {
+            volatile double lo = s->boxes[b].lo[a] - off;
+            volatile double hi = s->boxes[b].hi[a] + off;
+            g[a] = lo;
+            g[3 + a] = hi;
+            if (lo < s->encl_lo[a] || hi > s->encl_hi[a]) return DRWC_ERR_GEOMETRY;
+        }
+        B.push_back(g);
+    }
+    if (B.empty()) return DRWC_ERR_INVALID;
+    // no grown box may reach another net's box
+    for (int b = 0; b < s->n_boxes; ++b) {
+        if (s->boxes[b].net == p->master) continue;
+        for (const auto& g : B) {
+            bool overlap = true;
+            for (int a = 0; a < 3; ++a)
+                overlap &= s->boxes[b].lo[a] < g[3 + a] && s->boxes[b].hi[a] > g[a];
+            if (overlap) return DRWC_ERR_GEOMETRY;
+        }
+    }
+    for (int a = 0; a < 3; ++a) {  // the Gauss box: the union's bounds
+        G->lo[a] = INFINITY;
+        G->hi[a] = -INFINITY;
+        for (const auto& g : B) {
+            G->lo[a] = std::min(G->lo[a], g[a]);
+            G->hi[a] = std::max(G->hi[a], g[3 + a]);
+        }
+    }
+    rects->clear();
+    const int K = (int)B.size();
+    // Importance sampling: the first-hop weight grows as 1 / (distance to the
+    // master) and a start point on box k's face lies off_k from it, so face
+    // area of box k is sampled with density factor off_max / off_k (1 when
+    // all offsets agree) and the weight carries the inverse factor.
+    const double off_max = *std::max_element(offs.begin(), offs.end());
+    volatile double run = 0.0;
+    for (int k = 0; k < K; ++k) {
+        for (int f = 0; f < 6; ++f) {
+            const int axis = f < 2 ? 2 : f < 4 ? 1 : 0, side = f & 1;
+            const int t0 = axis == 0 ? 1 : 0, t1 = axis == 2 ? 1 : 2;
+            const double x = side ? B[k][3 + axis] : B[k][axis];
+            const double u0 = B[k][t0], u1 = B[k][3 + t0], v0 = B[k][t1], v1 = B[k][3 + t1];
+            // the other boxes that touch the face's plane region
+            std::vector<int> near;
+            std::vector<double> us{u0, u1}, vs{v0, v1};
+            for (int q = 0; q < K; ++q) {
+                if (q == k) continue;
+                if (!(B[q][axis] <= x && B[q][3 + axis] >= x)) continue;
+                if (!(B[q][t0] < u1 && B[q][3 + t0] > u0 && B[q][t1] < v1 && B[q][3 + t1] > v0))
+                    continue;
+                near.push_back(q);
+                for (double e : {B[q][t0], B[q][3 + t0]}) if (e > u0 && e < u1) us.push_back(e);
+                for (double e : {B[q][t1], B[q][3 + t1]}) if (e > v0 && e < v1) vs.push_back(e);
+            }
+            std::sort(us.begin(), us.end());
+            us.erase(std::unique(us.begin(), us.end()), us.end());
+            std::sort(vs.begin(), vs.end());
+            vs.erase(std::unique(vs.begin(), vs.end()), vs.end());
+            for (size_t iu = 0; iu + 1 < us.size(); ++iu) {
+                for (size_t iv = 0; iv + 1 < vs.size(); ++iv) {
+                    const double pu = 0.5 * (us[iu] + us[iu + 1]), pv = 0.5 * (vs[iv] + vs[iv + 1]);
+                    bool keep = true;
+                    for (int q : near) {
+                        const bool inside_t = B[q][t0] < pu && pu < B[q][3 + t0] &&
+                                              B[q][t1] < pv && pv < B[q][3 + t1];
+                        if (!inside_t) continue;
+                        // covers the space just outside the face
+                        const bool cover = side ? (B[q][axis] <= x && x < B[q][3 + axis])
+                                                : (B[q][axis] < x && x <= B[q][3 + axis]);
+                        // a lower coplanar face of the same orientation owns it
+                        const bool owner = q < k && (side ? B[q][3 + axis] == x : B[q][axis] == x);
+                        if (cover || owner) { keep = false; break; }
+                    }
+                    if (!keep) continue;
+                    volatile double du = us[iu + 1] - us[iu], dv = vs[iv + 1] - vs[iv];
+                    volatile double ar = du * dv;
+                    const double fk = offs[k] == off_max ? 1.0 : off_max / offs[k];
+                    volatile double mass = fk == 1.0 ? (double)ar : ar * fk;
+                    run = run + mass;
+                    rects->insert(rects->end(), {(double)axis, (double)side, x, us[iu], us[iu + 1],
+                                                 vs[iv], vs[iv + 1], (double)run, 1.0 / fk});
+                }
+            }
+        }
+    }
+    if (rects->empty()) return DRWC_ERR_GEOMETRY;
+    for (int f = 0; f < 6; ++f) G->area[f] = 0.0;
+    G->total = run;
     return DRWC_OK;
 }
 
@@ -827,7 +980,10 @@ inline int prepare(drwc_ctx* ctx, const drwc_structure* s, const drwc_job_params
     if (!p || !n_supported(p->N) || p->master < 0 || p->master >= s->n_nets ||
         !(p->gauss_offset > 0) || !(p->stop_dist > 0) || p->max_hops < 1)
         return DRWC_ERR_INVALID;
-    rc = gauss_build(s, p, G);
+    hg->grect.clear();
+    if (p->gauss_surface == 1) rc = gauss_union(s, p, G, &hg->grect);
+    else if (p->gauss_surface == 0) rc = gauss_build(s, p, G);
+    else rc = DRWC_ERR_INVALID;
     if (rc) return rc;
     rc = pack_geom(s, hg);  // the caller places the blob on the device
     if (rc) return rc;

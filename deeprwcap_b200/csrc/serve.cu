@@ -154,7 +154,7 @@ DRWC_DEV void sv_start(const SvArgs& A, int slot, int j, long long w) {
     const SvJob& J = A.jobs[j];
     double r[3], sgn;
     int code;
-    walk_start_point(J.G, J.W.seed, (uint64_t)w, r, &sgn, &code);
+    walk_start_point(J.G, J.g, J.W.seed, (uint64_t)w, r, &sgn, &code);
     A.st.px[slot] = r[0]; A.st.py[slot] = r[1]; A.st.pz[slot] = r[2];
     A.st.sgn[slot] = sgn;
     A.st.code[slot] = code;

@@ -90,7 +90,7 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
         const uint64_t w = (uint64_t)(walk0 + idx);
         // ---- start point on the Gaussian surface
         if (t == 0) {
-            walk_start_point(G, W.seed, w, S.r, &S.sgn_out, &S.code);
+            walk_start_point(G, g, W.seed, w, S.r, &S.sgn_out, &S.code);
             S.hops = 0;
             S.done = 0;
             S.omega = 0.0;
@@ -798,7 +798,7 @@ struct LwArgs {
 DRWC_DEV void lw_start(const LwArgs& A, int slot, long long w) {
     double r[3], sgn;
     int code;
-    walk_start_point(A.G, A.W.seed, (uint64_t)w, r, &sgn, &code);
+    walk_start_point(A.G, A.g, A.W.seed, (uint64_t)w, r, &sgn, &code);
     A.st.px[slot] = r[0]; A.st.py[slot] = r[1]; A.st.pz[slot] = r[2];
     A.st.sgn[slot] = sgn;
     A.st.code[slot] = code;

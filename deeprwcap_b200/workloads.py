@@ -297,6 +297,7 @@ def job_params_plain(N: int = 16, master: int = 0, seed: int = 1, **kw) -> JobPa
     p.max_walks = kw.get("max_walks", 1 << 26)
     p.batch_walks = kw.get("batch_walks", 1 << 16)
     p.max_hops = kw.get("max_hops", 10000)
+    p.gauss_surface = kw.get("gauss_surface", 0)
     p.fdm.tol = kw.get("tol", 1e-10)
     p.fdm.inner_tol = kw.get("inner_tol", 1e-5)
     p.fdm.max_outer = kw.get("max_outer", 8)

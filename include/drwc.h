@@ -281,7 +281,11 @@ typedef struct drwc_job_params {
     int64_t max_walks;        /* hard cap */
     int64_t batch_walks;      /* walks per device batch between checks */
     int32_t max_hops;         /* per walk; a walk reaching it is "lost" */
-    int32_t pad_;
+    int32_t gauss_surface;    /* 0: the master's bounding box grown by gauss_offset;
+                                 1: the outer boundary of the union of the master's boxes,
+                                 each grown by min(gauss_offset, half its clearance to
+                                 the other nets and the enclosure) (masters whose
+                                 bounding box reaches another net) */
     uint64_t seed;
     drwc_fdm_opts fdm;        /* per-hop solve knobs */
 } drwc_job_params;

@@ -134,8 +134,14 @@ def test_clearance_and_job_params():
     assert C.clearance(s, 1) == pytest.approx(0.7)
     p = C.job_params(s, 1, c_ratio=c.c_ratio)
     assert p.gauss_offset == pytest.approx(0.35) and p.stop_dist == pytest.approx(0.35e-4)
-    assert p.master == 1 and p.c_ratio == pytest.approx(0.9)
-    s.boxes[3, 1] = 1.2  # B now reaches into A's bounding box
+    assert p.master == 1 and p.c_ratio == pytest.approx(0.9) and p.gauss_surface == 0
+    # B reaches into A's (L-shaped) bounding box without touching A's boxes:
+    # the Gaussian surface follows A's boxes, grown by half their gap to B
+    s.boxes[3, 1] = 1.2
+    p = C.job_params(s, 1)
+    assert p.gauss_surface == 1 and C.box_clearance(s, 1) == pytest.approx(0.7)
+    assert p.stop_dist == pytest.approx(0.35e-4)  # offsets per box, up to gauss_offset
+    s.boxes[3, 3] = 1.7  # B now touches A's second box
     with pytest.raises(ValueError):
         C.job_params(s, 1)
 
@@ -173,3 +179,17 @@ def test_result_parsers_and_metric(tmp_path):
     out = tmp_path / "r.dspf"
     C.write_dspf([{"master": "A", "row_F": {"A": 1.0e-15, "B": 3.0e-16, "GROUND": 5.0e-16}}], out)
     _close(C.parse_result(out), ref)
+
+
+def test_reference_case5_fixture_round_trip():
+    """The committed fixture of the reference's case 5 (parsed structure and
+    QuickCap couplings) loads back into the front-end's structure."""
+    from pathlib import Path
+    text = (Path(__file__).parent / "golden" / "cap3d_case5.json").read_text()
+    c, ref = C.load_case(text)
+    assert C.dump_case(c, ref) == text
+    s = C.to_structure(c)
+    master = C.net_of(c.masters[0])
+    assert master in ref and set(ref[master]) <= set(c.net_names)
+    assert len(s.boxes) == 25 and len(s.diel) == 38 and len(c.plates) == 32
+    assert C.clearance(s, c.net_names.index(master)) > 0

@@ -31,3 +31,39 @@ def test_front_end_equals_engine(ctx, tmp_path):
     back = C.parse_result(tmp_path / "a.dspf")
     err, self_err = C.compute_error({"A": row}, back)
     assert err < 1e-6 and self_err["A"] < 1e-6
+
+
+def test_reference_case5_against_quickcap(ctx):
+    """The reference's test case 5 (tests/golden/cap3d_case5.json, written from
+    testcases/cap3d/case5.cap3d and its QuickCap result ref/case5.dspf by
+    tests/golden/make_cap3d_fixtures.py), 2^20 walks at N = 16: the coupling
+    row scored with the reference's metric (run_script.py:179-197) against
+    QuickCap. Converged runs of this case score 0.2 %; the bar leaves room
+    for the statistics of a fixed walk budget."""
+    from pathlib import Path
+    c, ref = C.load_case((Path(__file__).parent / "golden" / "cap3d_case5.json").read_text())
+    res = C.extract(c, ctx=ctx, max_walks=1 << 20, p_tol=1e-9, c_tol=1e-9)
+    assert res["walks"] == 1 << 20
+    err, self_err = C.compute_error({res["master"]: res["row_F"]}, ref)
+    assert err < 0.02, (err, res["row_F"], ref)
+    assert self_err[res["master"]] < 0.01, self_err
+
+
+def test_box_following_gauss_surface_agrees_with_bounding_box(ctx):
+    """The small case's master A is L-shaped: its bounding box and the
+    boundary of its own grown boxes are two different Gaussian surfaces
+    around the same conductor, so they give the same capacitance row within
+    the statistics (independent estimates)."""
+    c = C.parse(CASE)
+    s = C.to_structure(c)
+    p0 = C.job_params(s, 1, p_tol=1e-9, c_tol=1e-9, max_walks=400_000)
+    p1 = C.job_params(s, 1, p_tol=1e-9, c_tol=1e-9, max_walks=400_000)
+    p1.gauss_surface = 1
+    p1.gauss_offset = 0.5 * C.box_clearance(s, 1)
+    p1.stop_dist = 1e-4 * p1.gauss_offset
+    r0 = engine.extract(s, p0, ctx)
+    r1 = engine.extract(s, p1, ctx)
+    assert r0.walks == r1.walks == 400_000 and r1.lost == 0
+    for e in range(s.n_nets + 1):
+        z = abs(r1.cap[e] - r0.cap[e]) / np.hypot(r0.stderr[e], r1.stderr[e])
+        assert z < 4.0, (e, r0.cap, r1.cap)

@@ -112,3 +112,16 @@ def test_failed_solves_end_walks_lost(ctx):
                  batch_walks=4096)
     r = engine.extract(s, pj, ctx=ctx)
     assert r.solves_failed > 0 and r.lost >= r.solves_failed
+
+
+def test_union_gauss_surface_of_one_box_is_the_box(ctx):
+    """gauss_surface = 1 (the outer boundary of the master's grown boxes)
+    for a master of one box is the Gauss box itself, face by face with the
+    same areas: the walks are identical."""
+    s = W.two_layer_crossing()
+    # an offset below half the master's clearance (0.05 um), so the per-box
+    # offset of gauss_surface = 1 is gauss_offset itself
+    e0, h0, w0 = engine.frw_walks(s, _params(8, gauss_offset=0.04), 0, 2000, ctx=ctx)
+    e1, h1, w1 = engine.frw_walks(s, _params(8, gauss_offset=0.04, gauss_surface=1), 0, 2000,
+                                  ctx=ctx)
+    assert np.array_equal(e0, e1) and np.array_equal(h0, h1) and np.array_equal(w0, w1)
