@@ -108,7 +108,7 @@ class ServerOpts(C.Structure):
                 ("steps_per_graph", C.c_int32), ("max_materials", C.c_int32),
                 ("max_nets", C.c_int32), ("conf_threshold", C.c_float), ("audit_frac", C.c_float),
                 ("timing", C.c_int32), ("uniform_table", C.c_int32), ("fair_share", C.c_int32),
-                ("fdm_hops", C.c_int32)]
+                ("fdm_hops", C.c_int32), ("straggler_hops", C.c_int32)]
 
 
 class ServerStats(C.Structure):

@@ -50,6 +50,9 @@ constexpr int kSvMaxSteps = 8;
 constexpr int kSvPrepIters = 64;  // prepare-loop passes per slot and step
 constexpr int kSvWin = 8;         // record slots per job: batches of walk ids in flight
 constexpr size_t kSvBsumStride = 3 * (DRWC_MAX_NETS + 2) + 8;  // doubles per (job, window slot)
+// per-step row counters: 4 per bucket (below), then per bucket the FDM rows
+// that continue for several hops (kept at the top of the bucket's list)
+constexpr int kSvCnt = 5 * DRWC_SERVER_MAX_SIZES;
 
 struct SvJob {
     DevGeom g;
@@ -104,7 +107,7 @@ struct SvArgs {
     const SvHdr* hdr;
     SvSlots st;
     int* blist[DRWC_SERVER_MAX_SIZES];
-    int* bkind[DRWC_SERVER_MAX_SIZES];  // bit 0 audit, bits 1.. network row
+    int* bkind[DRWC_SERVER_MAX_SIZES];  // bit 0 audit, bit 1 continuing, bits 2.. network row
     // per bucket b: cnt[4b] network rows, [4b + 1] first-hop rows, [4b + 2] FDM
     // rows, [4b + 3] the next unclaimed FDM row
     unsigned* cnt;
@@ -124,7 +127,8 @@ struct SvArgs {
     // of the uniform-permittivity Green's function and their running sums
     int table;
     int fair;                           // claim policy (drwc_server_opts.fair_share)
-    int fdm_hops;                       // hops an FDM-only walk takes per step
+    int fdm_hops;                       // hops a continuing FDM-only walk takes per step
+    int strag_hops;                     // a walk with this many hops continues
     const double* tval[DRWC_SERVER_MAX_SIZES][4];
     const double* tcdf[DRWC_SERVER_MAX_SIZES][4];
 };
@@ -267,7 +271,7 @@ DRWC_DEV void sv_table_hop(const SvArgs& A, int slot, const SvJob& J, int m) {
 }
 
 __global__ void sv_reset_kernel(SvArgs A) {
-    if (threadIdx.x < 4 * DRWC_SERVER_MAX_SIZES) A.cnt[threadIdx.x] = 0;
+    if (threadIdx.x < kSvCnt) A.cnt[threadIdx.x] = 0;
 }
 
 // One warp per slot.
@@ -339,9 +343,20 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
                 A.st.grow[slot] = (int)f;
             }
         } else {
-            const unsigned idx = atomicAdd(&A.cnt[4 * b + 2], 1u);
-            A.blist[b][idx] = slot;
-            A.bkind[b][idx] = 0;
+            // a walk of a job without a network takes several hops per step
+            // inside the FDM solve once the job's walks are all claimed (its
+            // tail) or once it is long (it holds back its batch); those rows
+            // fill the list from the top and are solved first, so a launch
+            // does not end waiting for a chain of hops claimed last
+            const bool cont = !A.table && A.fdm_hops > 1 &&
+                              (A.st.hops[slot] >= A.strag_hops ||
+                               *(volatile unsigned long long*)&A.ctr[A.st.job[slot]].next >=
+                                   (unsigned long long)J.total);
+            unsigned pos;
+            if (cont) pos = (unsigned)A.S - 1u - atomicAdd(&A.cnt[4 * DRWC_SERVER_MAX_SIZES + b], 1u);
+            else pos = atomicAdd(&A.cnt[4 * b + 2], 1u);
+            A.blist[b][pos] = slot;
+            A.bkind[b][pos] = cont ? 2 : 0;
         }
     }
 }
@@ -485,7 +500,7 @@ __global__ void __launch_bounds__(256) sv_sample_kernel(SvArgs A, int bucket) {
             if (audit || conf > A.conf_thresh) {
                 const unsigned idx = atomicAdd(&A.cnt[4 * bucket + 2], 1u);
                 A.blist[bucket][idx] = slot;
-                A.bkind[bucket][idx] = (audit ? 1 : 0) | (row << 1);
+                A.bkind[bucket][idx] = (audit ? 1 : 0) | (row << 2);
                 route = 1;
                 atomicAdd(A.stats + (audit ? SV_AUDITS : SV_FALLBACKS), 1ull);
             }
@@ -583,7 +598,9 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
     centre_offsets<N>(tco);
     double* ys = scratch_y + (size_t)blockIdx.x * D::NNN;
     float* ss = scratch_s + (size_t)blockIdx.x * D::NNN;
-    const unsigned count = A.cnt[4 * bucket + 2];
+    // continuing rows (at the top of the list) first, then the others
+    const unsigned n_cont = A.cnt[4 * DRWC_SERVER_MAX_SIZES + bucket];
+    const unsigned count = A.cnt[4 * bucket + 2] + n_cont;
     unsigned* next_item = A.cnt + 4 * bucket + 3;
     __shared__ unsigned s_idx;
     __shared__ int s_go;
@@ -599,8 +616,9 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
         __syncthreads();
         const unsigned idx = s_idx;
         if (idx >= count) break;
-        const int slot = A.blist[bucket][idx];
-        const int kind = A.bkind[bucket][idx];
+        const unsigned pos = idx < n_cont ? (unsigned)A.S - 1u - idx : idx - n_cont;
+        const int slot = A.blist[bucket][pos];
+        const int kind = A.bkind[bucket][pos];
         const int j = A.st.job[slot];
         const SvJob& J = A.jobs[j];
         if (j != loaded) {
@@ -618,11 +636,11 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
             loaded = j;
         }
         __syncthreads();
-        // Once every walk of a job without a network (and without the uniform
-        // table) has been claimed, its remaining walks continue here for up to
-        // fdm_hops hops per step: otherwise each hop of such a tail walk waits
-        // a whole step (every other slot's hop), and the job's completion
-        // waits for its longest walks.
+        // A continuing row (a walk of a job without a network or uniform table,
+        // once the job's walks are all claimed or once the walk is long) takes
+        // up to fdm_hops hops here: otherwise each hop of such a walk waits a
+        // whole step (every other slot's hop), and its batch, or the job's
+        // completion, waits for the longest walks.
         for (int hh = 0;; ++hh) {
             const EpsPalette E{mat, pal, palinv, pair64, pair32, P};
             const long long w = A.st.walk[slot];
@@ -661,7 +679,7 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
             __syncthreads();
             if ((kind & 1) && !first) {
                 // audit: KL(FDM || network) over the panels
-                const float* o = A.O[bucket] + (size_t)(kind >> 1) * A.out_row[bucket];
+                const float* o = A.O[bucket] + (size_t)(kind >> 2) * A.out_row[bucket];
                 const double ls = block_lse<D::NW>(o, M, sm.red);
                 __syncthreads();
                 double kl = 0.0;
@@ -705,8 +723,9 @@ sv_fdm_kernel(SvArgs A, int bucket, int maxP, double* __restrict__ scratch_y,
                 my_fail += st.status == 1;
             }
             __syncthreads();
-            if (kind != 0 || J.use_net || A.table || hh + 1 >= A.fdm_hops) break;
-            if (*(volatile unsigned long long*)&A.ctr[j].next < (unsigned long long)J.total) break;
+            // a continuing row (bit 1, set by the prepare kernel) takes its
+            // next hops here
+            if (kind != 2 || hh + 1 >= A.fdm_hops) break;
             if (A.st.mode[slot] == 0) break;  // the walk finished on this hop
             // the next hop's cube: nearest conductor, absorption (the prepare
             // kernel's geometry step for this slot)
@@ -1011,7 +1030,7 @@ static int sv_step(drwc_server* v, int k) {
     cudaStream_t s = ctx->stream;
     const SvArgs& A = v->A;
     int rc;
-    sv_reset_kernel<<<1, 32, 0, s>>>(A);
+    sv_reset_kernel<<<1, kSvCnt, 0, s>>>(A);
     if ((rc = launch_check(ctx))) return rc;
     sv_prepare_kernel<<<(A.S * 32 + 255) / 256, 256, 0, s>>>(A);
     if ((rc = launch_check(ctx))) return rc;
@@ -1415,7 +1434,7 @@ static int sv_alloc(drwc_server* v) {
     auto take = [&](size_t bytes) { size_t r = off; off += (bytes + 255) / 256 * 256; return r; };
     const size_t o_jobs = take(sizeof(SvJob) * kSvMaxJobs), o_ctr = take(sizeof(SvCtr) * kSvMaxJobs),
                  o_hdr = take(sizeof(SvHdr)), o_bsum = take(8 * kSvBsumStride * kSvWin * kSvMaxJobs),
-                 o_stats = take(8 * SV_NSTATS), o_akl = take(16), o_cnt = take(64),
+                 o_stats = take(8 * SV_NSTATS), o_akl = take(16), o_cnt = take(4 * kSvCnt),
                  o_dbl = take(8 * (size_t)S * 7), o_walk = take(8 * (size_t)S),
                  o_int = take(4 * (size_t)S * 5),
                  o_b = take(4 * (size_t)S * 2 * DRWC_SERVER_MAX_SIZES);
@@ -1486,6 +1505,7 @@ static int sv_alloc(drwc_server* v) {
     A.table = v->o.uniform_table;
     A.fair = v->o.fair_share;
     A.fdm_hops = v->o.fdm_hops;
+    A.strag_hops = v->o.straggler_hops;
     for (int b = 0; b < v->o.n_sizes; ++b) {
         v->fdm_sy[b] = (double*)(B + o_sy[b]);
         v->fdm_ss[b] = (float*)(B + o_ss[b]);
@@ -1554,7 +1574,10 @@ DRWC_API void drwc_server_opts_default(drwc_server_opts* o) {
     o->uniform_table = 0;
     o->fair_share = 0;
     o->fdm_hops = 0;
+    o->straggler_hops = 0;
 }
+
+static_assert(sizeof(drwc_server_opts) == 80, "the option layout the bindings mirror");
 
 DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts,
                                 drwc_net* const* nets, int32_t n_nets, drwc_server** out) {
@@ -1568,7 +1591,8 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts,
         o.steps_per_graph < 1 || o.steps_per_graph > kSvMaxSteps || o.max_materials < 1 ||
         o.max_materials > kMaxMaterials || o.max_nets < 1 || o.max_nets > DRWC_MAX_NETS ||
         !(o.audit_frac >= 0.f && o.audit_frac <= 1.f) || o.uniform_table < 0 || o.uniform_table > 1 ||
-        o.fair_share < 0 || o.fair_share > 1 || o.fdm_hops < 0 || o.fdm_hops > 64)
+        o.fair_share < 0 || o.fair_share > 1 || o.fdm_hops < 0 || o.fdm_hops > 64 ||
+        o.straggler_hops < 0)
         return DRWC_ERR_INVALID;
     if (n_nets < 0 || n_nets > DRWC_SERVER_MAX_SIZES || (n_nets > 0 && !nets))
         return DRWC_ERR_INVALID;
@@ -1594,6 +1618,7 @@ DRWC_API int drwc_server_create(drwc_ctx* ctx, const drwc_server_opts* opts,
     }
     if (v->o.slots == 0) v->o.slots = 65536;
     if (v->o.fdm_hops == 0) v->o.fdm_hops = 64;
+    if (v->o.straggler_hops == 0) v->o.straggler_hops = 32;
     o = v->o;
     {
         std::lock_guard<std::mutex> lock(ctx->mu);

@@ -402,6 +402,11 @@ typedef struct drwc_server_opts {
                                  1..64; 0 (default) = 64. Otherwise each hop of such a
                                  tail walk waits a whole step, and the job's completion
                                  waits for its longest walks */
+    int32_t straggler_hops;   /* a walk of such a job (no network, uniform_table = 0) that
+                                 has taken this many hops also takes up to fdm_hops hops per
+                                 step, so a batch does not wait many steps for its longest
+                                 walks (a job holds at most 8 batches of walk ids in flight);
+                                 0 (default) = 32; a value above max_hops turns it off */
 } drwc_server_opts;
 DRWC_API void drwc_server_opts_default(drwc_server_opts* o);
 /* nets (n_nets of them, each of a different served resolution; none: every

@@ -65,9 +65,11 @@ def test_server_defaults_and_argument_checks_without_device():
     from deeprwcap_b200 import abi, engine
     L = abi.load()
     o = engine.server_opts()
-    # slots 0 / fdm_hops 0: defaults applied at creation (65536 slots, 64 tail hops per step)
+    # slots 0 / fdm_hops 0 / straggler_hops 0: defaults applied at creation (65536 slots,
+    # up to 64 hops per step for a walk past its 32nd hop or in a job's tail)
     assert (o.slots, o.max_jobs, o.hbm_budget, o.n_sizes) == (0, 32, 1 << 30, 3)
-    assert o.fdm_hops == 0
+    assert o.fdm_hops == 0 and o.straggler_hops == 0
+    assert C.sizeof(abi.ServerOpts) == 80  # static_assert in csrc/serve.cu
     assert list(o.sizes[:3]) == [16, 21, 23] and o.steps_per_graph == 2
     assert o.max_materials == 16 and o.max_nets == 64 and abs(o.audit_frac - 0.01) < 1e-7
     o2 = engine.server_opts(sizes=(16, 23), slots=1024)
