@@ -898,8 +898,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-fdm", action="store_true")
     ap.add_argument("--serve-jobs", type=int, default=10)
-    ap.add_argument("--serve-walks-max", type=float, default=1e6)
-    ap.add_argument("--serve-train-samples", type=int, default=1 << 18)
+    ap.add_argument("--serve-walks-max", type=float, default=1e7)
+    ap.add_argument("--serve-train-samples", type=int, default=1 << 20)
     args = ap.parse_args()
     world, rank, local = dist_init()
     if args.workload == "fdm_batch":

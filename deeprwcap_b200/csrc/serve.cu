@@ -233,10 +233,32 @@ DRWC_DEV int sv_homogeneous(const DevGeom& g, const double c[3], double a, int N
     return __any_sync(0xffffffffu, clash) ? -1 : m;
 }
 
+// First index i in [0, M) with cdf[i] > target, M - 1 when there is none
+// (the binary search's answer; cdf is nondecreasing), warp-wide in rounds of
+// 32 loads: the first of 32 strides whose last entry passes the target, then
+// the same within that stride. Three dependent loads for M <= 32768 instead
+// of a binary search's eleven or twelve.
+DRWC_DEV int warp_cdf_search(const double* __restrict__ cdf, int M, double target) {
+    const int lane = threadIdx.x & 31;
+    int lo = 0, len = M;  // the answer is in [lo, lo + len); its last entry passes
+    while (len > 1) {
+        const int s = (len + 31) >> 5;
+        const int pos = min(lo + (lane + 1) * s, lo + len) - 1;
+        const unsigned b = __ballot_sync(0xffffffffu, cdf[pos] > target);
+        if (b == 0u) return M - 1;  // only in the first round: nothing passes
+        const int f = __ffs(b) - 1;
+        const int nlo = lo + f * s;
+        len = min(lo + (f + 1) * s, lo + len) - nlo;
+        lo = nlo;
+    }
+    return lo;
+}
+
 // One hop of a homogeneous cube from the uniform-permittivity tables: the
 // surface values of a single-permittivity cube do not depend on that
 // permittivity, and its centre permittivity is the material's own, so the
 // draw needs no solve. Same Philox draws and weight formula as the FDM hop.
+// Warp-wide (the search); lane 0 writes the slot.
 DRWC_DEV void sv_table_hop(const SvArgs& A, int slot, const SvJob& J, int m) {
     const int N = J.W.N, M = 6 * N * N;
     const int h = A.st.hops[slot];
@@ -249,13 +271,8 @@ DRWC_DEV void sv_table_hop(const SvArgs& A, int slot, const SvJob& J, int m) {
                              : philox_uniform2(J.W.seed, (uint64_t)w, (uint32_t)h, 0);
     const double tot = cdf[M - 1];
     const double target = (first ? u2.y : u2.x) * tot;
-    int lo = 0, hi = M - 1;  // first panel whose running sum passes the target
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (cdf[mid] > target) hi = mid;
-        else lo = mid + 1;
-    }
-    const int b = lo;
+    const int b = warp_cdf_search(cdf, M, target);  // first panel whose running sum passes
+    if ((threadIdx.x & 31) != 0) return;
     const double a = A.st.a[slot];
     if (first) {
         const double v = J.g.pal[m];
@@ -319,7 +336,7 @@ __global__ void __launch_bounds__(256) sv_prepare_kernel(SvArgs A) {
             __syncwarp();
             const int m = sv_homogeneous(J.g, r, A.st.a[slot], J.W.N);
             if (m >= 0) {
-                if (lane == 0) sv_table_hop(A, slot, J, m);
+                sv_table_hop(A, slot, J, m);
                 table_hops += 1;
                 act = 0;
             }

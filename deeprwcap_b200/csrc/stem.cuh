@@ -176,13 +176,99 @@ struct Stem {
         pending = aborted();  // after a timeout the MMAs may still be in flight
     }
 
+    // Class of a conv1 output index along an axis whose input values do not
+    // vary: which of its three taps fall outside the grid (0: the first, 1:
+    // none, 2: the last). Rows of equal class along both such axes and the
+    // same index along the varying axis have the same 27 taps.
+    static DRWC_DEV int c1_class(int p) { return p == 0 ? 0 : (2 * p + 1 >= N ? 2 : 1); }
+
+    // conv1 of a cube whose values vary along uaxis alone: its D2 x 3 x 3
+    // distinct rows (index along uaxis; class along the other two axes in
+    // z, y, x order) fill one M tile, and each of the P2 rows of a1(cube)
+    // is copied from its class row. A row's result does not depend on the
+    // other rows of its tile, so a1 holds the values the full convolution
+    // writes, from one MMA batch instead of MT1 tiles.
+    DRWC_DEV bool conv1_uaxis(int cube, int* err, int uaxis,
+                              const __nv_bfloat16* __restrict__ pv) {
+        static_assert(9 * S::D2 <= kUmmaM, "the class rows fit one tile");
+        const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
+        // class rows after the operand tile (the operand area holds >= 4 tiles)
+        __nv_bfloat16* a1c = reinterpret_cast<__nv_bfloat16*>(opa() + 8192);
+        auto rep = [](int c) { return c == 2 ? S::D2 - 1 : c; };  // an index of each class
+        if (t < kUmmaM) {
+            const int r = t;
+            uint32_t pk[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) pk[i] = 0u;
+            if (r < 9 * S::D2) {
+                const int pu = r / 9, ca = rep((r / 3) % 3), cb = rep(r % 3);
+                const int pz = uaxis == 2 ? pu : ca;
+                const int py = uaxis == 2 ? ca : uaxis == 1 ? pu : cb;
+                const int px = uaxis == 0 ? pu : cb;
+                const int z0 = 2 * pz - 1, y0 = 2 * py - 1, x0 = 2 * px - 1;
+                const int u0 = uaxis == 2 ? z0 : uaxis == 1 ? y0 : x0;
+                uint32_t uv[3], ok[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    uv[d] = (unsigned)(u0 + d) < (unsigned)N
+                                ? (uint32_t)__bfloat16_as_ushort(pv[u0 + d]) : 0u;
+                    ok[d] = ((unsigned)(x0 + d) < (unsigned)N ? 1u : 0u) |
+                            ((unsigned)(y0 + d) < (unsigned)N ? 2u : 0u) |
+                            ((unsigned)(z0 + d) < (unsigned)N ? 4u : 0u);
+                }
+#pragma unroll
+                for (int tap = 0; tap < 27; ++tap) {
+                    const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+                    const bool in = (ok[dx] & 1u) && (ok[dy] & 2u) && (ok[dz] & 4u);
+                    const uint32_t v = uaxis == 2 ? uv[dz] : uaxis == 1 ? uv[dy] : uv[dx];
+                    pk[tap >> 1] |= (in ? v : 0u) << (16 * (tap & 1));
+                }
+            }
+            unsigned char* base = opa() + (r >> 3) * 256 + (r & 7) * 16;
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                *reinterpret_cast<uint4*>(base + (c >> 1) * 4096 + (c & 1) * 128) =
+                    make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
+        }
+        if (!staged()) return false;
+        if (t == 0) {
+            for (int k = 0; k < 2; ++k)
+                umma_bf16(tmem, umma_smem_desc(smem_u32(opa() + k * 4096), 128, 256),
+                          umma_smem_desc(smem_u32(sm + S::O_W1 + k * 512), 128, 256),
+                          umma_idesc_bf16<16>(), (uint32_t)k);
+            umma_commit(bar());
+        }
+        complete(err);
+        if (sub == 0) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16), v);
+            const int r = 32 * q + lane;
+            if (r < 9 * S::D2) stem_store16(v, b1(), a1c + (size_t)r * 16);
+        }
+        tc_fence_before();  // the next MMAs overwrite these columns
+        __syncthreads();
+        __nv_bfloat16* dst = a1(cube);
+        for (int e = t; e < 2 * S::P2; e += S::NT) {
+            const int p = e >> 1, h = e & 1;
+            const int pz = p / (S::D2 * S::D2), py = (p / S::D2) % S::D2, px = p % S::D2;
+            const int pu = uaxis == 2 ? pz : uaxis == 1 ? py : px;
+            const int ca = c1_class(uaxis == 2 ? py : pz), cb = c1_class(uaxis == 0 ? py : px);
+            const int r = pu * 9 + ca * 3 + cb;
+            *reinterpret_cast<uint4*>(dst + (size_t)p * 16 + 8 * h) =
+                *reinterpret_cast<const uint4*>(a1c + (size_t)r * 16 + 8 * h);
+        }
+        __syncthreads();  // a1 complete; every thread sees the same abort flag
+        return !aborted();
+    }
+
     // conv1 of the cube into a1(cube), up to R1 M tiles per batch, from the
     // voxels in xs() or, with uaxis >= 0, from pv: the cube's values then
     // vary along that index alone (0 = x, 1 = y, 2 = z; pv[t] is the value
     // at index t), so a row's 27 taps come from three values and the grid
-    // bounds (the same values xs would hold).
+    // bounds (the same values xs would hold), and conv1_uaxis computes it.
     DRWC_DEV bool conv1(int cube, int* err, int uaxis = -1,
                         const __nv_bfloat16* __restrict__ pv = nullptr) {
+        if (uaxis >= 0) return conv1_uaxis(cube, err, uaxis, pv);
         const __nv_bfloat16* x = xs();
         const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
         for (int m0 = 0; m0 < S::MT1; m0 += S::R1) {
