@@ -428,6 +428,7 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
     bool ok = true;
     for (int grp = blockIdx.x; ok && grp * D::CUBES < na; grp += gridDim.x) {
         const int g0 = grp * D::CUBES, nc = min(D::CUBES, na - g0);
+        int uaxis = -1;  // of the group's last cube
         for (int cb = 0; ok && cb < nc; ++cb) {
             // the group's headers were written after the previous group's last
             // barrier; later cubes follow conv1's closing barrier, which the
@@ -446,7 +447,7 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
             const int rot = first ? rot_of_code(h.code) : 0;
             const double c[3] = {h.px, h.py, h.pz};
             vox_prepare<N>(gs, c, h.a, tco, vs, pal, pvs);
-            int uaxis = -1;
+            uaxis = -1;
             if (vs.nrel == 0) {
                 // no block reaches the cube: its values vary along one index
                 // (the original z axis in the rotated frame), pvs holds them;
@@ -477,7 +478,13 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
         const bool fetch = (int)threadIdx.x < D::CUBES && gn < na;
         SvCubeHdr nh;
         if (fetch) nh = sv_cube_hdr(A, bucket, gn);
-        if (ok) ok = st.conv2(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err);
+        if constexpr (D::CUBES == 1) {
+            // one cube per group: a stratified one runs on its class rows
+            if (ok) ok = uaxis >= 0 ? st.conv2_uaxis(uaxis, W.a2 + (size_t)g0 * D::P3 * 32, W.err)
+                                    : st.conv2(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err);
+        } else {
+            if (ok) ok = st.conv2(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err);
+        }
         if (fetch) hdr[threadIdx.x] = nh;  // conv2 ended with a barrier: no cube reads hdr now
     }
     st.end();

@@ -180,7 +180,32 @@ struct Stem {
     // vary: which of its three taps fall outside the grid (0: the first, 1:
     // none, 2: the last). Rows of equal class along both such axes and the
     // same index along the varying axis have the same 27 taps.
-    static DRWC_DEV int c1_class(int p) { return p == 0 ? 0 : (2 * p + 1 >= N ? 2 : 1); }
+    static constexpr DRWC_DEV int c1_class(int p) { return p == 0 ? 0 : (2 * p + 1 >= N ? 2 : 1); }
+    // The same for a conv2 output index: its three taps read conv1 indices
+    // 2q - 1 .. 2q + 1 (or the zero padding), and those classes (0, 1, 1 at
+    // q = 0; 1, 1, 1 inside; at the last index of an odd N either 1, 1, 2 or
+    // 1, 2, padding) fix the row; rep2 is an index of each class.
+    static constexpr DRWC_DEV int c2_class(int q) {
+        return q == 0 ? 0 : (q == S::D3 - 1 && (N & 1) ? 2 : 1);
+    }
+    static constexpr DRWC_DEV int c2_rep(int c) { return c == 2 ? S::D3 - 1 : c; }
+    static constexpr int c2_sig(int q) {  // the conv1 classes (3: padding) of q's taps
+        int sg = 0;
+        for (int d = 0; d < 3; ++d) {
+            const int p = 2 * q - 1 + d;
+            sg = 4 * sg + ((p < 0 || p >= S::D2) ? 3 : c1_class(p));
+        }
+        return sg;
+    }
+    static constexpr bool c2_classes_exact() {
+        for (int a = 0; a < S::D3; ++a) {
+            if (c2_sig(a) != c2_sig(c2_rep(c2_class(a)))) return false;
+            for (int b = 0; b < S::D3; ++b)
+                if ((c2_class(a) == c2_class(b)) != (c2_sig(a) == c2_sig(b))) return false;
+        }
+        return true;
+    }
+    static_assert(c2_classes_exact(), "conv2 classes group exactly the rows with equal taps");
 
     // conv1 of a cube whose values vary along uaxis alone: its D2 x 3 x 3
     // distinct rows (index along uaxis; class along the other two axes in
@@ -192,8 +217,11 @@ struct Stem {
                               const __nv_bfloat16* __restrict__ pv) {
         static_assert(9 * S::D2 <= kUmmaM, "the class rows fit one tile");
         const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
-        // class rows after the operand tile (the operand area holds >= 4 tiles)
-        __nv_bfloat16* a1c = reinterpret_cast<__nv_bfloat16*>(opa() + 8192);
+        // class rows: a one-cube group keeps them at a1(0) for conv2_uaxis;
+        // otherwise after the operand tile (the operand area holds >= 4
+        // tiles) until they are copied to a1(cube)
+        __nv_bfloat16* a1c = S::CUBES == 1 ? a1(0)
+                                           : reinterpret_cast<__nv_bfloat16*>(opa() + 8192);
         auto rep = [](int c) { return c == 2 ? S::D2 - 1 : c; };  // an index of each class
         if (t < kUmmaM) {
             const int r = t;
@@ -247,6 +275,7 @@ struct Stem {
         }
         tc_fence_before();  // the next MMAs overwrite these columns
         __syncthreads();
+        if (S::CUBES == 1) return !aborted();
         __nv_bfloat16* dst = a1(cube);
         for (int e = t; e < 2 * S::P2; e += S::NT) {
             const int p = e >> 1, h = e & 1;
@@ -402,6 +431,81 @@ struct Stem {
         }
         tc_fence_before();
         __syncthreads();
+        return !aborted();
+    }
+
+    // conv2 of a one-cube group whose cube varies along uaxis alone (conv1_uaxis
+    // left its class rows at a1(0)): the D3 x 3 x 3 class rows (index along
+    // uaxis, conv2 class along the other two) in one M tile, their taps
+    // gathered from conv1's class rows; the epilogue stages them in shared
+    // memory and every a2 row of the cube is copied from its class row. Same
+    // operands per row as conv2, so the same a2.
+    DRWC_DEV bool conv2_uaxis(int uaxis, __nv_bfloat16* __restrict__ a2, int* err) {
+        static_assert(S::CUBES == 1 && 9 * S::D3 <= kUmmaM, "one cube, class rows in one tile");
+        const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
+        const __nv_bfloat16* a1c = a1(0);
+        constexpr int NR = 9 * S::D3;
+        const int pr = t & 255, r = pr >> 1, h = pr & 1;
+        const bool filler = t < 256;  // one (row, channel half) of the tile each
+        unsigned char* dst = opa() + (r >> 3) * 256 + h * 128 + (r & 7) * 16;
+        int qz = 0, qy = 0, qx = 0;
+        const bool row_ok = filler && r < NR;
+        if (row_ok) {
+            const int qu = r / 9, ca = c2_rep((r / 3) % 3), cb = c2_rep(r % 3);
+            qz = uaxis == 2 ? qu : ca;
+            qy = uaxis == 2 ? ca : uaxis == 1 ? qu : cb;
+            qx = uaxis == 0 ? qu : cb;
+        }
+        const int z0 = 2 * qz - 1, y0 = 2 * qy - 1, x0 = 2 * qx - 1;
+        for (int cc = 0; cc < 3; ++cc) {  // fill cc holds the taps with dz = cc
+            if (filler) {
+                const int z = z0 + cc;
+#pragma unroll
+                for (int ti = 0; ti < 9; ++ti) {
+                    const int y = y0 + ti / 3, x = x0 + ti % 3;
+                    uint4 val = make_uint4(0u, 0u, 0u, 0u);
+                    if (row_ok && (unsigned)z < (unsigned)S::D2 && (unsigned)y < (unsigned)S::D2 &&
+                        (unsigned)x < (unsigned)S::D2) {
+                        const int pu = uaxis == 2 ? z : uaxis == 1 ? y : x;
+                        const int ca1 = c1_class(uaxis == 2 ? y : z), cb1 = c1_class(uaxis == 0 ? y : x);
+                        val = *reinterpret_cast<const uint4*>(a1c + (size_t)(pu * 9 + ca1 * 3 + cb1) * 16 +
+                                                              8 * h);
+                    }
+                    *reinterpret_cast<uint4*>(dst + ti * 4096) = val;
+                }
+            }
+            if (!staged()) return false;
+            if (t == 0) {
+                for (int ti = 0; ti < S::TAPS; ++ti)
+                    umma_bf16(tmem + S::C2,
+                              umma_smem_desc(smem_u32(opa() + ti * 4096), 128, 256),
+                              umma_smem_desc(smem_u32(sm + S::O_W2 + (cc * S::TAPS + ti) * 1024), 128, 256),
+                              umma_idesc_bf16<32>(), (cc | ti) ? 1u : 0u);
+                umma_commit(bar());
+            }
+            complete(err);
+        }
+        // epilogue: the class rows (two 16-column halves) into shared memory
+        // (the operand area, free once the MMAs completed) ...
+        __nv_bfloat16* a2c = reinterpret_cast<__nv_bfloat16*>(opa());
+        if (sub < 2) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + S::C2 + 16 * sub, v);
+            const int R = 32 * q + lane;
+            if (R < NR) stem_store16(v, b2() + 16 * sub, a2c + (size_t)R * 32 + 16 * sub);
+        }
+        tc_fence_before();
+        __syncthreads();
+        // ... then every row of the cube from its class row (four 16-byte parts)
+        for (int e = t; e < 4 * S::P3; e += S::NT) {
+            const int p = e >> 2, k = e & 3;
+            const int pz = p / (S::D3 * S::D3), py = (p / S::D3) % S::D3, px = p % S::D3;
+            const int qu = uaxis == 2 ? pz : uaxis == 1 ? py : px;
+            const int ca = c2_class(uaxis == 2 ? py : pz), cb = c2_class(uaxis == 0 ? py : px);
+            *reinterpret_cast<uint4*>(a2 + (size_t)p * 32 + 8 * k) =
+                *reinterpret_cast<const uint4*>(a2c + (size_t)(qu * 9 + ca * 3 + cb) * 32 + 8 * k);
+        }
+        __syncthreads();  // the operand area is reused by the next group
         return !aborted();
     }
 
