@@ -47,7 +47,15 @@ namespace drwc {
 
 constexpr int kSvMaxJobs = 64;
 constexpr int kSvMaxSteps = 8;
-constexpr int kSvPrepIters = 64;  // prepare-loop passes per slot and step
+// Prepare-loop passes per slot and step (claims, finished walks, table hops).
+// A slot deep in a homogeneous region chains table hops; the launch ends with
+// its longest chain, so a short limit shortens every step, and the rest of
+// the chain continues in the next one (learned stream: 16 passes 3 % faster
+// than 64, 8 and 32 between them; the walks are the same whatever the limit).
+#ifndef DRWC_SV_PREP_ITERS
+#define DRWC_SV_PREP_ITERS 16
+#endif
+constexpr int kSvPrepIters = DRWC_SV_PREP_ITERS;
 constexpr int kSvWin = 8;         // record slots per job: batches of walk ids in flight
 constexpr size_t kSvBsumStride = 3 * (DRWC_MAX_NETS + 2) + 8;  // doubles per (job, window slot)
 // per-step row counters: 4 per bucket (below), then per bucket the FDM rows
@@ -428,7 +436,8 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
     bool ok = true;
     for (int grp = blockIdx.x; ok && grp * D::CUBES < na; grp += gridDim.x) {
         const int g0 = grp * D::CUBES, nc = min(D::CUBES, na - g0);
-        int uaxis = -1;  // of the group's last cube
+        int uaxis = -1;           // of the group's last cube
+        int ux0 = -1, ux1 = -1;   // of its cubes 0 and 1 (two-cube groups)
         for (int cb = 0; ok && cb < nc; ++cb) {
             // the group's headers were written after the previous group's last
             // barrier; later cubes follow conv1's closing barrier, which the
@@ -472,6 +481,8 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
                 }
             }
             ok = st.conv1(cb, W.err, uaxis, pvs);
+            if (cb == 0) ux0 = uaxis;
+            else ux1 = uaxis;
         }
         // the next group's cubes are fetched while conv2 runs
         const int gn = (grp + (int)gridDim.x) * D::CUBES + (int)threadIdx.x;
@@ -483,7 +494,10 @@ __global__ void __launch_bounds__(StemDims<N>::NT, StemDims<N>::CTAS)
             if (ok) ok = uaxis >= 0 ? st.conv2_uaxis(uaxis, W.a2 + (size_t)g0 * D::P3 * 32, W.err)
                                     : st.conv2(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err);
         } else {
-            if (ok) ok = st.conv2(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err);
+            // two cubes per group: the pair form when either is stratified
+            if (ok) ok = (ux0 >= 0 || ux1 >= 0)
+                             ? st.conv2_pair(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err, ux0, ux1)
+                             : st.conv2(nc, W.a2 + (size_t)g0 * D::P3 * 32, W.err);
         }
         if (fetch) hdr[threadIdx.x] = nh;  // conv2 ended with a barrier: no cube reads hdr now
     }

@@ -209,19 +209,17 @@ struct Stem {
 
     // conv1 of a cube whose values vary along uaxis alone: its D2 x 3 x 3
     // distinct rows (index along uaxis; class along the other two axes in
-    // z, y, x order) fill one M tile, and each of the P2 rows of a1(cube)
-    // is copied from its class row. A row's result does not depend on the
-    // other rows of its tile, so a1 holds the values the full convolution
-    // writes, from one MMA batch instead of MT1 tiles.
+    // z, y, x order) fill one M tile and stay at the start of a1(cube), where
+    // conv2 reads a row's values from its class row. A row's result does not
+    // depend on the other rows of its tile, so these are the values the full
+    // convolution writes, from one MMA batch instead of MT1 tiles.
     DRWC_DEV bool conv1_uaxis(int cube, int* err, int uaxis,
                               const __nv_bfloat16* __restrict__ pv) {
         static_assert(9 * S::D2 <= kUmmaM, "the class rows fit one tile");
         const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
-        // class rows: a one-cube group keeps them at a1(0) for conv2_uaxis;
-        // otherwise after the operand tile (the operand area holds >= 4
-        // tiles) until they are copied to a1(cube)
-        __nv_bfloat16* a1c = S::CUBES == 1 ? a1(0)
-                                           : reinterpret_cast<__nv_bfloat16*>(opa() + 8192);
+        // the class rows stay at the start of a1(cube): conv2_uaxis /
+        // conv2_pair gather from them
+        __nv_bfloat16* a1c = a1(cube);
         auto rep = [](int c) { return c == 2 ? S::D2 - 1 : c; };  // an index of each class
         if (t < kUmmaM) {
             const int r = t;
@@ -274,19 +272,7 @@ struct Stem {
             if (r < 9 * S::D2) stem_store16(v, b1(), a1c + (size_t)r * 16);
         }
         tc_fence_before();  // the next MMAs overwrite these columns
-        __syncthreads();
-        if (S::CUBES == 1) return !aborted();
-        __nv_bfloat16* dst = a1(cube);
-        for (int e = t; e < 2 * S::P2; e += S::NT) {
-            const int p = e >> 1, h = e & 1;
-            const int pz = p / (S::D2 * S::D2), py = (p / S::D2) % S::D2, px = p % S::D2;
-            const int pu = uaxis == 2 ? pz : uaxis == 1 ? py : px;
-            const int ca = c1_class(uaxis == 2 ? py : pz), cb = c1_class(uaxis == 0 ? py : px);
-            const int r = pu * 9 + ca * 3 + cb;
-            *reinterpret_cast<uint4*>(dst + (size_t)p * 16 + 8 * h) =
-                *reinterpret_cast<const uint4*>(a1c + (size_t)r * 16 + 8 * h);
-        }
-        __syncthreads();  // a1 complete; every thread sees the same abort flag
+        __syncthreads();  // class rows complete; every thread sees the same abort flag
         return !aborted();
     }
 
@@ -504,6 +490,93 @@ struct Stem {
             const int ca = c2_class(uaxis == 2 ? py : pz), cb = c2_class(uaxis == 0 ? py : px);
             *reinterpret_cast<uint4*>(a2 + (size_t)p * 32 + 8 * k) =
                 *reinterpret_cast<const uint4*>(a2c + (size_t)(qu * 9 + ca * 3 + cb) * 32 + 8 * k);
+        }
+        __syncthreads();  // the operand area is reused by the next group
+        return !aborted();
+    }
+
+    // conv2 of a two-cube group (N = 16) of which at least one cube varies
+    // along one axis alone (ux0 / ux1 >= 0; -1: a full cube): a class cube
+    // uses its D3 x 3 x 3 class rows at the start of its 64-row part of the
+    // tile, gathered from conv1's class rows, a full cube its 64 rows. The
+    // epilogue stages the tile in shared memory, then writes each a2 row of
+    // the group, a class cube's from its class row.
+    DRWC_DEV bool conv2_pair(int nc, __nv_bfloat16* __restrict__ a2, int* err, int ux0, int ux1) {
+        static_assert(S::CUBES == 2 && S::MT2 == 1 && S::NT == 256 && 9 * S::D3 <= S::P3,
+                      "two cubes in one tile, class rows inside a cube's part");
+        const int t = threadIdx.x, w = t >> 5, lane = t & 31, q = w & 3, sub = w >> 2;
+        const int r = t >> 1, h = t & 1;  // one (row, channel half) of the tile each
+        unsigned char* dst = opa() + (r >> 3) * 256 + h * 128 + (r & 7) * 16;
+        const int cube = r / S::P3, p = r % S::P3;
+        const int ux = cube == 0 ? ux0 : ux1;
+        const bool cls = ux >= 0;
+        const bool row_ok = cube < nc && (!cls || p < 9 * S::D3);
+        int qz, qy, qx;
+        if (cls) {
+            const int qu = p / 9, ca = c2_rep((p / 3) % 3), cb = c2_rep(p % 3);
+            qz = ux == 2 ? qu : ca;
+            qy = ux == 2 ? ca : ux == 1 ? qu : cb;
+            qx = ux == 0 ? qu : cb;
+        } else {
+            qz = p / (S::D3 * S::D3);
+            qy = (p / S::D3) % S::D3;
+            qx = p % S::D3;
+        }
+        const int z0 = 2 * qz - 1, y0 = 2 * qy - 1, x0 = 2 * qx - 1;
+        const __nv_bfloat16* A1 = a1(cube < nc ? cube : 0) + 8 * h;
+        for (int cc = 0; cc < 3; ++cc) {  // fill cc holds the taps with dz = cc
+            const int z = z0 + cc;
+#pragma unroll
+            for (int ti = 0; ti < 9; ++ti) {
+                const int y = y0 + ti / 3, x = x0 + ti % 3;
+                uint4 val = make_uint4(0u, 0u, 0u, 0u);
+                if (row_ok && (unsigned)z < (unsigned)S::D2 && (unsigned)y < (unsigned)S::D2 &&
+                    (unsigned)x < (unsigned)S::D2) {
+                    int idx;
+                    if (cls) {
+                        const int pu = ux == 2 ? z : ux == 1 ? y : x;
+                        idx = pu * 9 + c1_class(ux == 2 ? y : z) * 3 + c1_class(ux == 0 ? y : x);
+                    } else {
+                        idx = (z * S::D2 + y) * S::D2 + x;
+                    }
+                    val = *reinterpret_cast<const uint4*>(A1 + (size_t)idx * 16);
+                }
+                *reinterpret_cast<uint4*>(dst + ti * 4096) = val;
+            }
+            if (!staged()) return false;
+            if (t == 0) {
+                for (int ti = 0; ti < S::TAPS; ++ti)
+                    umma_bf16(tmem + S::C2,
+                              umma_smem_desc(smem_u32(opa() + ti * 4096), 128, 256),
+                              umma_smem_desc(smem_u32(sm + S::O_W2 + (cc * S::TAPS + ti) * 1024), 128, 256),
+                              umma_idesc_bf16<32>(), (cc | ti) ? 1u : 0u);
+                umma_commit(bar());
+            }
+            complete(err);
+        }
+        // epilogue: the tile's rows (two 16-column halves) into shared memory
+        // (the operand area, free once the MMAs completed) ...
+        __nv_bfloat16* a2s = reinterpret_cast<__nv_bfloat16*>(opa());
+        {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + S::C2 + 16 * sub, v);
+            stem_store16(v, b2() + 16 * sub, a2s + (size_t)(32 * q + lane) * 32 + 16 * sub);
+        }
+        tc_fence_before();
+        __syncthreads();
+        // ... then the group's a2 rows (four 16-byte parts each)
+        for (int e = t; e < 4 * nc * S::P3; e += S::NT) {
+            const int row = e >> 2, k = e & 3;
+            const int cb2 = row / S::P3, pp = row % S::P3;
+            const int u = cb2 == 0 ? ux0 : ux1;
+            int src = pp;
+            if (u >= 0) {
+                const int pz = pp / (S::D3 * S::D3), py = (pp / S::D3) % S::D3, px = pp % S::D3;
+                const int qu = u == 2 ? pz : u == 1 ? py : px;
+                src = qu * 9 + c2_class(u == 2 ? py : pz) * 3 + c2_class(u == 0 ? py : px);
+            }
+            *reinterpret_cast<uint4*>(a2 + (size_t)row * 32 + 8 * k) =
+                *reinterpret_cast<const uint4*>(a2s + (size_t)(cb2 * S::P3 + src) * 32 + 8 * k);
         }
         __syncthreads();  // the operand area is reused by the next group
         return !aborted();
