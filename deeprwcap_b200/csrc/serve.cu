@@ -1085,7 +1085,15 @@ static int sv_step(drwc_server* v, int k) {
     for (int b = 0; b < v->o.n_sizes; ++b)
         if (!v->bnet[b] && (rc = fork_fdm(b))) return rc;
     if (v->any_net && (rc = sv_mark(v, v->ev_t[k][0], s))) return rc;
-    for (int b = 0; b < v->o.n_sizes; ++b) {
+    // network stages largest cubes first: each bucket's FDM rows (audits,
+    // fallbacks) fork once its sampler has run, so the longest solves overlap
+    // the other buckets' network stages instead of ending the step
+    int order[DRWC_SERVER_MAX_SIZES];
+    for (int b = 0; b < v->o.n_sizes; ++b) order[b] = b;
+    std::sort(order, order + v->o.n_sizes,
+              [&](int a, int c) { return v->o.sizes[a] > v->o.sizes[c]; });
+    for (int i = 0; i < v->o.n_sizes; ++i) {
+        const int b = order[i];
         if (!v->bnet[b]) continue;
         const int g2 = std::min(A.S, ctx->sm_count * 16);
         rc = dispatch_N(v->o.sizes[b], [&](auto nc) -> int {

@@ -52,6 +52,23 @@ def test_served_job_equals_frw_run(ctx):
     assert st["completed"] == 1 and st["fdm_hops"] >= r.hops
 
 
+@pytest.mark.parametrize("fdm_hops,straggler_hops", [(1, 0), (64, 2), (5, 1)])
+def test_continuing_walks_give_the_same_rows(ctx, fdm_hops, straggler_hops):
+    """Walks that take several hops per step inside the FDM bucket (every
+    walk past its first hops, or past its second; at most 5 or 64 per step;
+    or none with fdm_hops = 1) give exactly drwc_frw_run's rows, alone and
+    beside a second job: a hop's draws depend only on (walk, hop)."""
+    jobs = [(W.two_layer_crossing(), _params(16, 21, 2 * 16384 + 777, 16384)),
+            (W.wire_stack(3, 5, diel_eps=[3.0, 4.0, 2.5], n_diel_blocks=4, seed=6),
+             _params(21, 22, 20000, 8192))]
+    alone = [engine.extract(s, p, ctx) for s, p in jobs]
+    with engine.Server(ctx, slots=4096, fdm_hops=fdm_hops, straggler_hops=straggler_hops) as srv:
+        ids = [srv.submit(s, p) for s, p in jobs]
+        res = [srv.wait(i, timeout=600) for i in ids]
+    for r, a in zip(res, alone):
+        _same(r, a)
+
+
 def test_mix_equals_alone_with_admission_by_footprint(ctx):
     jobs = _jobs()
     alone = [engine.extract(s, p, ctx) for s, p in jobs]
