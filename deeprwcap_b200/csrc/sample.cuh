@@ -26,7 +26,9 @@ DRWC_DEV double warp_incl_scan_d(double v) {
 // w: M weights in shared memory. Weight of panel b is |w_b| (use_abs) or
 // max(w_b, 0). red: scratch of >= NW + 4 doubles. Returns the panel (all
 // threads), -1 when every weight is zero; *total receives sum of weights.
-template <int NT>
+// TAIL = false leaves out the closing barrier (the one that lets the caller
+// write red again) for a caller that meets at a barrier of its own first.
+template <int NT, bool TAIL = true>
 DRWC_DEV int cta_sample(const double* w, int M, bool use_abs, double u, double* red,
                         double* total) {
     constexpr int NW = NT / 32;
@@ -77,7 +79,7 @@ DRWC_DEV int cta_sample(const double* w, int M, bool use_abs, double u, double* 
     int best = 0x7fffffff;
 #pragma unroll
     for (int q = 0; q < NW; ++q) best = min(best, ired[q]);
-    __syncthreads();
+    if constexpr (TAIL) __syncthreads();
     if (total) *total = tot;
     if (best == 0x7fffffff) best = lastall;
     return best;

@@ -161,7 +161,8 @@ walk_kernel(DevGeom g, Gauss G, WalkParams W, long long walk0, long long nwalks,
                                     : philox_uniform2(W.seed, w, (uint32_t)S.hops, 0);
             const double ud = first ? u.y : u.x;
             double tot = 0.0;
-            const int b = cta_sample<D::NT>(wv, M, first, ud, sm.red, &tot);
+            // the hop's closing barrier comes before red is written again
+            const int b = cta_sample<D::NT, false>(wv, M, first, ud, sm.red, &tot);
             if (t == 0) {
                 my_hops += 1;
                 my_iters += (unsigned long long)st.iters;
