@@ -67,28 +67,37 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.rows = []
-        self._stop = threading.Event()
         self._t = None
 
     def __enter__(self):
+        # one nvidia-smi process printing a line every 50 ms (a process per
+        # sample takes longer to start than a short timed region lasts)
+        self._p = None
+        try:
+            self._p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            return self
+
         def run():
-            while not self._stop.is_set():
-                try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.device),
-                                          f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
-                                         capture_output=True, text=True, timeout=5).stdout
-                    for line in out.strip().splitlines():
-                        self.rows.append([x.strip() for x in line.split(",")])
-                except Exception:
-                    pass
-                self._stop.wait(0.2)
+            for line in self._p.stdout:
+                if line.strip():
+                    self.rows.append([x.strip() for x in line.split(",")])
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
         return self
 
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self._p is None:
+            return
+        self._p.terminate()
+        try:
+            self._p.wait(timeout=5)
+        except Exception:
+            self._p.kill()
+        self._t.join(timeout=5)
 
     def summary(self):
         if not self.rows:
@@ -893,7 +902,8 @@ def run_fdm_batch(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 20; 5 for --impl reference, whose steps are ~8 s each)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--walks", type=int, default=32768)
@@ -914,6 +924,8 @@ def main():
     ap.add_argument("--serve-walks-max", type=float, default=1e7)
     ap.add_argument("--serve-train-samples", type=int, default=1 << 20)
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 5 if args.impl == "reference" else 20
     world, rank, local = dist_init()
     if args.workload == "fdm_batch":
         run_fdm_batch(args, world, rank, local)
